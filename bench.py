@@ -1,0 +1,356 @@
+"""Benchmark: fused set-algebra throughput on the 4096x4096 shape workload.
+
+Workload (one "step").  The expression ((A|B) - (C&D)) ^ E over the 4096x4096
+shapes: A = disk r=1500, B = annulus 800-1200, C = 64-px checkerboard,
+D = union of 200 seeded circles, E = the checkerboard shifted by 32 px.
+One copy is about 3e5 input intervals (2.4 MB), small enough to live in L2.
+The batch therefore stacks `--copies` x-shifted copies on disjoint row
+bands.  The default of 128 copies is 3.8e7 intervals, about 300 MB of
+inputs, which is larger than the 126 MB L2.  Every step evaluates the whole
+batch in one fused launch.
+
+Metric: input intervals per second (Gintervals/s), the reference's
+convention (subsetix_cupy/benchmarks/cases.py:88).  `value` is device-timed
+with the inputs resident in HBM.  `e2e` goes through the public API
+(subsetix_cupy.evaluate) with pinned host buffers: H2D copies of the
+operands, evaluation, then D2H of the result, all inside the timed region.
+
+Multi-GPU: every rank evaluates its own batch (weak scaling, no
+collective).  Times are the max over ranks.
+
+`--impl reference` times the reference algorithm on the host CPU: the
+reference's own kernel code compiled for the host (oracle/_ref) when
+available, else the oracle port.  It reports the same metric and config.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+SPEC = ("symmetric_difference", ("difference", ("union", "A", "B"), ("intersection", "C", "D")), "E")
+METRIC = "set-op Gintervals/s (fused ((A|B)-(C&D))^E, input intervals/s)"
+UNIT = "Gintervals/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=50)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--copies", type=int, default=128)
+    p.add_argument("--e2e-steps", type=int, default=5)
+    p.add_argument("--cpu-seconds", type=float, default=10.0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def workload(copies: int):
+    from subsetix_b200 import synth
+
+    shapes = synth.shape_operands(4096)
+    return [synth.stack_rows(s, copies, 4096) for s in shapes]
+
+
+def algorithmic_bytes(leaves, n_out: int, r_out: int) -> int:
+    """Minimum traffic of one evaluation: every input once, the output once.
+
+    8 bytes per input interval, 8 per output interval, 4 per row-offset
+    entry and 4 per row id, counting the leaves and the result.
+    """
+    total = 8 * n_out + 4 * (r_out + 1) + 4 * r_out
+    for b, _, off, rows in leaves:
+        total += 8 * int(b.size) + 4 * int(off.size) + 4 * int(rows.size)
+    return total
+
+
+class ClockSampler:
+    """Polls SM clocks and throttle reasons through NVML while the timed region runs."""
+
+    REASONS = {
+        "hw_slowdown": 0x8,
+        "hw_thermal_slowdown": 0x40,
+        "sw_thermal_slowdown": 0x20,
+        "sw_power_cap": 0x4,
+        "hw_power_brake_slowdown": 0x80,
+    }
+
+    def __init__(self, index: int, period: float = 0.005):
+        self.index = index
+        self.period = period
+        self.samples = []
+        self.reasons = set()
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._thread = None
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            self.handle = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.handle, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.nvml = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                mhz = self.nvml.nvmlDeviceGetClockInfo(self.handle, self.nvml.NVML_CLOCK_SM)
+                active = self.nvml.nvmlDeviceGetCurrentClocksEventReasons(self.handle)
+                self.samples.append(mhz)
+                for name, bit in self.REASONS.items():
+                    if active & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(self.period)
+
+    def __enter__(self):
+        if self.nvml is not None:
+            self._thread = threading.Thread(target=self._run, daemon=True)
+            self._thread.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._thread is not None:
+            self._thread.join()
+
+    def summary(self):
+        if self.nvml is None or not self.samples:
+            return None
+        return {"sm_mhz": float(statistics.median(self.samples)), "sm_max_mhz": float(self.max_mhz),
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+def peak_hbm():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_per_launch(copies: int):
+    """DRAM bytes of one fused launch, from the committed ncu summary (scaled by copies)."""
+    path = os.path.join(REPO, "profiles", "sx_sweep_kernel_shapes4096.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_copy:"):
+                return int(float(line.split(":")[1]) * copies)
+    except OSError:
+        pass
+    return None
+
+
+def cpu_baseline(leaves_host, seconds: float, use_ref: bool):
+    """Time the host implementation on a bounded sample (whole copies of the workload)."""
+    from oracle import oracle as O
+
+    runner = None
+    kind = "port"
+    cores = O.threads()
+    if use_ref:
+        try:
+            from oracle import ref_runner
+
+            if ref_runner.available():
+                runner = ref_runner
+                kind = "reference"
+                cores = ref_runner.threads()
+        except Exception:
+            runner = None
+    one = [tuple(a for a in leaf) for leaf in leaves_host]
+    leaves = {n: O.ISet(*h) for n, h in zip("ABCDE", one)}
+    n_in = sum(int(h[0].size) for h in one)
+    done = 0
+    t0 = time.perf_counter()
+    while True:
+        if runner is not None:
+            runner.evaluate(SPEC, leaves)
+        else:
+            O.evaluate(SPEC, leaves)
+        done += 1
+        if time.perf_counter() - t0 >= seconds:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": n_in * done / dt / 1e9, "unit": UNIT, "cores": int(cores), "kind": kind,
+            "sample": f"{done} evaluations of one 4096x4096 copy ({n_in} input intervals), {dt:.1f} s"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from subsetix_b200 import synth
+
+    one = [synth.stack_rows(s, 1, 4096) for s in synth.shape_operands(4096)]
+    vals = []
+    base = None
+    for _ in range(args.warmup):
+        cpu_baseline(one, 0.0, True)
+    for _ in range(args.steps):
+        base = cpu_baseline(one, 0.0, True)
+        vals.append(base["value"])
+    value = float(statistics.median(vals)) if vals else 0.0
+    n_in = sum(int(h[0].size) for h in one)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": n_in / (value * 1e9) * 1e3 if value else None,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": "shapes4096 ((A|B)-(C&D))^E, one copy per step on the host CPU", "copies": 1,
+                   "input_intervals_per_step": n_in},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": base["cores"] if base else None,
+                         "kind": base["kind"] if base else None, "sample": "one copy per step"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", init_method="env://", timeout=timedelta(seconds=120),
+                                device_id=device)
+
+    from subsetix_b200 import _core, _lib
+    from subsetix_b200.subsetix_cupy import expressions as E
+
+    leaves_host = workload(args.copies)
+    n_in = sum(int(h[0].size) for h in leaves_host)
+    R = int(leaves_host[0][3].size)
+    dev = [tuple(torch.as_tensor(a, device=device) for a in h) for h in leaves_host]
+    node = E._remap(("symmetric_difference", ("difference", ("union", ("leaf", 0), ("leaf", 1)),
+                                               ("intersection", ("leaf", 2), ("leaf", 3))), ("leaf", 4)), {i: i for i in range(5)})
+    table = E.truth_table(node, 5)
+    specs = [(b, e, off, 0) for b, e, off, _ in dev]
+    cap = max(1, n_in)
+    ob = torch.empty(cap, dtype=torch.int32, device=device)
+    oe = torch.empty(cap, dtype=torch.int32, device=device)
+    res_buf = torch.empty(2, dtype=torch.int32, device=device)
+    off_buf = torch.empty(R + 1, dtype=torch.int32, device=device)
+
+    def step():
+        return _core.bool_eval_async(specs, R, table, _lib.MODE_TABLE, device, out=(ob, oe), result=res_buf,
+                                     offsets=off_buf)
+
+    # correctness guard + output size for the roofline bytes
+    _, _, ooff, result = step()
+    total, flags = (int(x) for x in result.cpu())
+    if flags:
+        raise SystemExit(f"fused kernel raised flags {flags}")
+    algo = algorithmic_bytes(leaves_host, total, R)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    stream = torch.cuda.current_stream(device)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        ev[0].record(stream)
+        for i in range(args.steps):
+            step()
+            ev[i + 1].record(stream)
+        torch.cuda.synchronize()
+    per_step = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
+    elapsed_ms = ev[0].elapsed_time(ev[-1])
+    if world > 1:
+        t = torch.tensor([elapsed_ms], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+    value = world * n_in * args.steps / (elapsed_ms / 1e3) / 1e9
+
+    # end to end through the public API with pinned host buffers
+    pinned = [tuple(torch.as_tensor(a).pin_memory() for a in h) for h in leaves_host]
+    h2d = sum(sum(int(t.numel()) * 4 for t in h) for h in pinned)
+    e2e_times = []
+    d2h = 0
+    for i in range(args.e2e_steps + 1):
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        s0.record(stream)
+        sets = []
+        for b, e, off, rows in pinned:
+            tb, te, to, tr = (x.to(device, non_blocking=True) for x in (b, e, off, rows))
+            s = E.IntervalSet._trusted(tb, te, to, tr, R)
+            sets.append(s)
+        A, B, C, D, F = [E.make_input(s) for s in sets]
+        res = E.evaluate(E.make_symmetric_difference(E.make_difference(E.make_union(A, B), E.make_intersection(C, D)), F))
+        outs = [torch.empty(x.shape, dtype=x.dtype, pin_memory=True) for x in (res.begin, res.end, res.row_offsets)]
+        for o, x in zip(outs, (res.begin, res.end, res.row_offsets)):
+            o.copy_(x, non_blocking=True)
+        s1.record(stream)
+        torch.cuda.synchronize()
+        d2h = sum(int(o.numel()) * 4 for o in outs)
+        if i > 0:
+            e2e_times.append(s0.elapsed_time(s1))
+    e2e_ms = statistics.median(e2e_times)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * n_in / (e2e_ms / 1e3) / 1e9
+
+    kernel_ms = statistics.mean(per_step)
+    peak, peak_kind = peak_hbm()
+    achieved = algo / (kernel_ms / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int32", "data": "synthetic",
+        "config": {"workload": f"shapes4096 ((A|B)-(C&D))^E x{args.copies} stacked copies per rank",
+                   "copies": args.copies, "input_intervals_per_step": n_in, "output_intervals": total,
+                   "rows": R, "l2": "inputs larger than L2 (no flush)", "parallelism": f"independent batch per rank x{world}"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": e2e_ms},
+        "gpu_launches": args.steps,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic_per_launch(args.copies),
+                     "peak_source": peak_kind, "algorithmic_bytes": algo, "kernel": "sx_sweep_kernel<5,MODE_TABLE>",
+                     "kernel_ms": kernel_ms},
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        one = [synth_one for synth_one in workload(1)]
+        line["cpu_baseline"] = cpu_baseline(one, args.cpu_seconds, True)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

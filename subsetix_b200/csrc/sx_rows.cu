@@ -1,0 +1,106 @@
+// Row alignment: the sorted union of several row-id lists, and each list's
+// row offsets re-expressed on that union.
+//
+// This is the device form of the reference's _align_interval_sets /
+// _reindex_interval_set (subsetix_cupy/expressions.py:58-141).  The output
+// row list is union1d of the operands' rows.  Each operand keeps its
+// intervals in order, and rows it lacks become empty rows.  Because the
+// intervals keep their order, only the offsets change:
+//     aligned_off[y] = off[lower_bound(rows + shift, rows_out[y])].
+// Dilation uses the same kernels.  There each list is a set's occupied rows
+// shifted by dy (skip_empty = 1), matching morphology.py:236-247.
+//
+// The union is built from a bitmap over [row_min, row_max], a scan of the
+// per-word popcounts, and a compaction.  row_min and row_max come from the
+// host.
+
+#include "sx_internal.cuh"
+
+__global__ void sx_align_clear_kernel(unsigned* bitmap, long long nwords)
+{
+    for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < nwords;
+         w += (long long)gridDim.x * blockDim.x)
+        bitmap[w] = 0u;
+}
+
+__global__ void sx_align_mark_kernel(SxAlignArgs A)
+{
+    const int l = blockIdx.y;
+    const SxRowList L = A.list[l];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L.count; i += gridDim.x * blockDim.x) {
+        if (L.skip_empty && L.off[i + 1] <= L.off[i]) continue;
+        const long long v = (long long)L.rows[i] + L.shift - A.row_min;
+        if (v < 0 || v >= A.nbits) continue;  // excluded by the caller's bounds
+        atomicOr(&A.bitmap[v >> 5], 1u << (v & 31));
+    }
+}
+
+__global__ void sx_align_popc_kernel(const unsigned* bitmap, long long nwords, int* wcount)
+{
+    for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < nwords;
+         w += (long long)gridDim.x * blockDim.x)
+        wcount[w] = __popc(bitmap[w]);
+}
+
+__global__ void sx_align_compact_kernel(SxAlignArgs A, long long nwords)
+{
+    for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < nwords;
+         w += (long long)gridDim.x * blockDim.x) {
+        unsigned m = A.bitmap[w];
+        int o = A.wprefix[w];
+        while (m) {
+            const int bit = __ffs(m) - 1;
+            m &= m - 1u;
+            A.rows_out[o++] = A.row_min + (int)(w * 32 + bit);
+        }
+    }
+}
+
+// aligned[l][y] for y in [0, R_out]; R_out is read from the device.
+__global__ void sx_align_offsets_kernel(SxAlignArgs A)
+{
+    const int l = blockIdx.y;
+    int* dst = A.aligned[l];
+    if (dst == nullptr) return;
+    const SxRowList L = A.list[l];
+    const int rout = A.result[0];
+    for (int y = blockIdx.x * blockDim.x + threadIdx.x; y <= rout; y += gridDim.x * blockDim.x) {
+        int pos;
+        if (y == rout) {
+            pos = L.count;
+        } else {
+            const long long key = (long long)A.rows_out[y] - L.shift;
+            int lo = 0, hi = L.count;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if ((long long)L.rows[mid] < key) lo = mid + 1; else hi = mid;
+            }
+            pos = lo;
+        }
+        dst[y] = L.count > 0 ? L.off[pos] : 0;
+    }
+}
+
+cudaError_t sx_align_launch(SxAlignArgs& A, int out_capacity, const SxScanState& st, cudaStream_t stream)
+{
+    const long long nwords = (A.nbits + 31) / 32;
+    const int block = 256;
+    int grid = (int)((nwords + block - 1) / block);
+    if (grid < 1) grid = 1;
+    if (grid > 4096) grid = 4096;
+    sx_align_clear_kernel<<<grid, block, 0, stream>>>(A.bitmap, nwords);
+    int maxc = 1;
+    for (int l = 0; l < A.k; ++l) maxc = A.list[l].count > maxc ? A.list[l].count : maxc;
+    int gx = (maxc + block - 1) / block;
+    if (gx > 4096) gx = 4096;
+    sx_align_mark_kernel<<<dim3(gx, A.k), block, 0, stream>>>(A);
+    sx_align_popc_kernel<<<grid, block, 0, stream>>>(A.bitmap, nwords, A.wcount);
+    cudaError_t err = sx_scan_i32_launch(A.wcount, nwords, A.wprefix, A.result, st, stream);
+    if (err != cudaSuccess) return err;
+    sx_align_compact_kernel<<<grid, block, 0, stream>>>(A, nwords);
+    int gy = (out_capacity + 1 + block - 1) / block;
+    if (gy > 4096) gy = 4096;
+    if (gy < 1) gy = 1;
+    sx_align_offsets_kernel<<<dim3(gy, A.k), block, 0, stream>>>(A);
+    return cudaGetLastError();
+}

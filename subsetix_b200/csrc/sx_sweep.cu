@@ -1,0 +1,707 @@
+// Row sweeps: fused boolean expressions over canonical sets, and run merging
+// of widened, row-shifted sets (dilation).
+//
+// Why one kernel covers a whole expression.  Take canonical sets: inside
+// each row, intervals are non-empty, strictly increasing and non-touching.
+// On them the reference's union, intersection, difference and xor each
+// return the maximal runs of the cell-set result
+// (subsetix_cupy/kernels.py:36-113; xor is (A\B) | (B\A),
+// expressions.py:380-388).  Maximal runs are canonical again, so any nested
+// expression of those ops returns the maximal runs of f(in_1(x), ...,
+// in_k(x)), where f is the expression as a boolean function.  MODE_TABLE
+// computes exactly that from a truth table of f.
+//
+// MODE_UNION merges widened intervals ([b - w, e + w)) from k row-shifted
+// views of one set.  A run continues while the next begin is <= the running
+// end.  This is the merge of subsetix_cupy/kernels.py:292-381 after the
+// (row, begin) sort of morphology.py:21-107, which dilation uses
+// (morphology.py:211-248).  It needs non-empty intervals with strictly
+// increasing begins and ends inside each row.
+//
+// Layout of the work.  One lane owns one row of the aligned row list, and a
+// warp owns a tile of 32 consecutive rows.  A lane sweeps its row as a k-way
+// merge of the leaves' boundary streams in coordinate order.  It applies
+// every event at a coordinate, then evaluates f once.  A change of f opens
+// or closes a run.
+//   pass 1   count the row's runs;
+//   scan     warp-wide exclusive scan of the counts, then a look-back over
+//            tiles for the tile's global base;
+//   pass 2   sweep the row again and write its runs.  The row's intervals
+//            were read moments before, so this second read is served from
+//            L1/L2 and DRAM sees each input about once.
+// No shared memory is used.  A row of any length stays on one lane, so
+// there is no tile capacity to overflow.
+//
+// Look-back.  Tiles publish their aggregate and, once known, their
+// inclusive prefix (sx_common.cuh).  Groups of 32 consecutive tiles also
+// publish a group aggregate (the last member to finish adds it up) and a
+// group prefix (posted by the group's last tile).  A tile walks back at
+// most 31 tile statuses of its own group, then whole groups, 32 per step.
+// The walk stays short even with thousands of tiles in flight.
+//
+// Inputs outside the contract raise SXF_CONTRACT, and the host then reruns
+// the exact reference-order kernels (sx_exact.cu).  All waits are bounded
+// (SX_LOOKBACK_SPIN_LIMIT).
+
+#include <climits>
+
+#include "sx_internal.cuh"
+
+#define SX_SWEEP_WARPS 8
+#define SX_GROUP 32
+
+enum { MODE_TABLE = 0, MODE_UNION = 1 };
+
+// Look-back state in the workspace: counters[4] | tile status[tiles] |
+// group status[groups] | group sum[groups] | group count[groups].
+struct SxSweepState {
+    unsigned* counters;
+    unsigned long long* tile_status;
+    unsigned long long* group_status;
+    int* group_sum;
+    unsigned* group_count;
+};
+
+__device__ __forceinline__ unsigned long long sx_ld_status(const unsigned long long* p)
+{
+    return *((volatile const unsigned long long*)p);
+}
+
+// Wait until a status word is published (kind != 0); bounded.
+__device__ __forceinline__ unsigned long long sx_wait_status(const unsigned long long* p, bool& timed_out)
+{
+    unsigned spins = 0;
+    while (true) {
+        const unsigned long long w = sx_ld_status(p);
+        if ((w >> 32) & 3ull) return w;
+        if (++spins > SX_LOOKBACK_SPIN_LIMIT) {
+            timed_out = true;
+            return (SX_KIND_PREFIX << 32);  // treat as a zero prefix so the kernel finishes
+        }
+        if (spins > 4) __nanosleep(32);
+    }
+}
+
+__device__ __forceinline__ unsigned long long sx_word(unsigned long long kind, int value)
+{
+    return (kind << 32) | (unsigned long long)(unsigned)value;
+}
+
+// Returns the exclusive prefix of `tile` (whole warp participates).
+__device__ __forceinline__ int sx_hier_lookback(const SxSweepState& st, int tile, int tiles, int aggregate,
+                                                unsigned& flags)
+{
+    const int lane = threadIdx.x & 31;
+    const int group = tile / SX_GROUP;
+    const int gfirst = group * SX_GROUP;
+    const int gsize = min(SX_GROUP, tiles - gfirst);
+    bool timed_out = false;
+    int exclusive = 0;
+    if (tile == 0) {
+        if (lane == 0) atomicExch(&st.tile_status[0], sx_word(SX_KIND_PREFIX, aggregate));
+    } else {
+        if (lane == 0) atomicExch(&st.tile_status[tile], sx_word(SX_KIND_AGG, aggregate));
+    }
+    // group aggregate: the last member to add publishes it (never over a prefix)
+    if (lane == 0) {
+        atomicAdd(&st.group_sum[group], aggregate);
+        __threadfence();
+        const unsigned done = atomicAdd(&st.group_count[group], 1u);
+        if (done == (unsigned)gsize - 1u) {
+            __threadfence();
+            const int gsum = atomicAdd(&st.group_sum[group], 0);
+            atomicCAS(&st.group_status[group], 0ull, sx_word(SX_KIND_AGG, gsum));
+        }
+    }
+    if (tile > 0) {
+        // 1. tiles of the own group before this one (at most 31)
+        bool found = false;
+        {
+            const int t = tile - 1 - lane;
+            unsigned long long w = sx_word(SX_KIND_AGG, 0);
+            if (t >= gfirst) w = sx_wait_status(&st.tile_status[t], timed_out);
+            const bool is_prefix = (t >= gfirst) && (((w >> 32) & 3ull) == SX_KIND_PREFIX);
+            const unsigned pm = __ballot_sync(0xFFFFFFFFu, is_prefix);
+            const int stop = pm ? __ffs(pm) - 1 : 32;
+            int v = (t >= gfirst && lane <= stop) ? (int)(unsigned)(w & 0xFFFFFFFFull) : 0;
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+            exclusive = v;
+            found = pm != 0u;
+        }
+        // 2. whole groups before the own group, 32 per step
+        int g = group - 1;
+        while (!found && g >= 0) {
+            const int gg = g - lane;
+            unsigned long long w = sx_word(SX_KIND_PREFIX, 0);
+            if (gg >= 0) w = sx_wait_status(&st.group_status[gg], timed_out);
+            const bool is_prefix = ((w >> 32) & 3ull) == SX_KIND_PREFIX;
+            const unsigned pm = __ballot_sync(0xFFFFFFFFu, is_prefix);
+            const int stop = pm ? __ffs(pm) - 1 : 32;
+            int v = (gg >= 0 && lane <= stop) ? (int)(unsigned)(w & 0xFFFFFFFFull) : 0;
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+            exclusive += v;
+            found = pm != 0u;
+            g -= 32;
+        }
+        if (lane == 0) atomicExch(&st.tile_status[tile], sx_word(SX_KIND_PREFIX, exclusive + aggregate));
+    }
+    if (lane == 0 && tile == gfirst + gsize - 1)
+        atomicExch(&st.group_status[group], sx_word(SX_KIND_PREFIX, exclusive + aggregate));
+    if (__any_sync(0xFFFFFFFFu, timed_out)) flags |= SXF_TIMEOUT;
+    return exclusive;
+}
+
+__device__ __forceinline__ bool sx_table(const SxBoolArgs& A, unsigned state)
+{
+    return (A.table[state >> 5] >> (state & 31u)) & 1u;
+}
+
+// One row, canonical leaves, truth-table function.  Returns the run count;
+// writes runs at out_begin/out_end + pos when WRITE.
+template <int K, bool WRITE>
+__device__ __forceinline__ int sx_sweep_table(const SxBoolArgs& A, const int* s, const int* lim, int* out_b, int* out_e,
+                                              long long pos, bool& bad, bool& over)
+{
+    int q[K], h[K];
+    int rem = 0;
+#pragma unroll
+    for (int l = 0; l < K; ++l) {
+        q[l] = 0;
+        h[l] = lim[l] > 0 ? __ldg(A.leaf[l].begin + s[l]) : INT_MAX;
+        rem += lim[l];
+    }
+    unsigned state = 0u;
+    bool fprev = false;
+    int run_start = 0;
+    int n = 0;
+    while (rem > 0) {
+        int c = INT_MAX;
+#pragma unroll
+        for (int l = 0; l < K; ++l)
+            if (q[l] < lim[l]) c = min(c, h[l]);
+#pragma unroll
+        for (int l = 0; l < K; ++l) {
+            if (q[l] < lim[l] && h[l] == c) {
+                state ^= 1u << l;
+                const int qn = q[l] + 1;
+                q[l] = qn;
+                --rem;
+                if (qn < lim[l]) {
+                    const int i = s[l] + (qn >> 1);
+                    const int v = (qn & 1) ? __ldg(A.leaf[l].end + i) : __ldg(A.leaf[l].begin + i);
+                    if (v <= c) bad = true;  // boundaries must rise strictly: non-empty, non-touching
+                    h[l] = v;
+                }
+            }
+        }
+        const bool fn = sx_table(A, state);
+        if (fn != fprev) {
+            if (fn) {
+                run_start = c;
+            } else {
+                if (WRITE) {
+                    const long long o = pos + n;
+                    if (o < A.capacity) {
+                        out_b[o] = run_start;
+                        out_e[o] = c;
+                    } else {
+                        over = true;
+                    }
+                }
+                ++n;
+            }
+            fprev = fn;
+        }
+        if (c == INT_MAX) break;  // only reachable with malformed input
+    }
+    return n;
+}
+
+// One row, K row-shifted views of one set, widened by A.leaf[l].widen:
+// union with merge semantics (touching runs join).
+template <int K, bool WRITE>
+__device__ __forceinline__ int sx_sweep_union(const SxBoolArgs& A, const int* s, const int* cnt, int* out_b, int* out_e,
+                                              long long pos, bool& bad, bool& over)
+{
+    int qb[K], qe[K], hb[K], he[K];
+    int rem = 0;
+#pragma unroll
+    for (int l = 0; l < K; ++l) {
+        qb[l] = 0;
+        qe[l] = 0;
+        const int w = A.leaf[l].widen;
+        hb[l] = cnt[l] > 0 ? __ldg(A.leaf[l].begin + s[l]) - w : INT_MAX;
+        he[l] = cnt[l] > 0 ? __ldg(A.leaf[l].end + s[l]) + w : INT_MAX;
+        rem += 2 * cnt[l];
+    }
+    int active = 0;
+    int run_start = 0;
+    int n = 0;
+    while (rem > 0) {
+        int c = INT_MAX;
+#pragma unroll
+        for (int l = 0; l < K; ++l) {
+            if (qb[l] < cnt[l]) c = min(c, hb[l]);
+            if (qe[l] < cnt[l]) c = min(c, he[l]);
+        }
+        const bool was = active > 0;
+#pragma unroll
+        for (int l = 0; l < K; ++l) {
+            const int w = A.leaf[l].widen;
+            // ends before begins: an element whose begin has not been taken at
+            // an earlier coordinate is empty (or reversed) and breaks the contract
+            if (qe[l] < cnt[l] && he[l] == c) {
+                --active;
+                --rem;
+                if (qe[l] >= qb[l]) bad = true;
+                const int qn = ++qe[l];
+                if (qn < cnt[l]) {
+                    const int v = __ldg(A.leaf[l].end + s[l] + qn) + w;
+                    if (v <= c) bad = true;
+                    he[l] = v;
+                }
+            }
+            if (qb[l] < cnt[l] && hb[l] == c) {
+                ++active;
+                --rem;
+                const int qn = ++qb[l];
+                if (qn < cnt[l]) {
+                    const int v = __ldg(A.leaf[l].begin + s[l] + qn) - w;
+                    if (v <= c) bad = true;
+                    hb[l] = v;
+                }
+            }
+        }
+        const bool now = active > 0;
+        if (now != was) {
+            if (now) {
+                run_start = c;
+            } else {
+                if (WRITE) {
+                    const long long o = pos + n;
+                    if (o < A.capacity) {
+                        out_b[o] = run_start;
+                        out_e[o] = c;
+                    } else {
+                        over = true;
+                    }
+                }
+                ++n;
+            }
+        }
+        if (active < 0) bad = true;
+        if (c == INT_MAX) break;
+    }
+    return n;
+}
+
+template <int K, int MODE>
+__global__ void __launch_bounds__(32 * SX_SWEEP_WARPS) sx_sweep_kernel(SxBoolArgs A, SxSweepState st, int tiles)
+{
+    const int lane = threadIdx.x & 31;
+    const int wid = threadIdx.x >> 5;
+    if (blockIdx.x * SX_SWEEP_WARPS + wid >= tiles) return;  // exactly `tiles` warps take tickets
+
+    int tile = 0;
+    if (lane == 0) tile = (int)atomicAdd(&st.counters[0], 1u);
+    tile = __shfl_sync(0xFFFFFFFFu, tile, 0);
+
+    const int row = tile * 32 + lane;
+    const bool active = row < A.rows;
+    int s[K], lim[K];
+#pragma unroll
+    for (int l = 0; l < K; ++l) {
+        const int a = active ? A.leaf[l].off[row] : 0;
+        const int b = active ? A.leaf[l].off[row + 1] : 0;
+        s[l] = a;
+        lim[l] = MODE == MODE_TABLE ? 2 * (b - a) : (b - a);
+    }
+    bool bad = false, over = false;
+    int count = 0;
+    if (active) {
+        count = MODE == MODE_TABLE ? sx_sweep_table<K, false>(A, s, lim, nullptr, nullptr, 0, bad, over)
+                                   : sx_sweep_union<K, false>(A, s, lim, nullptr, nullptr, 0, bad, over);
+    }
+    int incl = count;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    const int total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    unsigned flags = __any_sync(0xFFFFFFFFu, bad) ? SXF_CONTRACT : 0u;
+    const int base = sx_hier_lookback(st, tile, tiles, total, flags);
+    if (active) {
+        const long long pos = (long long)base + incl - count;
+        if (count > 0) {
+            bool bad2 = false;
+            if (MODE == MODE_TABLE)
+                sx_sweep_table<K, true>(A, s, lim, A.out_begin, A.out_end, pos, bad2, over);
+            else
+                sx_sweep_union<K, true>(A, s, lim, A.out_begin, A.out_end, pos, bad2, over);
+        }
+        A.out_off[row + 1] = base + incl;
+        if (row == 0) A.out_off[0] = 0;
+    }
+    if (__any_sync(0xFFFFFFFFu, over)) flags |= SXF_CAPACITY;
+    if (lane == 0) {
+        // retire: the last tile publishes the total and the flags
+        if (flags) atomicOr(&st.counters[3], flags);
+        __threadfence();
+        const unsigned prev = atomicAdd(&st.counters[1], 1u);
+        if (prev == (unsigned)tiles - 1u) {
+            __threadfence();
+            const unsigned long long last = sx_ld_status(&st.tile_status[tiles - 1]);
+            const unsigned f = atomicExch(&st.counters[3], 0u);
+            A.result[0] = (int)(unsigned)(last & 0xFFFFFFFFull);
+            A.result[1] = (int)f;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Shared-memory form of the table sweep (the main path for set algebra).
+//
+// The warp stages its 32-row tile with coalesced loads.  Each leaf's
+// segment is stored interleaved, [b0, e0, b1, e1, ...], so a lane's
+// boundary stream for one leaf is contiguous.  The lane then sweeps its row
+// from shared memory in one pass.  Its runs go to a provisional slice of
+// the output staging area (a row never yields more runs than it has
+// elements).  After the warp scan and the look-back, the warp copies the
+// runs out to global memory with coalesced stores.  Tiles larger than the
+// staging capacity use the global-memory sweep above.
+// ---------------------------------------------------------------------------
+
+#define SX_SMEM_WARPS 4
+
+__host__ __device__ inline int sx_smem_warp_ints(int ecap) { return 4 * ecap + 8 + 64; }
+
+template <int K>
+__device__ __forceinline__ int sx_smem_sweep_table(const SxBoolArgs& A, const int* __restrict__ S, const int* qs,
+                                                   const int* qend, int* __restrict__ ob, int* __restrict__ oe,
+                                                   bool& bad)
+{
+    int q[K], h[K];
+#pragma unroll
+    for (int l = 0; l < K; ++l) {
+        q[l] = qs[l];
+        h[l] = q[l] < qend[l] ? S[q[l]] : INT_MAX;
+    }
+    unsigned state = 0u;
+    bool fprev = false;
+    int run_start = 0;
+    int n = 0;
+    while (true) {
+        int c = h[0];
+#pragma unroll
+        for (int l = 1; l < K; ++l) c = min(c, h[l]);
+        if (c == INT_MAX) break;
+#pragma unroll
+        for (int l = 0; l < K; ++l) {
+            if (h[l] == c) {
+                state ^= 1u << l;
+                const int qn = q[l] + 1;
+                q[l] = qn;
+                const int v = S[qn];  // one slot of slack after the staged data
+                if (qn < qend[l]) {
+                    if (v <= c) bad = true;
+                    h[l] = v;
+                } else {
+                    h[l] = INT_MAX;
+                }
+            }
+        }
+        const bool fn = sx_table(A, state);
+        if (fn != fprev) {
+            if (fn) {
+                run_start = c;
+            } else {
+                ob[n] = run_start;
+                oe[n] = c;
+                ++n;
+            }
+            fprev = fn;
+        }
+    }
+    return n;
+}
+
+template <int K>
+__global__ void __launch_bounds__(32 * SX_SMEM_WARPS) sx_sweep_smem_kernel(SxBoolArgs A, SxSweepState st, int tiles,
+                                                                          int ecap)
+{
+    extern __shared__ int smem_raw[];
+    const int lane = threadIdx.x & 31;
+    const int wid = threadIdx.x >> 5;
+    if (blockIdx.x * SX_SMEM_WARPS + wid >= tiles) return;  // exactly `tiles` warps take tickets
+    int* S = smem_raw + wid * sx_smem_warp_ints(ecap);
+    int* Ob = S + 2 * ecap + 8;
+    int* Oe = Ob + ecap;
+    int* X = Oe + ecap;  // [32] exclusive run counts, [32] provisional starts
+
+    int tile = 0;
+    if (lane == 0) tile = (int)atomicAdd(&st.counters[0], 1u);
+    tile = __shfl_sync(0xFFFFFFFFu, tile, 0);
+    const int lo = tile * 32;
+    const int hi = min(A.rows, lo + 32);
+    const int row = lo + lane;
+    const bool active = row < A.rows;
+
+    // tile range of every leaf
+    int g0v = 0, g1v = 0;
+    if (lane < K) {
+        g0v = A.leaf[lane].off[lo];
+        g1v = A.leaf[lane].off[hi];
+    }
+    int g0[K], g1[K], lb2[K];
+    int E = 0;
+#pragma unroll
+    for (int l = 0; l < K; ++l) {
+        g0[l] = __shfl_sync(0xFFFFFFFFu, g0v, l);
+        g1[l] = __shfl_sync(0xFFFFFFFFu, g1v, l);
+        lb2[l] = 2 * E;
+        E += g1[l] - g0[l];
+    }
+    // this lane's row range in every leaf
+    int qs[K], qend[K], s[K], lim[K];
+    int nrow = 0;
+#pragma unroll
+    for (int l = 0; l < K; ++l) {
+        const int a = active ? A.leaf[l].off[row] : g1[l];
+        const int b = active ? A.leaf[l].off[row + 1] : g1[l];
+        qs[l] = lb2[l] + 2 * (a - g0[l]);
+        qend[l] = lb2[l] + 2 * (b - g0[l]);
+        s[l] = a;
+        lim[l] = 2 * (b - a);
+        nrow += b - a;
+    }
+    int prov = nrow;  // provisional start of this lane's runs (exclusive scan of row elements)
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xFFFFFFFFu, prov, o);
+        if (lane >= o) prov += y;
+    }
+    prov -= nrow;
+
+    const bool staged = E <= ecap;
+    bool bad = false, over = false;
+    int count = 0;
+    if (staged) {
+#pragma unroll
+        for (int l = 0; l < K; ++l) {
+            const int cnt = g1[l] - g0[l];
+            const int* gb = A.leaf[l].begin + g0[l];
+            const int* ge = A.leaf[l].end + g0[l];
+            for (int j = lane; j < cnt; j += 32) {
+                const int b = __ldg(gb + j);
+                const int e = __ldg(ge + j);
+                if (b == INT_MAX || e == INT_MAX) bad = true;  // reserved as the stream sentinel
+                S[lb2[l] + 2 * j] = b;
+                S[lb2[l] + 2 * j + 1] = e;
+            }
+        }
+        if (lane == 0) S[2 * E] = INT_MAX;
+        __syncwarp();
+        if (active) count = sx_smem_sweep_table<K>(A, S, qs, qend, Ob + prov, Oe + prov, bad);
+    } else if (active) {
+        count = sx_sweep_table<K, false>(A, s, lim, nullptr, nullptr, 0, bad, over);
+    }
+
+    int incl = count;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    const int total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    const int excl = incl - count;
+    unsigned flags = __any_sync(0xFFFFFFFFu, bad) ? SXF_CONTRACT : 0u;
+    const int base = sx_hier_lookback(st, tile, tiles, total, flags);
+
+    if (staged) {
+        X[lane] = excl;
+        X[32 + lane] = prov;
+        __syncwarp();
+        for (int i = lane; i < total; i += 32) {
+            int lo2 = 0, hi2 = 31;  // owner: last lane with excl <= i
+            while (lo2 < hi2) {
+                const int mid = (lo2 + hi2 + 1) >> 1;
+                if (X[mid] <= i) lo2 = mid; else hi2 = mid - 1;
+            }
+            const int src = X[32 + lo2] + (i - X[lo2]);
+            const long long o = (long long)base + i;
+            if (o < A.capacity) {
+                A.out_begin[o] = Ob[src];
+                A.out_end[o] = Oe[src];
+            } else {
+                over = true;
+            }
+        }
+    } else if (active && count > 0) {
+        bool bad2 = false;
+        sx_sweep_table<K, true>(A, s, lim, A.out_begin, A.out_end, (long long)base + excl, bad2, over);
+    }
+    if (active) {
+        A.out_off[row + 1] = base + incl;
+        if (row == 0) A.out_off[0] = 0;
+    }
+    if (__any_sync(0xFFFFFFFFu, over)) flags |= SXF_CAPACITY;
+    if (lane == 0) {
+        if (flags) atomicOr(&st.counters[3], flags);
+        __threadfence();
+        const unsigned prev = atomicAdd(&st.counters[1], 1u);
+        if (prev == (unsigned)tiles - 1u) {
+            __threadfence();
+            const unsigned long long last = sx_ld_status(&st.tile_status[tiles - 1]);
+            const unsigned f = atomicExch(&st.counters[3], 0u);
+            A.result[0] = (int)(unsigned)(last & 0xFFFFFFFFull);
+            A.result[1] = (int)f;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+
+static size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+size_t sx_sweep_state_bytes(long long tiles)
+{
+    const long long groups = (tiles + SX_GROUP - 1) / SX_GROUP;
+    return a256(16) + a256((size_t)tiles * 8) + a256((size_t)groups * 8) + a256((size_t)groups * 4) +
+           a256((size_t)groups * 4);
+}
+
+long long sx_sweep_tiles(int rows) { return ((long long)rows + 31) / 32; }
+
+static SxSweepState sx_sweep_state(void* ws, long long tiles)
+{
+    const long long groups = (tiles + SX_GROUP - 1) / SX_GROUP;
+    char* p = (char*)ws;
+    SxSweepState st;
+    st.counters = (unsigned*)p;
+    p += a256(16);
+    st.tile_status = (unsigned long long*)p;
+    p += a256((size_t)tiles * 8);
+    st.group_status = (unsigned long long*)p;
+    p += a256((size_t)groups * 8);
+    st.group_sum = (int*)p;
+    p += a256((size_t)groups * 4);
+    st.group_count = (unsigned*)p;
+    return st;
+}
+
+template <int K, int MODE>
+static cudaError_t sx_sweep_launch_k(const SxBoolArgs& A, const SxSweepState& st, int tiles, cudaStream_t stream)
+{
+    // Residency cap through unused dynamic shared memory.  Fewer resident
+    // rows keep every lane's boundary streams inside L1.
+    int pad = 0;
+    if (A.tune_blocks_per_sm > 0) {
+        pad = 233472 / A.tune_blocks_per_sm - 1024 - 256;
+        if (pad > 232448) pad = 232448;
+        if (pad < 0) pad = 0;
+        static int configured = 0;
+        if (pad > configured) {
+            cudaError_t err = cudaFuncSetAttribute(sx_sweep_kernel<K, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   pad);
+            if (err != cudaSuccess) return err;
+            configured = pad;
+        }
+    }
+    const int blocks = (tiles + SX_SWEEP_WARPS - 1) / SX_SWEEP_WARPS;
+    sx_sweep_kernel<K, MODE><<<blocks, 32 * SX_SWEEP_WARPS, pad, stream>>>(A, st, tiles);
+    return cudaGetLastError();
+}
+
+template <int K>
+static cudaError_t sx_sweep_smem_launch_k(const SxBoolArgs& A, const SxSweepState& st, int tiles, int ecap,
+                                          cudaStream_t stream)
+{
+    static int configured = 0;  // largest dynamic shared memory set for this instantiation
+    const int smem = SX_SMEM_WARPS * sx_smem_warp_ints(ecap) * (int)sizeof(int);
+    if (smem > configured) {
+        cudaError_t err = cudaFuncSetAttribute(sx_sweep_smem_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (err != cudaSuccess) return err;
+        configured = smem;
+    }
+    const int blocks = (tiles + SX_SMEM_WARPS - 1) / SX_SMEM_WARPS;
+    sx_sweep_smem_kernel<K><<<blocks, 32 * SX_SMEM_WARPS, smem, stream>>>(A, st, tiles, ecap);
+    return cudaGetLastError();
+}
+
+// Staging capacity per warp: 1.25x the average tile size, in [256, 3584]
+// elements.  Tiles above it take the global-memory sweep.  3584 keeps four
+// warps' staging under the 227 KB per-block limit.
+static int sx_pick_ecap(long long elems, long long tiles)
+{
+    long long avg = tiles > 0 ? (elems + tiles - 1) / tiles : 0;
+    long long e = (avg * 5) / 4;
+    e = (e + 63) / 64 * 64;
+    if (e < 256) e = 256;
+    if (e > 3584) e = 3584;
+    return (int)e;
+}
+
+cudaError_t sx_sweep_launch(const SxBoolArgs& A, bool union_mode, void* workspace, cudaStream_t stream)
+{
+    const long long tiles = sx_sweep_tiles(A.rows);
+    if (tiles <= 0) return cudaSuccess;
+    // The look-back state must start cleared; the workspace may hold other scratch.
+    cudaError_t err = cudaMemsetAsync(workspace, 0, sx_sweep_state_bytes(tiles), stream);
+    if (err != cudaSuccess) return err;
+    SxSweepState st = sx_sweep_state(workspace, tiles);
+    const int t = (int)tiles;
+    if (union_mode) {
+        switch (A.k) {
+            case 1: return sx_sweep_launch_k<1, MODE_UNION>(A, st, t, stream);
+            case 2: return sx_sweep_launch_k<2, MODE_UNION>(A, st, t, stream);
+            case 3: return sx_sweep_launch_k<3, MODE_UNION>(A, st, t, stream);
+            case 4: return sx_sweep_launch_k<4, MODE_UNION>(A, st, t, stream);
+            case 5: return sx_sweep_launch_k<5, MODE_UNION>(A, st, t, stream);
+            case 6: return sx_sweep_launch_k<6, MODE_UNION>(A, st, t, stream);
+            case 7: return sx_sweep_launch_k<7, MODE_UNION>(A, st, t, stream);
+            case 8: return sx_sweep_launch_k<8, MODE_UNION>(A, st, t, stream);
+            case 9: return sx_sweep_launch_k<9, MODE_UNION>(A, st, t, stream);
+            default: return cudaErrorInvalidValue;
+        }
+    }
+    // Automatic choice: staged sweep for light tiles (it keeps many warps
+    // resident), global sweep with a residency cap of 3 blocks per SM for
+    // heavy tiles (measured best on the 4096x4096 shape expression).
+    SxBoolArgs B = A;
+    if (B.tune_kernel == 0) {
+        const long long avg = (A.capacity + tiles - 1) / tiles;
+        B.tune_kernel = avg <= 1024 ? 2 : 1;
+        if (B.tune_kernel == 1 && B.tune_blocks_per_sm == 0) B.tune_blocks_per_sm = 3;
+    }
+    if (B.tune_kernel == 1) {
+        const SxBoolArgs& A = B;
+        switch (A.k) {
+            case 1: return sx_sweep_launch_k<1, MODE_TABLE>(A, st, t, stream);
+            case 2: return sx_sweep_launch_k<2, MODE_TABLE>(A, st, t, stream);
+            case 3: return sx_sweep_launch_k<3, MODE_TABLE>(A, st, t, stream);
+            case 4: return sx_sweep_launch_k<4, MODE_TABLE>(A, st, t, stream);
+            case 5: return sx_sweep_launch_k<5, MODE_TABLE>(A, st, t, stream);
+            case 6: return sx_sweep_launch_k<6, MODE_TABLE>(A, st, t, stream);
+            case 7: return sx_sweep_launch_k<7, MODE_TABLE>(A, st, t, stream);
+            case 8: return sx_sweep_launch_k<8, MODE_TABLE>(A, st, t, stream);
+            default: return cudaErrorInvalidValue;
+        }
+    }
+    int ecap = A.tune_staging_cap > 0 ? A.tune_staging_cap : sx_pick_ecap(A.capacity, tiles);
+    if (ecap > 3584) ecap = 3584;
+    if (ecap < 64) ecap = 64;
+    switch (A.k) {
+        case 1: return sx_sweep_smem_launch_k<1>(A, st, t, ecap, stream);
+        case 2: return sx_sweep_smem_launch_k<2>(A, st, t, ecap, stream);
+        case 3: return sx_sweep_smem_launch_k<3>(A, st, t, ecap, stream);
+        case 4: return sx_sweep_smem_launch_k<4>(A, st, t, ecap, stream);
+        case 5: return sx_sweep_smem_launch_k<5>(A, st, t, ecap, stream);
+        case 6: return sx_sweep_smem_launch_k<6>(A, st, t, ecap, stream);
+        case 7: return sx_sweep_smem_launch_k<7>(A, st, t, ecap, stream);
+        case 8: return sx_sweep_smem_launch_k<8>(A, st, t, ecap, stream);
+        default: return cudaErrorInvalidValue;
+    }
+}

@@ -1,0 +1,228 @@
+"""Set algebra on the GPU against the reference's goldens and the oracle.
+
+Interval outputs must be bit-exact: begin, end, row_offsets and rows.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from subsetix_b200 import synth
+from tests.golden_io import get_set, load
+from tests.gpu_util import assert_same, dev_set, host, iset
+
+pytestmark = pytest.mark.gpu
+
+sc = pytest.importorskip("subsetix_b200.subsetix_cupy")
+
+
+def _ops():
+    return {
+        "union": sc.make_union,
+        "intersection": sc.make_intersection,
+        "difference": sc.make_difference,
+        "symmetric_difference": sc.make_symmetric_difference,
+        "complement": sc.make_complement,
+    }
+
+
+@pytest.fixture(scope="module")
+def surfaces(cuda_device):
+    b = sc.build_interval_set
+    return {
+        "A": b(row_offsets=[0, 2, 3], begin=[0, 6, 1], end=[4, 9, 5]),
+        "B": b(row_offsets=[0, 1, 2], begin=[2, 0], end=[7, 4]),
+        "C": b(row_offsets=[0, 1, 2], begin=[3, 2], end=[6, 3]),
+        "D": b(row_offsets=[0, 1, 2], begin=[5, 5], end=[11, 8]),
+        "E": b(row_offsets=[0, 1, 2], begin=[7, 6], end=[10, 9]),
+    }
+
+
+def _check(result, begin, end, offsets, rows=None):
+    rows = list(range(len(offsets) - 1)) if rows is None else rows
+    assert_same(result, (begin, end, offsets, rows))
+
+
+# Golden vectors of the reference's own unit tests (subsetix_cupy/tests/test_expressions.py:154-309)
+
+def test_nested_expression(surfaces):
+    s = surfaces
+    expr = sc.make_union(
+        sc.make_difference(sc.make_intersection(sc.make_input(s["A"]), sc.make_input(s["B"])), sc.make_input(s["C"])),
+        sc.make_intersection(sc.make_input(s["D"]), sc.make_input(s["E"])))
+    _check(sc.evaluate(expr), [2, 6, 1, 3, 6], [3, 10, 2, 4, 8], [0, 2, 5])
+
+
+def test_union_aligns_sparse_rows(surfaces):
+    extra = sc.build_interval_set(row_offsets=[0, 1], begin=[0], end=[1])
+    _check(sc.evaluate(sc.make_union(sc.make_input(surfaces["A"]), sc.make_input(extra))),
+           [0, 6, 1], [4, 9, 5], [0, 2, 3])
+
+
+def test_difference_handles_empty_rhs(surfaces):
+    empty = sc.build_interval_set(row_offsets=[0, 0, 0], begin=[], end=[])
+    _check(sc.evaluate(sc.make_difference(sc.make_input(surfaces["A"]), sc.make_input(empty))),
+           [0, 6, 1], [4, 9, 5], [0, 2, 3])
+
+
+def test_union_sparse_row_ids(cuda_device):
+    lhs = sc.build_interval_set(row_offsets=[0, 1], begin=[0], end=[2], rows=[5])
+    rhs = sc.build_interval_set(row_offsets=[0, 1], begin=[3], end=[4], rows=[7])
+    _check(sc.evaluate(sc.make_union(sc.make_input(lhs), sc.make_input(rhs))), [0, 3], [2, 4], [0, 1, 2], [5, 7])
+
+
+def test_symmetric_difference(surfaces):
+    _check(sc.evaluate(sc.make_symmetric_difference(sc.make_input(surfaces["A"]), sc.make_input(surfaces["B"]))),
+           [0, 4, 7, 0, 4], [2, 6, 9, 1, 5], [0, 3, 5])
+
+
+def test_complement(surfaces):
+    universe = sc.build_interval_set(row_offsets=[0, 1, 2], begin=[0, 0], end=[12, 6])
+    _check(sc.evaluate(sc.make_complement(sc.make_input(universe), sc.make_input(surfaces["A"]))),
+           [4, 9, 0, 5], [6, 12, 1, 6], [0, 2, 4])
+
+
+def test_multishape_union(cuda_device):
+    rect = sc.build_interval_set(row_offsets=[0, 2, 4, 6], begin=[0, 4, 1, 5, 2, 6], end=[2, 6, 3, 7, 4, 8])
+    circ = sc.build_interval_set(row_offsets=[0, 1, 3, 4], begin=[1, 0, 4, 3], end=[5, 2, 6, 7])
+    _check(sc.evaluate(sc.make_union(sc.make_input(rect), sc.make_input(circ))), [0, 0, 4, 2], [6, 3, 7, 8],
+           [0, 1, 3, 4])
+    ws = sc.CuPyWorkspace()
+    _check(sc.evaluate(sc.make_union(sc.make_input(rect), sc.make_input(circ)), ws), [0, 0, 4, 2], [6, 3, 7, 8],
+           [0, 1, 3, 4])
+
+
+def test_backend_returns_device_arrays(surfaces):
+    s = surfaces
+    expr = sc.make_union(sc.make_intersection(sc.make_input(s["A"]), sc.make_input(s["B"])),
+                         sc.make_difference(sc.make_input(s["D"]), sc.make_input(s["C"])))
+    r = sc.evaluate(expr)
+    assert isinstance(r.begin, torch.Tensor) and r.begin.is_cuda
+    _check(r, [2, 6, 1, 5], [4, 11, 4, 8], [0, 2, 4])
+
+
+def test_workspace_reuses_output_buffers(surfaces):
+    ws = sc.CuPyWorkspace()
+    expr = sc.make_union(sc.make_input(surfaces["A"]), sc.make_input(surfaces["B"]))
+    r1 = sc.evaluate(expr, ws)
+    p1 = r1.begin.data_ptr()
+    del r1
+    r2 = sc.evaluate(expr, ws)
+    assert r2.begin.data_ptr() == p1
+
+
+def test_interval_set_validation(cuda_device):
+    with pytest.raises(TypeError):
+        sc.IntervalSet(begin=torch.zeros(1, dtype=torch.int64, device="cuda"),
+                       end=torch.zeros(1, dtype=torch.int32, device="cuda"),
+                       row_offsets=torch.tensor([0, 1], dtype=torch.int32, device="cuda"), rows=[0])
+    with pytest.raises(ValueError):
+        sc.build_interval_set(row_offsets=[0, 2], begin=[0], end=[1])
+    with pytest.raises(ValueError):
+        sc.build_interval_set(row_offsets=[0, 1, 1], begin=[0], end=[1], rows=[3, 3])
+
+
+# Fixtures produced by the reference itself
+
+BIN = ["union", "intersection", "difference", "symmetric_difference", "complement"]
+
+
+def _binop(name, a, b):
+    return sc.evaluate(_ops()[name](sc.make_input(a), sc.make_input(b)))
+
+
+def test_config1_setops(cuda_device):
+    g = load("setops.npz")
+    A, B = dev_set(get_set(g, "cfg1/A")), dev_set(get_set(g, "cfg1/B"))
+    for op in BIN:
+        assert_same(_binop(op, A, B), get_set(g, f"cfg1/{op}"), op)
+
+
+def test_fixture_binary_cases(cuda_device):
+    g = load("setops.npz")
+    for c in range(int(g["bin_count"])):
+        A, B = dev_set(get_set(g, f"bin{c}/A")), dev_set(get_set(g, f"bin{c}/B"))
+        for op in BIN:
+            assert_same(_binop(op, A, B), get_set(g, f"bin{c}/{op}"), f"case {c} {op}")
+
+
+EXPRS = {
+    "e0": ("symmetric_difference", ("difference", ("union", "A", "B"), ("intersection", "C", "D")), "E"),
+    "e1": ("union", ("intersection", ("difference", "D", "A"), "B"), ("symmetric_difference", "C", "E")),
+    "e2": ("complement", ("union", "D", "E"), ("intersection", "A", "B")),
+    "e3": ("intersection", ("union", "A", ("intersection", "B", "C")), ("difference", "E", "D")),
+}
+
+
+def _build(spec, leaves):
+    if isinstance(spec, str):
+        return sc.make_input(leaves[spec])
+    return _ops()[spec[0]](_build(spec[1], leaves), _build(spec[2], leaves))
+
+
+def test_fixture_expressions(cuda_device):
+    g = load("setops.npz")
+    for c in range(int(g["expr_count"])):
+        leaves = {n: dev_set(get_set(g, f"expr{c}/{n}")) for n in "ABCDE"}
+        for name, spec in EXPRS.items():
+            assert_same(sc.evaluate(_build(spec, leaves)), get_set(g, f"expr{c}/{name}"), f"expr{c} {name}")
+    leaves = {n: dev_set(get_set(g, f"shape512/{n}")) for n in "ABCDE"}
+    assert_same(sc.evaluate(_build(EXPRS["e0"], leaves)), get_set(g, "shape512/e0"), "shape512")
+
+
+def _random_canonical(rng, rows, width, mean_count, row_ids=None):
+    begins, ends, off = [], [], [0]
+    for _ in range(rows):
+        k = int(rng.poisson(mean_count))
+        x = int(rng.integers(-20, 20))
+        for _ in range(k):
+            x += int(rng.geometric(1 / 6.0))
+            b = x
+            x += int(rng.geometric(1 / 9.0))
+            begins.append(b)
+            ends.append(x)
+        off.append(len(begins))
+    rid = np.arange(rows, dtype=np.int32) if row_ids is None else row_ids
+    return (np.asarray(begins, np.int32), np.asarray(ends, np.int32), np.asarray(off, np.int32), rid)
+
+
+@pytest.mark.parametrize("mean_count", [0.5, 4.0, 40.0, 700.0])
+def test_random_large_vs_oracle(cuda_device, mean_count):
+    rng = np.random.default_rng(int(mean_count * 10))
+    rows = max(4, int(40000 / max(mean_count, 1)))
+    hs = [_random_canonical(rng, rows, 0, mean_count) for _ in range(5)]
+    leaves_h = {n: iset(h) for n, h in zip("ABCDE", hs)}
+    leaves_d = {n: dev_set(h) for n, h in zip("ABCDE", hs)}
+    for name, spec in EXPRS.items():
+        assert_same(sc.evaluate(_build(spec, leaves_d)), O.evaluate(spec, leaves_h), f"{name} m={mean_count}")
+    for op in BIN:
+        assert_same(_binop(op, leaves_d["A"], leaves_d["B"]), O.BINARY[op](leaves_h["A"], leaves_h["B"]), op)
+
+
+def test_sparse_unaligned_rows_vs_oracle(cuda_device):
+    rng = np.random.default_rng(7)
+    hs = []
+    for i in range(5):
+        rid = np.sort(rng.choice(np.arange(-3000, 9000), size=3000, replace=False)).astype(np.int32)
+        hs.append(_random_canonical(rng, rid.size, 0, 3.0, row_ids=rid))
+    leaves_h = {n: iset(h) for n, h in zip("ABCDE", hs)}
+    leaves_d = {n: dev_set(h) for n, h in zip("ABCDE", hs)}
+    for name, spec in EXPRS.items():
+        assert_same(sc.evaluate(_build(spec, leaves_d)), O.evaluate(spec, leaves_h), name)
+
+
+def test_long_rows_take_exact_path(cuda_device):
+    # one row far longer than a fused tile: the exact path must produce the same result
+    rng = np.random.default_rng(11)
+    hs = [_random_canonical(rng, 3, 0, 20000.0) for _ in range(2)]
+    A, B = dev_set(hs[0]), dev_set(hs[1])
+    for op in BIN:
+        assert_same(_binop(op, A, B), O.BINARY[op](iset(hs[0]), iset(hs[1])), op)
+
+
+def test_shapes_4096_expression(cuda_device):
+    ops = synth.shape_operands(4096)
+    leaves_h = {n: iset(h) for n, h in zip("ABCDE", ops)}
+    leaves_d = {n: dev_set(h) for n, h in zip("ABCDE", ops)}
+    assert_same(sc.evaluate(_build(EXPRS["e0"], leaves_d)), O.evaluate(EXPRS["e0"], leaves_h), "shapes4096")
