@@ -105,6 +105,26 @@ int sx_bool_eval(const sx_leaf* leaves /* host array of k */, int k, int32_t row
                  void* stream);
 
 /* ---------------------------------------------------------------------------
+ * sx_bool_eval without a caller workspace.  This entry point has no
+ * counterpart in the reference; it exists for callers that cannot allocate
+ * device memory: a host application that owns the device heap under a fixed
+ * budget and gives plugins no allocator, or a latency-critical loop that
+ * cannot accept the device-wide synchronisation cudaMalloc/cudaFree may
+ * cause.  Inputs and outputs are still the caller's.  The look-back scratch
+ * is a fixed 1 MiB array in this library's device memory, which every GPU
+ * that loads the library holds until the process exits, so rows must not
+ * exceed 3,944,448 (larger inputs fail with SX_ERR_CAPACITY).  Nothing is
+ * allocated and the tuning is automatic.
+ * The first call on each device looks up the array's device address with
+ * that device current; make that first call before any stream capture.
+ * Every call shares the one array and clears the part it uses on its own
+ * stream, so calls that overlap on the GPU race: serialise them.
+ * ------------------------------------------------------------------------- */
+int sx_bool_eval_static(const sx_leaf* leaves /* host array of k */, int k, int32_t rows,
+                        const uint32_t* table /* host, 8 */, int mode, int32_t* out_begin, int32_t* out_end,
+                        int32_t* out_offsets, int64_t capacity, int32_t* result, void* stream);
+
+/* ---------------------------------------------------------------------------
  * Exact reference-order binary operation, one thread per row.
  * Replaces: subsetix_cupy/kernels.py:11-117 (count_segments) when out_begin
  * is NULL, and subsetix_cupy/kernels.py:120-235 (write_segments) otherwise.

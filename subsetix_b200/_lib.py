@@ -54,6 +54,9 @@ _SIGNATURES = {
     "sx_bool_eval": (ctypes.c_int, [ctypes.POINTER(SxLeaf), ctypes.c_int, ctypes.c_int32,
                                     ctypes.POINTER(ctypes.c_uint32), ctypes.c_int, c_vp, c_vp, c_vp, ctypes.c_int64,
                                     c_vp, c_vp, ctypes.c_size_t, ctypes.POINTER(SxTuning), c_vp]),
+    "sx_bool_eval_static": (ctypes.c_int, [ctypes.POINTER(SxLeaf), ctypes.c_int, ctypes.c_int32,
+                                           ctypes.POINTER(ctypes.c_uint32), ctypes.c_int, c_vp, c_vp, c_vp,
+                                           ctypes.c_int64, c_vp, c_vp]),
     "sx_exact_setop": (ctypes.c_int, [ctypes.c_int, ctypes.c_int32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
                                       c_vp, c_vp, c_vp]),
     "sx_merge_rows": (ctypes.c_int, [ctypes.c_int32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),

@@ -208,3 +208,5 @@ int sx_align_rows(const sx_rowlist* lists, int k, int32_t row_min, int32_t row_m
 }
 
 }  // extern "C"
+
+int sx_set_error(int code, const char* msg) { return fail(code, "%s", msg); }

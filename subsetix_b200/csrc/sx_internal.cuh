@@ -68,3 +68,6 @@ cudaError_t sx_exact_setop_launch(int op, int rows, const int* lb, const int* le
 cudaError_t sx_merge_rows_launch(int rows, const int* b, const int* e, const int* off, int* counts, const int* out_off,
                                  int* ob, int* oe, cudaStream_t stream);
 cudaError_t sx_align_launch(SxAlignArgs& A, int out_capacity, const SxScanState& st, cudaStream_t stream);
+
+// Records `msg` as the calling thread's sx_last_error() text and returns `code`.
+int sx_set_error(int code, const char* msg);
