@@ -71,9 +71,9 @@ const char* sx_last_error(void);
  *     l; bit s of table[s >> 5] is f(s); f(0) must be 0).  Output: the
  *     maximal runs of f.
  *   mode SX_MODE_UNION (k <= 9): leaves are widened by `widen` ([b - w, e + w))
- *     and must have non-empty intervals with strictly increasing begins and
- *     ends per row.  Output: the merged union (runs whose next begin is <=
- *     the running end join).
+ *     or coarsened by `scale`, and after that must have non-empty intervals
+ *     whose begins and whose ends are each non-decreasing per row.  Output:
+ *     the merged union (runs whose next begin is <= the running end join).
  * Inputs outside the contract set SX_FLAG_CONTRACT in result[1]; the caller
  * then uses the exact kernels.  Outputs: `out_offsets[rows + 1]`,
  * result = {total, flags}.  A capacity of sum(leaf sizes) always suffices.
@@ -84,8 +84,10 @@ const char* sx_last_error(void);
 typedef struct sx_leaf {
     const int32_t* begin;
     const int32_t* end;
-    const int32_t* row_offsets; /* aligned, rows + 1 entries */
-    int32_t widen;
+    const int32_t* row_offsets; /* aligned, rows + 1 entries: row y = [row_offsets[y], row_offsets[y+1]) */
+    const int32_t* row_ends;    /* optional: row y = [row_offsets[y], row_ends[y]) (rows entries) */
+    int32_t widen;              /* SX_MODE_UNION: intervals read as [b - widen, e + widen) */
+    int32_t scale;              /* SX_MODE_UNION, > 1: intervals read as [floor(b/scale), ceil(e/scale)) */
 } sx_leaf;
 
 /* Launch tuning for sx_bool_eval; NULL or zero fields select automatic values.
@@ -159,21 +161,193 @@ int sx_scan_i32(const int32_t* in, int64_t n, int32_t* out, int32_t* result, voi
  * Replaces: subsetix_cupy/expressions.py:58-141 (_reindex_interval_set,
  * _align_interval_sets) and the row-id construction of dilation,
  * subsetix_cupy/morphology.py:236-247.
- * row_min / row_max bound every (row + shift) that should be kept.
- * result = {number of output rows, flags}.
+ * row_min / row_max bound every (row + shift) that should be kept; the
+ * closing offset aligned[l][R] stops after the last output row, so source
+ * rows past row_max are excluded too.  result = {number of output rows,
+ * flags}.
  * ------------------------------------------------------------------------- */
 typedef struct sx_rowlist {
     const int32_t* rows;
     const int32_t* row_offsets; /* count + 1 entries */
     int32_t count;
-    int32_t shift;
-    int32_t skip_empty;
+    int32_t shift;      /* row v maps to output row floor((v + shift) / div) */
+    int32_t skip_empty; /* rows without intervals produce no output row */
+    int32_t div;        /* >= 1; 0 is read as 1 */
+    int32_t phase;      /* ranges: output row y reads source row y * div + phase - shift */
 } sx_rowlist;
 
 size_t sx_align_workspace_bytes(int32_t row_min, int32_t row_max);
 int sx_align_rows(const sx_rowlist* lists /* host array of k */, int k, int32_t row_min, int32_t row_max,
                   int32_t* rows_out, int32_t out_capacity, int32_t* const* aligned /* host array of k */,
-                  int32_t* result, void* workspace, size_t workspace_bytes, void* stream);
+                  int32_t* const* aligned_ends /* host array of k, may be NULL */, int32_t* result, void* workspace,
+                  size_t workspace_bytes, void* stream);
+/* With aligned_ends[l] set, list l gets explicit ranges instead of
+ * consecutive offsets: aligned[l][y] = start and aligned_ends[l][y] = stop of
+ * source row y * div + phase - shift (empty when that row is absent). */
+
+/* ---------------------------------------------------------------------------
+ * Row shape check.  flags (device int, overwritten) receives the OR of
+ *   SX_ROWS_UNSORTED_BEGIN  a begin is smaller than the previous begin of its row
+ *   SX_ROWS_OVERLAP         an interval starts before the previous one ends
+ *   SX_ROWS_EMPTY           an interval has end <= begin
+ *   SX_ROWS_TOUCH           an interval starts where the previous one ends
+ *   SX_ROWS_UNSORTED_END    an end is smaller than the previous end of its row
+ * No reference counterpart: the reference never checks, and its kernels
+ * follow their own visiting order on such rows.  Callers use the check to
+ * pick between the fast paths and the exact reference-order paths.
+ * ------------------------------------------------------------------------- */
+#define SX_ROWS_UNSORTED_BEGIN 1
+#define SX_ROWS_OVERLAP 2
+#define SX_ROWS_EMPTY 4
+#define SX_ROWS_TOUCH 8
+#define SX_ROWS_UNSORTED_END 16
+int sx_check_rows(const int32_t* begin, const int32_t* end, const int32_t* row_offsets, int32_t rows, int64_t n,
+                  int32_t* flags, void* stream);
+
+/* ---------------------------------------------------------------------------
+ * Interval fields: one value per active cell, stored row by row, with int32
+ * cell offsets per interval (subsetix_cupy/interval_field.py:19-89).
+ * Value types: SX_F32 or SX_F64 (the reference computes in float32 only;
+ * float64 is this library's addition with the same formulas).
+ * ------------------------------------------------------------------------- */
+#define SX_F32 0
+#define SX_F64 1
+
+/* cell_offsets[n + 1] = exclusive prefix sum of end - begin; result = {total
+ * cells, flags}.  Replaces interval_field.py:67-73 (cumsum + .item()).
+ * Workspace: sx_scan_workspace_bytes(n). */
+int sx_cell_offsets(const int32_t* begin, const int32_t* end, int64_t n, int32_t* cell_offsets, int32_t* result,
+                    void* workspace, size_t workspace_bytes, void* stream);
+
+/* Prolongation of a set by `ratio` (>= 2): [b*r, e*r) on rows row*r + 0..r-1
+ * for every occupied row, intervals in input order.
+ * Replaces subsetix_cupy/multilevel.py:213-264 (_prolong_set_impl).
+ * Outputs (capacities rows*ratio, rows*ratio + 1, n*ratio, n*ratio):
+ * rows_out, offsets_out, out_begin, out_end.  result = {occupied input rows,
+ * flags}; the output has result[0] * ratio rows.  result[1] gets
+ * SX_ROWS_UNSORTED_BEGIN when a row's begins decrease; the reference sorts
+ * each output row by begin, so the caller must then sort.
+ * Workspace: sx_prolong_set_workspace_bytes(rows). */
+size_t sx_prolong_set_workspace_bytes(int32_t rows);
+int sx_prolong_set(const int32_t* rows, const int32_t* row_offsets, const int32_t* begin, const int32_t* end,
+                   int32_t row_count, int64_t n, int32_t ratio, int32_t* rows_out, int32_t* offsets_out,
+                   int32_t* out_begin, int32_t* out_end, int32_t* result, void* workspace, size_t workspace_bytes,
+                   void* stream);
+
+/* Piecewise-constant injection of a coarse field onto the fine field of
+ * prolong_set(coarse).  Every coarse row must hold an interval (the
+ * reference raises otherwise).  Coarse interval i, ordinal o in row ordinal
+ * p, maps in sub-row d to fine interval f = fine_row_offsets[p*ratio + d] +
+ * o, and fine cell k of f takes coarse cell k / ratio.
+ * Replaces subsetix_cupy/multilevel.py:365-407 with the kernel of
+ * subsetix_cupy/kernels.py:384-418. */
+int sx_prolong_field(int dtype, const int32_t* coarse_row_offsets, int32_t coarse_rows,
+                     const int32_t* coarse_cell_offsets, int64_t n, const int32_t* fine_row_offsets,
+                     const int32_t* fine_cell_offsets, int32_t ratio, const void* coarse_values, void* fine_values,
+                     void* stream);
+int sx_prolong_field_f32(const int32_t* coarse_row_offsets, int32_t coarse_rows, const int32_t* coarse_cell_offsets,
+                         int64_t n, const int32_t* fine_row_offsets, const int32_t* fine_cell_offsets, int32_t ratio,
+                         const float* coarse_values, float* fine_values, void* stream);
+int sx_prolong_field_f64(const int32_t* coarse_row_offsets, int32_t coarse_rows, const int32_t* coarse_cell_offsets,
+                         int64_t n, const int32_t* fine_row_offsets, const int32_t* fine_cell_offsets, int32_t ratio,
+                         const double* coarse_values, double* fine_values, void* stream);
+
+/* Alignment checks of a fine set against a coarse set for restriction
+ * (subsetix_cupy/multilevel.py:169-210,433-451), in the reference's order.
+ * flags (device int, overwritten): 1 = fine row count != coarse rows *
+ * ratio, 2 = fine rows differ from coarse_row*ratio + dy, 8 = a mapped fine
+ * interval is not [r*b, r*e) of its coarse interval. */
+int sx_coarse_fine_check(const int32_t* coarse_rows, int32_t coarse_row_count, const int32_t* coarse_row_offsets,
+                         const int32_t* coarse_begin, const int32_t* coarse_end, int64_t coarse_n,
+                         const int32_t* fine_rows, int32_t fine_row_count, const int32_t* fine_row_offsets,
+                         const int32_t* fine_begin, const int32_t* fine_end, int64_t fine_n, int32_t ratio,
+                         int32_t* flags, void* stream);
+
+/* ratio x ratio block reduction of a fine field onto a coarse field whose
+ * set is restrict_set(fine set) and which passed sx_coarse_fine_check.
+ * reducer: 0 mean (sum * 1/r^2), 1 sum, 2 min, 3 max; sums run sub-row
+ * outer, column inner, stopping at the fine interval's end.
+ * Replaces subsetix_cupy/multilevel.py:410-479 with the kernel of
+ * subsetix_cupy/kernels.py:458-527. */
+int sx_restrict_field(int dtype, const int32_t* coarse_row_offsets, int32_t coarse_rows,
+                      const int32_t* coarse_cell_offsets, int64_t coarse_n, const int32_t* fine_row_offsets,
+                      const int32_t* fine_cell_offsets, int32_t ratio, int reducer, const void* fine_values,
+                      void* coarse_values, void* stream);
+int sx_restrict_field_f32(const int32_t* coarse_row_offsets, int32_t coarse_rows, const int32_t* coarse_cell_offsets,
+                          int64_t coarse_n, const int32_t* fine_row_offsets, const int32_t* fine_cell_offsets,
+                          int32_t ratio, int reducer, const float* fine_values, float* coarse_values, void* stream);
+int sx_restrict_field_f64(const int32_t* coarse_row_offsets, int32_t coarse_rows, const int32_t* coarse_cell_offsets,
+                          int64_t coarse_n, const int32_t* fine_row_offsets, const int32_t* fine_cell_offsets,
+                          int32_t ratio, int reducer, const double* fine_values, double* coarse_values, void* stream);
+
+/* Subset copies between fields on a subset geometry and a superset geometry
+ * with the same coordinates (subsetix_amr2/fields.py:127-294, K15/K16).
+ * sx_subset_rows: pos[i] = superset row ordinal of subset interval i; flags
+ * (device int, overwritten) = 1 when a subset row is missing from the
+ * superset (fields.py:310-316).  sx_subset_copy: scatter 0 copies superset
+ * -> subset (gather), 1 copies subset -> superset; elem_size 1, 4 or 8
+ * bytes covers bool, int8, int32, float32, int64 and float64. */
+int sx_subset_rows(const int32_t* sub_row_offsets, const int32_t* sub_rows, int32_t sub_row_count, int64_t sub_n,
+                   const int32_t* sup_rows, int32_t sup_row_count, int32_t* pos, int32_t* flags, void* stream);
+int sx_subset_copy(int scatter, int64_t sub_n, const int32_t* pos, const int32_t* sub_begin, const int32_t* sub_end,
+                   const int32_t* sub_cell_offsets, const int32_t* sup_row_offsets, const int32_t* sup_begin,
+                   const int32_t* sup_end, const int32_t* sup_cell_offsets, int32_t sup_row_count, void* sub_values,
+                   void* sup_values, int elem_size, void* stream);
+
+/* First-order upwind step with zero exterior
+ * (subsetix_cupy/interval_stencil.py:16-251, K9):
+ *   out = c - dt * (a * du_dx + b * du_dy)
+ * with the upwind side chosen by the sign of a and b, and cells outside
+ * [0, width) x [0, height) or outside the set reading as 0.
+ * sx_row_lookup fills lookup[height] with the row ordinal of each row id
+ * (-1 when absent) and sets flags (device int, overwritten) to 1 when a
+ * row lies outside [0, height); the reference wraps such rows instead.
+ * direct = 1 is allowed when sx_check_rows reported no UNSORTED_BEGIN,
+ * OVERLAP or EMPTY flag: neighbours inside the cell's own interval are then
+ * read without a search (same results).  row_ids (optional, one per
+ * interval) overrides the row each interval's stencil is taken in, like the
+ * reference's row_ids argument; NULL uses the set's own rows. */
+int sx_row_lookup(const int32_t* rows, int32_t row_count, int32_t height, int32_t* lookup, int32_t* flags,
+                  void* stream);
+int sx_upwind(int dtype, const int32_t* rows, const int32_t* row_ids, const int32_t* row_offsets, int32_t row_count,
+              const int32_t* begin, const int32_t* end, const int32_t* cell_offsets, int64_t n, int64_t cells, const int32_t* lookup,
+              const void* values, void* out, int32_t width, int32_t height, double a, double b, double dt, double dx,
+              double dy, int direct, void* stream);
+int sx_upwind_f32(const int32_t* rows, const int32_t* row_offsets, int32_t row_count, const int32_t* begin,
+                  const int32_t* end, const int32_t* cell_offsets, int64_t n, int64_t cells, const int32_t* lookup,
+                  const float* values, float* out, int32_t width, int32_t height, float a, float b, float dt, float dx,
+                  float dy, int direct, void* stream);
+int sx_upwind_f64(const int32_t* rows, const int32_t* row_offsets, int32_t row_count, const int32_t* begin,
+                  const int32_t* end, const int32_t* cell_offsets, int64_t n, int64_t cells, const int32_t* lookup,
+                  const double* values, double* out, int32_t width, int32_t height, double a, double b, double dt,
+                  double dx, double dy, int direct, void* stream);
+
+/* Threshold run-length encoding of a full width x height float32 grid
+ * (subsetix_amr2/regrid.py:20-124 K11/K12, and regrid.py:172-223 K14 when
+ * gradient = 1): a run is a stretch of value >= threshold, where value is
+ * the grid itself or its gradient magnitude sqrt(gx^2 + gy^2) with central
+ * differences inside and one-sided ones at the borders.  Count pass:
+ * out_begin == NULL, counts[height] written.  Write pass: offsets[height]
+ * (exclusive scan of counts), out_begin/out_end written. */
+int sx_threshold_rle(const float* values, int32_t width, int32_t height, float threshold, int gradient, int32_t* counts,
+                     const int32_t* offsets, int32_t* out_begin, int32_t* out_end, void* stream);
+int sx_gradient_threshold_rle(const float* values, int32_t width, int32_t height, float threshold, int32_t* counts,
+                              const int32_t* offsets, int32_t* out_begin, int32_t* out_end, void* stream);
+
+/* Global interval index holding each (row, col) query, or -1
+ * (subsetix_cupy/interval_field.py:162-297, locate_interval_cells). */
+int sx_locate_cells(const int32_t* rows, const int32_t* row_offsets, const int32_t* begin, const int32_t* end,
+                    int32_t row_count, const int32_t* query_rows, const int32_t* query_cols, int64_t count,
+                    int32_t* out, void* stream);
+
+/* Compensated (Neumaier) FP64 sum of n values times `scale`, in a fixed
+ * order (deterministic).  partials: 2 * parts doubles of scratch, parts in
+ * [1, 4096].  No reference counterpart (the reference has no mass
+ * integral); used for conservation checks. */
+int sx_mass_integral(int dtype, const void* values, int64_t n, double scale, double* partials, int parts, double* out,
+                     void* stream);
+int sx_mass_integral_f64(const double* values, int64_t n, double scale, double* partials, int parts, double* out,
+                         void* stream);
 
 #ifdef __cplusplus
 }

@@ -34,7 +34,8 @@ def bool_eval(leaves: Sequence[Tuple[torch.Tensor, torch.Tensor, torch.Tensor, i
               mode: int, device, out: Optional[Tuple[torch.Tensor, torch.Tensor]] = None):
     """Run the row sweep (sx_bool_eval) and read back its result pair.
 
-    ``leaves`` are ``(begin, end, aligned_offsets, widen)`` tuples; ``mode``
+    ``leaves`` are ``(begin, end, aligned_offsets, widen[, scale[, row_ends]])``
+    tuples; ``mode``
     is ``_lib.MODE_TABLE`` (truth table over canonical leaves) or
     ``_lib.MODE_UNION`` (merged union of widened leaves).  Returns
     ``(begin, end, offsets, total, flags)``; begin and end are capacity
@@ -58,7 +59,7 @@ def bool_eval_async(leaves: Sequence[Tuple[torch.Tensor, torch.Tensor, torch.Ten
     """
     lib = _lib.load()
     k = len(leaves)
-    sizes = [int(b.numel()) for b, _, _, _ in leaves]
+    sizes = [int(leaf[0].numel()) for leaf in leaves]
     cap = max(1, sum(sizes))
     if out is None:
         ob = empty_i32(cap, device)
@@ -74,11 +75,16 @@ def bool_eval_async(leaves: Sequence[Tuple[torch.Tensor, torch.Tensor, torch.Ten
     if result is None:
         result = empty_i32(2, device)
     arr = (_lib.SxLeaf * k)()
-    for i, (b, e, off, widen) in enumerate(leaves):
+    for i, leaf in enumerate(leaves):
+        b, e, off, widen = leaf[:4]
+        scale = leaf[4] if len(leaf) > 4 else 0
+        ends = leaf[5] if len(leaf) > 5 else None
         arr[i].begin = ptr(b)
         arr[i].end = ptr(e)
         arr[i].row_offsets = ptr(off)
+        arr[i].row_ends = ptr(ends)
         arr[i].widen = int(widen)
+        arr[i].scale = int(scale)
     tab = (ctypes.c_uint32 * 8)(*[int(x) & 0xFFFFFFFF for x in (list(table) + [0] * 8)[:8]])
     wsp, wsn = workspace(device, lib.sx_bool_workspace_bytes(int(rows)))
     t = TUNING if tuning is None else tuning
@@ -145,36 +151,210 @@ def merge_rows(begin: torch.Tensor, end: torch.Tensor, offsets: torch.Tensor, de
     return ob, oe, off
 
 
-def align_rows(lists: Sequence[Tuple[torch.Tensor, torch.Tensor, int, bool]], row_min: int, row_max: int, device,
-               want_offsets: Sequence[bool]) -> Tuple[torch.Tensor, List[Optional[torch.Tensor]]]:
-    """Sorted union of ``rows + shift`` over the lists, plus aligned offsets.
+def align_rows(lists: Sequence[tuple], row_min: int, row_max: int, device, want_offsets: Sequence[bool],
+               want_ends: Optional[Sequence[bool]] = None):
+    """Sorted union of ``floor((rows + shift) / div)`` over the lists, plus aligned offsets.
 
-    ``lists`` holds ``(rows, offsets, shift, skip_empty)`` tuples.  Returns
-    ``(rows_out, [aligned offsets or None])``.  This call synchronises.
+    ``lists`` holds ``(rows, offsets, shift, skip_empty[, div, phase])``
+    tuples.  Returns ``(rows_out, [aligned offsets or None])``, or with
+    ``want_ends`` ``(rows_out, [starts or None], [stops or None])``.  This
+    call synchronises.
     """
     lib = _lib.load()
     k = len(lists)
     cap = 0
-    for rows, _, _, _ in lists:
-        cap += int(rows.numel())
+    for item in lists:
+        cap += int(item[0].numel())
     span = int(row_max) - int(row_min) + 1
     cap = max(1, min(cap, max(span, 1)))
     rows_out = empty_i32(cap, device)
     aligned = [empty_i32(cap + 1, device) if w else None for w in want_offsets]
+    ends = [empty_i32(cap, device) if w else None for w in (want_ends or [False] * k)]
     arr = (_lib.SxRowList * k)()
-    for i, (rows, off, shift, skip) in enumerate(lists):
+    for i, item in enumerate(lists):
+        rows, off, shift, skip = item[:4]
         arr[i].rows = ptr(rows)
         arr[i].row_offsets = ptr(off)
         arr[i].count = int(rows.numel())
         arr[i].shift = int(shift)
         arr[i].skip_empty = 1 if skip else 0
+        arr[i].div = int(item[4]) if len(item) > 4 else 1
+        arr[i].phase = int(item[5]) if len(item) > 5 else 0
     aptrs = (ctypes.c_void_p * k)(*[ptr(a) if a is not None else None for a in aligned])
+    eptrs = (ctypes.c_void_p * k)(*[ptr(a) if a is not None else None for a in ends])
     result = empty_i32(2, device)
     wsp, wsn = workspace(device, lib.sx_align_workspace_bytes(int(row_min), int(row_max)))
-    rc = lib.sx_align_rows(arr, k, int(row_min), int(row_max), ptr(rows_out), cap, aptrs, ptr(result), wsp, wsn,
-                           stream_handle(device))
+    rc = lib.sx_align_rows(arr, k, int(row_min), int(row_max), ptr(rows_out), cap, aptrs,
+                           eptrs if want_ends else None, ptr(result), wsp, wsn, stream_handle(device))
     _lib.check(rc, "sx_align_rows")
     n, flags = read_pair(result)
     if flags & _lib.FLAG_TIMEOUT:
         raise _lib.SubsetixError("sx_align_rows: look-back wait timed out")
-    return rows_out[:n], [a[: n + 1] if a is not None else None for a in aligned]
+    starts = [a[: n + 1] if a is not None else None for a in aligned]
+    if want_ends:
+        return rows_out[:n], starts, [a[:n] if a is not None else None for a in ends]
+    return rows_out[:n], starts
+
+
+# ---------------------------------------------------------------------------
+# Interval fields and multilevel kernels
+# ---------------------------------------------------------------------------
+
+def _flag_word(device) -> torch.Tensor:
+    return empty_i32(1, device)
+
+
+def check_rows(begin: torch.Tensor, end: torch.Tensor, offsets: torch.Tensor, device, sync: bool = True):
+    """OR of ``_lib.ROWS_*`` bits over adjacent interval pairs (sx_check_rows)."""
+    lib = _lib.load()
+    flags = _flag_word(device)
+    rows = int(offsets.numel()) - 1
+    _lib.check(lib.sx_check_rows(ptr(begin), ptr(end), ptr(offsets), max(rows, 0), int(begin.numel()), ptr(flags),
+                                 stream_handle(device)), "sx_check_rows")
+    return int(flags.item()) if sync else flags
+
+
+def cell_offsets(begin: torch.Tensor, end: torch.Tensor, device, sync: bool = True):
+    """int32 exclusive scan of interval lengths.  Returns ``(offsets, total)``."""
+    lib = _lib.load()
+    n = int(begin.numel())
+    out = empty_i32(n + 1, device)
+    result = empty_i32(2, device)
+    wsp, wsn = workspace(device, lib.sx_scan_workspace_bytes(n))
+    _lib.check(lib.sx_cell_offsets(ptr(begin), ptr(end), n, ptr(out), ptr(result), wsp, wsn, stream_handle(device)),
+               "sx_cell_offsets")
+    if not sync:
+        return out, result
+    total, flags = read_pair(result)
+    if flags & _lib.FLAG_TIMEOUT:
+        raise _lib.SubsetixError("sx_cell_offsets: look-back wait timed out")
+    return out, total
+
+
+def prolong_set(rows: torch.Tensor, offsets: torch.Tensor, begin: torch.Tensor, end: torch.Tensor, ratio: int,
+                device):
+    """sx_prolong_set.  Returns ``(rows_out, offsets_out, begin, end, unsorted)`` sized to the output."""
+    lib = _lib.load()
+    R = int(rows.numel())
+    n = int(begin.numel())
+    rows_out = empty_i32(R * ratio, device)
+    off_out = empty_i32(R * ratio + 1, device)
+    ob = empty_i32(n * ratio, device)
+    oe = empty_i32(n * ratio, device)
+    result = empty_i32(2, device)
+    wsp, wsn = workspace(device, lib.sx_prolong_set_workspace_bytes(R))
+    _lib.check(lib.sx_prolong_set(ptr(rows), ptr(offsets), ptr(begin), ptr(end), R, n, int(ratio), ptr(rows_out),
+                                  ptr(off_out), ptr(ob), ptr(oe), ptr(result), wsp, wsn, stream_handle(device)),
+               "sx_prolong_set")
+    occupied, flags = read_pair(result)
+    if flags & _lib.FLAG_TIMEOUT:
+        raise _lib.SubsetixError("sx_prolong_set: look-back wait timed out")
+    m = occupied * ratio
+    return rows_out[:m], off_out[: m + 1], ob, oe, bool(flags & 1)
+
+
+def _dtype_code(t: torch.Tensor) -> int:
+    if t.dtype == torch.float32:
+        return _lib.SX_F32
+    if t.dtype == torch.float64:
+        return _lib.SX_F64
+    raise TypeError(f"field values must be float32 or float64, got {t.dtype}")
+
+
+def prolong_field(coarse_offsets, coarse_cell_offsets, n: int, fine_offsets, fine_cell_offsets, ratio: int,
+                  coarse_values, fine_values, device):
+    lib = _lib.load()
+    rows = int(coarse_offsets.numel()) - 1
+    _lib.check(lib.sx_prolong_field(_dtype_code(coarse_values), ptr(coarse_offsets), rows, ptr(coarse_cell_offsets),
+                                    int(n), ptr(fine_offsets), ptr(fine_cell_offsets), int(ratio), ptr(coarse_values),
+                                    ptr(fine_values), stream_handle(device)), "sx_prolong_field")
+
+
+def coarse_fine_check(coarse, fine, ratio: int, device, sync: bool = True):
+    """Flags of sx_coarse_fine_check.  ``coarse``/``fine`` are ``(rows, offsets, begin, end)``."""
+    lib = _lib.load()
+    cr, coff, cb, ce = coarse
+    fr, foff, fb, fe = fine
+    flags = _flag_word(device)
+    _lib.check(lib.sx_coarse_fine_check(ptr(cr), int(cr.numel()), ptr(coff), ptr(cb), ptr(ce), int(cb.numel()),
+                                        ptr(fr), int(fr.numel()), ptr(foff), ptr(fb), ptr(fe), int(fb.numel()),
+                                        int(ratio), ptr(flags), stream_handle(device)), "sx_coarse_fine_check")
+    return int(flags.item()) if sync else flags
+
+
+def restrict_field(coarse_offsets, coarse_cell_offsets, coarse_n: int, fine_offsets, fine_cell_offsets, ratio: int,
+                   reducer: int, fine_values, coarse_values, device):
+    lib = _lib.load()
+    rows = int(coarse_offsets.numel()) - 1
+    _lib.check(lib.sx_restrict_field(_dtype_code(fine_values), ptr(coarse_offsets), rows, ptr(coarse_cell_offsets),
+                                     int(coarse_n), ptr(fine_offsets), ptr(fine_cell_offsets), int(ratio),
+                                     int(reducer), ptr(fine_values), ptr(coarse_values), stream_handle(device)),
+               "sx_restrict_field")
+
+
+def subset_rows(sub_offsets, sub_rows, sub_n: int, sup_rows, device, sync: bool = True):
+    """Superset row ordinal per subset interval.  Returns ``(pos, missing)``."""
+    lib = _lib.load()
+    pos = empty_i32(sub_n, device)
+    flags = _flag_word(device)
+    _lib.check(lib.sx_subset_rows(ptr(sub_offsets), ptr(sub_rows), int(sub_rows.numel()), int(sub_n), ptr(sup_rows),
+                                  int(sup_rows.numel()), ptr(pos), ptr(flags), stream_handle(device)),
+               "sx_subset_rows")
+    return pos, (bool(flags.item()) if sync else flags)
+
+
+def subset_copy(scatter: bool, pos, sub, sup, sub_values, sup_values, device):
+    """sx_subset_copy.  ``sub`` = ``(begin, end, cell_offsets)``; ``sup`` = ``(offsets, begin, end, cell_offsets)``."""
+    lib = _lib.load()
+    sb, se, scoff = sub
+    uoff, ub, ue, ucoff = sup
+    _lib.check(lib.sx_subset_copy(1 if scatter else 0, int(sb.numel()), ptr(pos), ptr(sb), ptr(se), ptr(scoff),
+                                  ptr(uoff), ptr(ub), ptr(ue), ptr(ucoff), int(uoff.numel()) - 1, ptr(sub_values),
+                                  ptr(sup_values), int(sub_values.element_size()), stream_handle(device)),
+               "sx_subset_copy")
+
+
+def row_lookup(rows, height: int, device, sync: bool = True):
+    """Row ordinal per row id in [0, height) (-1 when absent).  Returns ``(lookup, out_of_range)``."""
+    lib = _lib.load()
+    lookup = empty_i32(height, device)
+    flags = _flag_word(device)
+    _lib.check(lib.sx_row_lookup(ptr(rows), int(rows.numel()), int(height), ptr(lookup), ptr(flags),
+                                 stream_handle(device)), "sx_row_lookup")
+    return lookup, (bool(flags.item()) if sync else flags)
+
+
+def upwind(rows, offsets, begin, end, cell_offs, cells: int, lookup, values, out, width: int, height: int, a, b, dt,
+           dx, dy, direct: bool, device, row_ids=None):
+    lib = _lib.load()
+    _lib.check(lib.sx_upwind(_dtype_code(values), ptr(rows), ptr(row_ids), ptr(offsets), int(rows.numel()), ptr(begin),
+                             ptr(end), ptr(cell_offs), int(begin.numel()), int(cells), ptr(lookup), ptr(values),
+                             ptr(out), int(width), int(height), float(a), float(b), float(dt), float(dx), float(dy),
+                             1 if direct else 0, stream_handle(device)), "sx_upwind")
+
+
+def threshold_rle(values, width: int, height: int, threshold: float, gradient: bool, device):
+    """Runs of value >= threshold per row of a full grid.  Returns ``(begin, end, offsets)`` (synchronising)."""
+    lib = _lib.load()
+    counts = empty_i32(height, device)
+    s = stream_handle(device)
+    _lib.check(lib.sx_threshold_rle(ptr(values), int(width), int(height), float(threshold), 1 if gradient else 0,
+                                    ptr(counts), None, None, None, s), "sx_threshold_rle(count)")
+    off, total = scan(counts, device)
+    ob = empty_i32(total, device)
+    oe = empty_i32(total, device)
+    if total:
+        _lib.check(lib.sx_threshold_rle(ptr(values), int(width), int(height), float(threshold), 1 if gradient else 0,
+                                        None, ptr(off), ptr(ob), ptr(oe), s), "sx_threshold_rle(write)")
+    return ob, oe, off
+
+
+def mass_integral(values, scale: float, device, out: Optional[torch.Tensor] = None, parts: int = 592):
+    """Compensated FP64 sum times ``scale`` into a device scalar (no synchronisation)."""
+    lib = _lib.load()
+    if out is None:
+        out = torch.empty(1, dtype=torch.float64, device=device)
+    part = torch.empty(2 * parts, dtype=torch.float64, device=device)
+    _lib.check(lib.sx_mass_integral(_dtype_code(values), ptr(values), int(values.numel()), float(scale), ptr(part),
+                                    int(parts), ptr(out), stream_handle(device)), "sx_mass_integral")
+    return out

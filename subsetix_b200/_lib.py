@@ -34,7 +34,8 @@ c_vp = ctypes.c_void_p
 
 
 class SxLeaf(ctypes.Structure):
-    _fields_ = [("begin", c_vp), ("end", c_vp), ("row_offsets", c_vp), ("widen", ctypes.c_int32)]
+    _fields_ = [("begin", c_vp), ("end", c_vp), ("row_offsets", c_vp), ("row_ends", c_vp), ("widen", ctypes.c_int32),
+                ("scale", ctypes.c_int32)]
 
 
 class SxTuning(ctypes.Structure):
@@ -43,7 +44,7 @@ class SxTuning(ctypes.Structure):
 
 class SxRowList(ctypes.Structure):
     _fields_ = [("rows", c_vp), ("row_offsets", c_vp), ("count", ctypes.c_int32), ("shift", ctypes.c_int32),
-                ("skip_empty", ctypes.c_int32)]
+                ("skip_empty", ctypes.c_int32), ("div", ctypes.c_int32), ("phase", ctypes.c_int32)]
 
 
 # name -> (restype, argtypes)
@@ -64,8 +65,63 @@ _SIGNATURES = {
     "sx_scan_i32": (ctypes.c_int, [c_vp, ctypes.c_int64, c_vp, c_vp, c_vp, ctypes.c_size_t, c_vp]),
     "sx_align_workspace_bytes": (ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32]),
     "sx_align_rows": (ctypes.c_int, [ctypes.POINTER(SxRowList), ctypes.c_int, ctypes.c_int32, ctypes.c_int32, c_vp,
-                                     ctypes.c_int32, ctypes.POINTER(c_vp), c_vp, c_vp, ctypes.c_size_t, c_vp]),
+                                     ctypes.c_int32, ctypes.POINTER(c_vp), ctypes.POINTER(c_vp), c_vp, c_vp,
+                                     ctypes.c_size_t, c_vp]),
+    "sx_check_rows": (ctypes.c_int, [c_vp, c_vp, c_vp, ctypes.c_int32, ctypes.c_int64, c_vp, c_vp]),
+    "sx_cell_offsets": (ctypes.c_int, [c_vp, c_vp, ctypes.c_int64, c_vp, c_vp, c_vp, ctypes.c_size_t, c_vp]),
+    "sx_prolong_set_workspace_bytes": (ctypes.c_size_t, [ctypes.c_int32]),
+    "sx_prolong_set": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, ctypes.c_int32, ctypes.c_int64, ctypes.c_int32, c_vp,
+                                      c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.c_size_t, c_vp]),
+    "sx_prolong_field": (ctypes.c_int, [ctypes.c_int, c_vp, ctypes.c_int32, c_vp, ctypes.c_int64, c_vp, c_vp,
+                                        ctypes.c_int32, c_vp, c_vp, c_vp]),
+    "sx_prolong_field_f32": (ctypes.c_int, [c_vp, ctypes.c_int32, c_vp, ctypes.c_int64, c_vp, c_vp, ctypes.c_int32,
+                                            c_vp, c_vp, c_vp]),
+    "sx_prolong_field_f64": (ctypes.c_int, [c_vp, ctypes.c_int32, c_vp, ctypes.c_int64, c_vp, c_vp, ctypes.c_int32,
+                                            c_vp, c_vp, c_vp]),
+    "sx_coarse_fine_check": (ctypes.c_int, [c_vp, ctypes.c_int32, c_vp, c_vp, c_vp, ctypes.c_int64, c_vp,
+                                            ctypes.c_int32, c_vp, c_vp, c_vp, ctypes.c_int64, ctypes.c_int32, c_vp,
+                                            c_vp]),
+    "sx_restrict_field": (ctypes.c_int, [ctypes.c_int, c_vp, ctypes.c_int32, c_vp, ctypes.c_int64, c_vp, c_vp,
+                                         ctypes.c_int32, ctypes.c_int, c_vp, c_vp, c_vp]),
+    "sx_restrict_field_f32": (ctypes.c_int, [c_vp, ctypes.c_int32, c_vp, ctypes.c_int64, c_vp, c_vp, ctypes.c_int32,
+                                             ctypes.c_int, c_vp, c_vp, c_vp]),
+    "sx_restrict_field_f64": (ctypes.c_int, [c_vp, ctypes.c_int32, c_vp, ctypes.c_int64, c_vp, c_vp, ctypes.c_int32,
+                                             ctypes.c_int, c_vp, c_vp, c_vp]),
+    "sx_subset_rows": (ctypes.c_int, [c_vp, c_vp, ctypes.c_int32, ctypes.c_int64, c_vp, ctypes.c_int32, c_vp, c_vp,
+                                      c_vp]),
+    "sx_subset_copy": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
+                                      ctypes.c_int32, c_vp, c_vp, ctypes.c_int, c_vp]),
+    "sx_row_lookup": (ctypes.c_int, [c_vp, ctypes.c_int32, ctypes.c_int32, c_vp, c_vp, c_vp]),
+    "sx_upwind": (ctypes.c_int, [ctypes.c_int, c_vp, c_vp, c_vp, ctypes.c_int32, c_vp, c_vp, c_vp, ctypes.c_int64,
+                                 ctypes.c_int64, c_vp, c_vp, c_vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
+                                 ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                 c_vp]),
+    "sx_upwind_f32": (ctypes.c_int, [c_vp, c_vp, ctypes.c_int32, c_vp, c_vp, c_vp, ctypes.c_int64, ctypes.c_int64,
+                                     c_vp, c_vp, c_vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_float, ctypes.c_float,
+                                     ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_int, c_vp]),
+    "sx_upwind_f64": (ctypes.c_int, [c_vp, c_vp, ctypes.c_int32, c_vp, c_vp, c_vp, ctypes.c_int64, ctypes.c_int64,
+                                     c_vp, c_vp, c_vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
+                                     ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                     c_vp]),
+    "sx_threshold_rle": (ctypes.c_int, [c_vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_float, ctypes.c_int, c_vp,
+                                        c_vp, c_vp, c_vp, c_vp]),
+    "sx_gradient_threshold_rle": (ctypes.c_int, [c_vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_float, c_vp, c_vp,
+                                                 c_vp, c_vp, c_vp]),
+    "sx_locate_cells": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, ctypes.c_int32, c_vp, c_vp, ctypes.c_int64, c_vp,
+                                       c_vp]),
+    "sx_mass_integral": (ctypes.c_int, [ctypes.c_int, c_vp, ctypes.c_int64, ctypes.c_double, c_vp, ctypes.c_int, c_vp,
+                                        c_vp]),
+    "sx_mass_integral_f64": (ctypes.c_int, [c_vp, ctypes.c_int64, ctypes.c_double, c_vp, ctypes.c_int, c_vp, c_vp]),
 }
+
+SX_F32 = 0
+SX_F64 = 1
+
+ROWS_UNSORTED_BEGIN = 1
+ROWS_OVERLAP = 2
+ROWS_EMPTY = 4
+ROWS_TOUCH = 8
+ROWS_UNSORTED_END = 16
 
 _lock = threading.Lock()
 _lib = None

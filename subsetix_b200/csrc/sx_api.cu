@@ -3,6 +3,7 @@
 
 #include <cstdarg>
 #include <cstdio>
+#include <climits>
 #include <cstring>
 
 #include "../../include/subsetix_b200.h"
@@ -78,6 +79,10 @@ int sx_bool_eval(const sx_leaf* leaves, int k, int32_t rows, const uint32_t* tab
         A.leaf[l].end = leaves[l].end;
         A.leaf[l].off = leaves[l].row_offsets;
         A.leaf[l].widen = mode == SX_MODE_UNION ? leaves[l].widen : 0;
+        A.leaf[l].scale = mode == SX_MODE_UNION ? leaves[l].scale : 0;
+        A.leaf[l].off_end = leaves[l].row_ends;
+        if (leaves[l].row_ends && mode != SX_MODE_UNION)
+            return fail(SX_ERR_INVALID, "sx_bool_eval: row_ends is only supported in SX_MODE_UNION");
     }
     A.k = k;
     A.rows = rows;
@@ -157,7 +162,8 @@ size_t sx_align_workspace_bytes(int32_t row_min, int32_t row_max)
 }
 
 int sx_align_rows(const sx_rowlist* lists, int k, int32_t row_min, int32_t row_max, int32_t* rows_out,
-                  int32_t out_capacity, int32_t* const* aligned, int32_t* result, void* workspace,
+                  int32_t out_capacity, int32_t* const* aligned, int32_t* const* aligned_ends, int32_t* result,
+                  void* workspace,
                   size_t workspace_bytes, void* stream)
 {
     if (k < 1 || k > 2 * SX_MAX_LEAVES) return fail(SX_ERR_INVALID, "sx_align_rows: k=%d outside [1, %d]", k,
@@ -176,6 +182,11 @@ int sx_align_rows(const sx_rowlist* lists, int k, int32_t row_min, int32_t row_m
         A.list[l].count = lists[l].count;
         A.list[l].shift = lists[l].shift;
         A.list[l].skip_empty = lists[l].skip_empty;
+        A.list[l].div = lists[l].div > 1 ? lists[l].div : 1;
+        A.list[l].phase = lists[l].phase;
+        A.aligned_end[l] = aligned_ends ? aligned_ends[l] : nullptr;
+        if (A.aligned_end[l] && !lists[l].row_offsets)
+            return fail(SX_ERR_INVALID, "sx_align_rows: list %d needs row offsets for ranges", l);
         if (lists[l].count < 0) return fail(SX_ERR_INVALID, "sx_align_rows: negative count");
         if (lists[l].count > 0 && !lists[l].rows) return fail(SX_ERR_INVALID, "sx_align_rows: null rows");
         if ((lists[l].skip_empty || (aligned && aligned[l])) && !lists[l].row_offsets)
@@ -205,6 +216,302 @@ int sx_align_rows(const sx_rowlist* lists, int k, int32_t row_min, int32_t row_m
     cudaError_t err = sx_align_launch(A, out_capacity, st, (cudaStream_t)stream);
     if (err != cudaSuccess) return cuda_fail(err, "sx_align_rows");
     return SX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Interval fields
+// ---------------------------------------------------------------------------
+
+int sx_check_rows(const int32_t* begin, const int32_t* end, const int32_t* row_offsets, int32_t rows, int64_t n,
+                  int32_t* flags, void* stream)
+{
+    if (rows < 0 || n < 0) return fail(SX_ERR_INVALID, "sx_check_rows: negative size");
+    if (!flags || (n > 0 && (!begin || !end || !row_offsets))) return fail(SX_ERR_INVALID, "sx_check_rows: null argument");
+    if (n > INT32_MAX) return fail(SX_ERR_INVALID, "sx_check_rows: more than 2^31-1 intervals");
+    cudaError_t err = sx_check_rows_launch(begin, end, row_offsets, rows, n, flags, (cudaStream_t)stream);
+    if (err != cudaSuccess) return cuda_fail(err, "sx_check_rows");
+    return SX_OK;
+}
+
+int sx_cell_offsets(const int32_t* begin, const int32_t* end, int64_t n, int32_t* cell_offsets, int32_t* result,
+                    void* workspace, size_t workspace_bytes, void* stream)
+{
+    if (n < 0 || n > INT32_MAX) return fail(SX_ERR_INVALID, "sx_cell_offsets: interval count out of range");
+    if (!cell_offsets || !result || (n > 0 && (!begin || !end))) return fail(SX_ERR_INVALID, "sx_cell_offsets: null argument");
+    const long long tiles = sx_scan_tiles(n);
+    if (!workspace || workspace_bytes < scan_state_bytes(tiles))
+        return fail(SX_ERR_WORKSPACE, "sx_cell_offsets: workspace needs %zu bytes", scan_state_bytes(tiles));
+    cudaError_t err = sx_cell_offsets_launch(begin, end, n, cell_offsets, result, scan_state(workspace, tiles),
+                                             (cudaStream_t)stream);
+    if (err != cudaSuccess) return cuda_fail(err, "sx_cell_offsets");
+    return SX_OK;
+}
+
+size_t sx_prolong_set_workspace_bytes(int32_t rows)
+{
+    const long long r = rows < 1 ? 1 : rows;
+    return scan_state_bytes(sx_scan_tiles(r)) + align256((size_t)r * 4) + align256((size_t)(r + 1) * 4);
+}
+
+int sx_prolong_set(const int32_t* rows, const int32_t* row_offsets, const int32_t* begin, const int32_t* end,
+                   int32_t row_count, int64_t n, int32_t ratio, int32_t* rows_out, int32_t* offsets_out,
+                   int32_t* out_begin, int32_t* out_end, int32_t* result, void* workspace, size_t workspace_bytes,
+                   void* stream)
+{
+    if (ratio < 2) return fail(SX_ERR_INVALID, "sx_prolong_set: ratio must be >= 2 (ratio 1 is the identity)");
+    if (row_count < 0 || n < 0) return fail(SX_ERR_INVALID, "sx_prolong_set: negative size");
+    if ((long long)row_count * ratio + 1 > INT32_MAX || n * ratio > INT32_MAX)
+        return fail(SX_ERR_INVALID, "sx_prolong_set: output exceeds int32 indexing");
+    if (!result || !offsets_out) return fail(SX_ERR_INVALID, "sx_prolong_set: null argument");
+    if (row_count == 0) return SX_OK;
+    if (!rows || !row_offsets || !rows_out || (n > 0 && (!begin || !end || !out_begin || !out_end)))
+        return fail(SX_ERR_INVALID, "sx_prolong_set: null argument");
+    if (!workspace || workspace_bytes < sx_prolong_set_workspace_bytes(row_count))
+        return fail(SX_ERR_WORKSPACE, "sx_prolong_set: workspace needs %zu bytes",
+                    sx_prolong_set_workspace_bytes(row_count));
+    const long long tiles = sx_scan_tiles(row_count);
+    char* p = (char*)workspace;
+    SxScanState st = scan_state(p, tiles);
+    p += scan_state_bytes(tiles);
+    int* occupied = (int*)p;
+    p += align256((size_t)row_count * 4);
+    int* ord = (int*)p;
+    cudaError_t err = sx_prolong_set_launch(rows, row_offsets, begin, end, row_count, (int)n, ratio, occupied, ord,
+                                            result, st, rows_out, offsets_out, out_begin, out_end,
+                                            (cudaStream_t)stream);
+    if (err != cudaSuccess) return cuda_fail(err, "sx_prolong_set");
+    return SX_OK;
+}
+
+int sx_prolong_field(int dtype, const int32_t* coarse_row_offsets, int32_t coarse_rows,
+                     const int32_t* coarse_cell_offsets, int64_t n, const int32_t* fine_row_offsets,
+                     const int32_t* fine_cell_offsets, int32_t ratio, const void* coarse_values, void* fine_values,
+                     void* stream)
+{
+    if (dtype != SX_F32 && dtype != SX_F64) return fail(SX_ERR_INVALID, "sx_prolong_field: dtype %d", dtype);
+    if (ratio < 1) return fail(SX_ERR_INVALID, "sx_prolong_field: ratio must be >= 1");
+    if (coarse_rows < 0 || n < 0 || n > INT32_MAX || (long long)coarse_rows * ratio > INT32_MAX)
+        return fail(SX_ERR_INVALID, "sx_prolong_field: bad size");
+    if (n == 0 || coarse_rows == 0) return SX_OK;
+    if (!coarse_row_offsets || !coarse_cell_offsets || !fine_row_offsets || !fine_cell_offsets || !coarse_values ||
+        !fine_values)
+        return fail(SX_ERR_INVALID, "sx_prolong_field: null argument");
+    cudaError_t err = sx_prolong_field_launch(coarse_row_offsets, coarse_rows, coarse_cell_offsets, (int)n,
+                                              fine_row_offsets, fine_cell_offsets, ratio, coarse_values, fine_values,
+                                              dtype == SX_F64, (cudaStream_t)stream);
+    if (err != cudaSuccess) return cuda_fail(err, "sx_prolong_field");
+    return SX_OK;
+}
+
+int sx_prolong_field_f32(const int32_t* coarse_row_offsets, int32_t coarse_rows, const int32_t* coarse_cell_offsets,
+                         int64_t n, const int32_t* fine_row_offsets, const int32_t* fine_cell_offsets, int32_t ratio,
+                         const float* coarse_values, float* fine_values, void* stream)
+{
+    return sx_prolong_field(SX_F32, coarse_row_offsets, coarse_rows, coarse_cell_offsets, n, fine_row_offsets,
+                            fine_cell_offsets, ratio, coarse_values, fine_values, stream);
+}
+
+int sx_prolong_field_f64(const int32_t* coarse_row_offsets, int32_t coarse_rows, const int32_t* coarse_cell_offsets,
+                         int64_t n, const int32_t* fine_row_offsets, const int32_t* fine_cell_offsets, int32_t ratio,
+                         const double* coarse_values, double* fine_values, void* stream)
+{
+    return sx_prolong_field(SX_F64, coarse_row_offsets, coarse_rows, coarse_cell_offsets, n, fine_row_offsets,
+                            fine_cell_offsets, ratio, coarse_values, fine_values, stream);
+}
+
+int sx_coarse_fine_check(const int32_t* coarse_rows, int32_t coarse_row_count, const int32_t* coarse_row_offsets,
+                         const int32_t* coarse_begin, const int32_t* coarse_end, int64_t coarse_n,
+                         const int32_t* fine_rows, int32_t fine_row_count, const int32_t* fine_row_offsets,
+                         const int32_t* fine_begin, const int32_t* fine_end, int64_t fine_n, int32_t ratio,
+                         int32_t* flags, void* stream)
+{
+    if (ratio < 1) return fail(SX_ERR_INVALID, "sx_coarse_fine_check: ratio must be >= 1");
+    if (coarse_row_count < 0 || fine_row_count < 0 || coarse_n < 0 || fine_n < 0 || coarse_n > INT32_MAX ||
+        fine_n > INT32_MAX || (long long)coarse_row_count * ratio > INT32_MAX)
+        return fail(SX_ERR_INVALID, "sx_coarse_fine_check: bad size");
+    if (!flags) return fail(SX_ERR_INVALID, "sx_coarse_fine_check: null flags");
+    cudaError_t err = cudaMemsetAsync(flags, 0, sizeof(int32_t), (cudaStream_t)stream);
+    if (err != cudaSuccess) return cuda_fail(err, "sx_coarse_fine_check");
+    if (coarse_row_count == 0 && fine_row_count == 0) return SX_OK;
+    err = sx_restrict_check_launch(coarse_rows, coarse_row_count, coarse_row_offsets, coarse_begin, coarse_end,
+                                   (int)coarse_n, fine_rows, fine_row_count, fine_row_offsets, fine_begin, fine_end,
+                                   (int)fine_n, ratio, flags, (cudaStream_t)stream);
+    if (err != cudaSuccess) return cuda_fail(err, "sx_coarse_fine_check");
+    return SX_OK;
+}
+
+int sx_restrict_field(int dtype, const int32_t* coarse_row_offsets, int32_t coarse_rows,
+                      const int32_t* coarse_cell_offsets, int64_t coarse_n, const int32_t* fine_row_offsets,
+                      const int32_t* fine_cell_offsets, int32_t ratio, int reducer, const void* fine_values,
+                      void* coarse_values, void* stream)
+{
+    if (dtype != SX_F32 && dtype != SX_F64) return fail(SX_ERR_INVALID, "sx_restrict_field: dtype %d", dtype);
+    if (ratio < 1) return fail(SX_ERR_INVALID, "sx_restrict_field: ratio must be >= 1");
+    if (reducer < 0 || reducer > 3) return fail(SX_ERR_INVALID, "sx_restrict_field: reducer %d", reducer);
+    if (coarse_rows < 0 || coarse_n < 0 || coarse_n > INT32_MAX) return fail(SX_ERR_INVALID, "sx_restrict_field: bad size");
+    if (coarse_n == 0 || coarse_rows == 0) return SX_OK;
+    if (!coarse_row_offsets || !coarse_cell_offsets || !fine_row_offsets || !fine_cell_offsets || !fine_values ||
+        !coarse_values)
+        return fail(SX_ERR_INVALID, "sx_restrict_field: null argument");
+    // norm = 1 / r^2 rounded once to the value type, as the reference computes it
+    const double norm = reducer == 0 ? 1.0 / ((double)ratio * ratio) : 1.0;
+    cudaError_t err = sx_restrict_field_launch(coarse_row_offsets, coarse_rows, coarse_cell_offsets, (int)coarse_n,
+                                               fine_row_offsets, fine_cell_offsets, ratio, reducer, norm, fine_values,
+                                               coarse_values, dtype == SX_F64, (cudaStream_t)stream);
+    if (err != cudaSuccess) return cuda_fail(err, "sx_restrict_field");
+    return SX_OK;
+}
+
+int sx_restrict_field_f32(const int32_t* coarse_row_offsets, int32_t coarse_rows, const int32_t* coarse_cell_offsets,
+                          int64_t coarse_n, const int32_t* fine_row_offsets, const int32_t* fine_cell_offsets,
+                          int32_t ratio, int reducer, const float* fine_values, float* coarse_values, void* stream)
+{
+    return sx_restrict_field(SX_F32, coarse_row_offsets, coarse_rows, coarse_cell_offsets, coarse_n, fine_row_offsets,
+                             fine_cell_offsets, ratio, reducer, fine_values, coarse_values, stream);
+}
+
+int sx_restrict_field_f64(const int32_t* coarse_row_offsets, int32_t coarse_rows, const int32_t* coarse_cell_offsets,
+                          int64_t coarse_n, const int32_t* fine_row_offsets, const int32_t* fine_cell_offsets,
+                          int32_t ratio, int reducer, const double* fine_values, double* coarse_values, void* stream)
+{
+    return sx_restrict_field(SX_F64, coarse_row_offsets, coarse_rows, coarse_cell_offsets, coarse_n, fine_row_offsets,
+                             fine_cell_offsets, ratio, reducer, fine_values, coarse_values, stream);
+}
+
+int sx_subset_rows(const int32_t* sub_row_offsets, const int32_t* sub_rows, int32_t sub_row_count, int64_t sub_n,
+                   const int32_t* sup_rows, int32_t sup_row_count, int32_t* pos, int32_t* flags, void* stream)
+{
+    if (sub_row_count < 0 || sup_row_count < 0 || sub_n < 0 || sub_n > INT32_MAX)
+        return fail(SX_ERR_INVALID, "sx_subset_rows: bad size");
+    if (!flags) return fail(SX_ERR_INVALID, "sx_subset_rows: null flags");
+    cudaError_t err = cudaMemsetAsync(flags, 0, sizeof(int32_t), (cudaStream_t)stream);
+    if (err != cudaSuccess) return cuda_fail(err, "sx_subset_rows");
+    if (sub_n == 0) return SX_OK;
+    if (!sub_row_offsets || !sub_rows || !pos || (sup_row_count > 0 && !sup_rows))
+        return fail(SX_ERR_INVALID, "sx_subset_rows: null argument");
+    err = sx_subset_rows_launch(sub_row_offsets, sub_rows, sub_row_count, (int)sub_n, sup_rows, sup_row_count, pos,
+                                flags, (cudaStream_t)stream);
+    if (err != cudaSuccess) return cuda_fail(err, "sx_subset_rows");
+    return SX_OK;
+}
+
+int sx_subset_copy(int scatter, int64_t sub_n, const int32_t* pos, const int32_t* sub_begin, const int32_t* sub_end,
+                   const int32_t* sub_cell_offsets, const int32_t* sup_row_offsets, const int32_t* sup_begin,
+                   const int32_t* sup_end, const int32_t* sup_cell_offsets, int32_t sup_row_count, void* sub_values,
+                   void* sup_values, int elem_size, void* stream)
+{
+    if (scatter != 0 && scatter != 1) return fail(SX_ERR_INVALID, "sx_subset_copy: scatter must be 0 or 1");
+    if (elem_size != 1 && elem_size != 4 && elem_size != 8)
+        return fail(SX_ERR_INVALID, "sx_subset_copy: element size %d not in {1, 4, 8}", elem_size);
+    if (sub_n < 0 || sub_n > INT32_MAX || sup_row_count < 0) return fail(SX_ERR_INVALID, "sx_subset_copy: bad size");
+    if (sub_n == 0 || sup_row_count == 0) return SX_OK;
+    if (!pos || !sub_begin || !sub_end || !sub_cell_offsets || !sup_row_offsets || !sup_begin || !sup_end ||
+        !sup_cell_offsets || !sub_values || !sup_values)
+        return fail(SX_ERR_INVALID, "sx_subset_copy: null argument");
+    cudaError_t err = sx_subset_copy_launch(scatter, (int)sub_n, pos, sub_begin, sub_end, sub_cell_offsets,
+                                            sup_row_offsets, sup_begin, sup_end, sup_cell_offsets, sup_row_count,
+                                            sub_values, sup_values, elem_size, (cudaStream_t)stream);
+    if (err != cudaSuccess) return cuda_fail(err, "sx_subset_copy");
+    return SX_OK;
+}
+
+int sx_row_lookup(const int32_t* rows, int32_t row_count, int32_t height, int32_t* lookup, int32_t* flags,
+                  void* stream)
+{
+    if (row_count < 0 || height <= 0) return fail(SX_ERR_INVALID, "sx_row_lookup: bad size");
+    if (!lookup || !flags || (row_count > 0 && !rows)) return fail(SX_ERR_INVALID, "sx_row_lookup: null argument");
+    cudaError_t err = cudaMemsetAsync(flags, 0, sizeof(int32_t), (cudaStream_t)stream);
+    if (err == cudaSuccess) err = sx_row_lookup_launch(rows, row_count, height, lookup, flags, (cudaStream_t)stream);
+    if (err != cudaSuccess) return cuda_fail(err, "sx_row_lookup");
+    return SX_OK;
+}
+
+int sx_upwind(int dtype, const int32_t* rows, const int32_t* row_ids, const int32_t* row_offsets, int32_t row_count,
+              const int32_t* begin, const int32_t* end, const int32_t* cell_offsets, int64_t n, int64_t cells, const int32_t* lookup,
+              const void* values, void* out, int32_t width, int32_t height, double a, double b, double dt, double dx,
+              double dy, int direct, void* stream)
+{
+    if (dtype != SX_F32 && dtype != SX_F64) return fail(SX_ERR_INVALID, "sx_upwind: dtype %d", dtype);
+    if (width <= 0 || height <= 0) return fail(SX_ERR_INVALID, "sx_upwind: width and height must be positive");
+    if (row_count < 0 || n < 0 || n > INT32_MAX || cells < 0 || cells > INT32_MAX)
+        return fail(SX_ERR_INVALID, "sx_upwind: bad size");
+    if (n == 0 || cells == 0) return SX_OK;
+    if (!rows || !row_offsets || !begin || !end || !cell_offsets || !lookup || !values || !out)
+        return fail(SX_ERR_INVALID, "sx_upwind: null argument");
+    cudaError_t err = sx_upwind_launch(rows, row_ids, row_offsets, row_count, begin, end, cell_offsets, (int)n, cells, lookup,
+                                       values, out, width, height, a, b, dt, dx, dy, direct ? 1 : 0, dtype == SX_F64,
+                                       (cudaStream_t)stream);
+    if (err != cudaSuccess) return cuda_fail(err, "sx_upwind");
+    return SX_OK;
+}
+
+int sx_upwind_f32(const int32_t* rows, const int32_t* row_offsets, int32_t row_count, const int32_t* begin,
+                  const int32_t* end, const int32_t* cell_offsets, int64_t n, int64_t cells, const int32_t* lookup,
+                  const float* values, float* out, int32_t width, int32_t height, float a, float b, float dt, float dx,
+                  float dy, int direct, void* stream)
+{
+    return sx_upwind(SX_F32, rows, nullptr, row_offsets, row_count, begin, end, cell_offsets, n, cells, lookup, values, out,
+                     width, height, a, b, dt, dx, dy, direct, stream);
+}
+
+int sx_upwind_f64(const int32_t* rows, const int32_t* row_offsets, int32_t row_count, const int32_t* begin,
+                  const int32_t* end, const int32_t* cell_offsets, int64_t n, int64_t cells, const int32_t* lookup,
+                  const double* values, double* out, int32_t width, int32_t height, double a, double b, double dt,
+                  double dx, double dy, int direct, void* stream)
+{
+    return sx_upwind(SX_F64, rows, nullptr, row_offsets, row_count, begin, end, cell_offsets, n, cells, lookup, values, out,
+                     width, height, a, b, dt, dx, dy, direct, stream);
+}
+
+int sx_threshold_rle(const float* values, int32_t width, int32_t height, float threshold, int gradient, int32_t* counts,
+                     const int32_t* offsets, int32_t* out_begin, int32_t* out_end, void* stream)
+{
+    if (width <= 0 || height <= 0) return fail(SX_ERR_INVALID, "sx_threshold_rle: width and height must be positive");
+    if ((long long)width * height > INT32_MAX) return fail(SX_ERR_INVALID, "sx_threshold_rle: grid too large");
+    if (!values) return fail(SX_ERR_INVALID, "sx_threshold_rle: null values");
+    if (!out_begin && !counts) return fail(SX_ERR_INVALID, "sx_threshold_rle: need counts or outputs");
+    if (out_begin && (!out_end || !offsets)) return fail(SX_ERR_INVALID, "sx_threshold_rle: write mode needs offsets");
+    cudaError_t err = sx_threshold_launch(values, width, height, threshold, gradient ? 1 : 0, out_begin ? nullptr : counts,
+                                          offsets, out_begin, out_end, (cudaStream_t)stream);
+    if (err != cudaSuccess) return cuda_fail(err, "sx_threshold_rle");
+    return SX_OK;
+}
+
+int sx_gradient_threshold_rle(const float* values, int32_t width, int32_t height, float threshold, int32_t* counts,
+                              const int32_t* offsets, int32_t* out_begin, int32_t* out_end, void* stream)
+{
+    return sx_threshold_rle(values, width, height, threshold, 1, counts, offsets, out_begin, out_end, stream);
+}
+
+int sx_locate_cells(const int32_t* rows, const int32_t* row_offsets, const int32_t* begin, const int32_t* end,
+                    int32_t row_count, const int32_t* query_rows, const int32_t* query_cols, int64_t count,
+                    int32_t* out, void* stream)
+{
+    if (row_count < 0 || count < 0) return fail(SX_ERR_INVALID, "sx_locate_cells: negative size");
+    if (count == 0) return SX_OK;
+    if (!query_rows || !query_cols || !out || (row_count > 0 && (!rows || !row_offsets)))
+        return fail(SX_ERR_INVALID, "sx_locate_cells: null argument");
+    cudaError_t err = sx_locate_cells_launch(rows, row_offsets, begin, end, row_count, query_rows, query_cols, count,
+                                             out, (cudaStream_t)stream);
+    if (err != cudaSuccess) return cuda_fail(err, "sx_locate_cells");
+    return SX_OK;
+}
+
+int sx_mass_integral(int dtype, const void* values, int64_t n, double scale, double* partials, int parts, double* out,
+                     void* stream)
+{
+    if (dtype != SX_F32 && dtype != SX_F64) return fail(SX_ERR_INVALID, "sx_mass_integral: dtype %d", dtype);
+    if (n < 0 || parts < 1 || parts > 4096) return fail(SX_ERR_INVALID, "sx_mass_integral: bad size");
+    if (!partials || !out || (n > 0 && !values)) return fail(SX_ERR_INVALID, "sx_mass_integral: null argument");
+    cudaError_t err = sx_mass_launch(values, n, dtype == SX_F64, scale, partials, parts, out, (cudaStream_t)stream);
+    if (err != cudaSuccess) return cuda_fail(err, "sx_mass_integral");
+    return SX_OK;
+}
+
+int sx_mass_integral_f64(const double* values, int64_t n, double scale, double* partials, int parts, double* out,
+                         void* stream)
+{
+    return sx_mass_integral(SX_F64, values, n, scale, partials, parts, out, stream);
 }
 
 }  // extern "C"

@@ -1,0 +1,772 @@
+// Interval fields: cell offsets, prolongation/restriction, subset copies,
+// first-order upwind, gradient-threshold run-length encoding, and the
+// compensated mass integral.
+//
+// A field stores one value per active cell, row by row, with int32 cell
+// offsets per interval (subsetix_cupy/interval_field.py:19-89).  Every
+// float formula below follows the reference's source order.  It is written
+// with explicit round-to-nearest intrinsics, so the compiler cannot fuse a
+// multiply and an add.  Results are therefore reproducible bit for bit
+// against a host build without FMA contraction, and the same code serves
+// FP32 and FP64.
+
+#include <climits>
+
+#include "sx_internal.cuh"
+
+// ---------------------------------------------------------------------------
+// Arithmetic helpers without contraction (float and double)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float sx_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float sx_sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float sx_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float sx_div(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ float sx_sqrt(float a) { return __fsqrt_rn(a); }
+__device__ __forceinline__ double sx_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sx_sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double sx_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double sx_div(double a, double b) { return __ddiv_rn(a, b); }
+
+// Row ordinal of interval i: the last p with off[p] <= i and off[p+1] > i.
+__device__ __forceinline__ int sx_row_of(const int* __restrict__ off, int rows, int i)
+{
+    int lo = 0, hi = rows - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= i) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// ---------------------------------------------------------------------------
+// Exclusive scan of interval lengths: int32 cell offsets
+// (interval_field.py:67-73).  Single pass with look-back, like sx_scan_i32.
+// ---------------------------------------------------------------------------
+#define SX_LEN_ITEMS 8
+__global__ void __launch_bounds__(SX_BLOCK) sx_cell_offsets_kernel(const int* __restrict__ b, const int* __restrict__ e,
+                                                                   long long n, int* __restrict__ out, int* result,
+                                                                   SxScanState st)
+{
+    __shared__ int s_tile;
+    __shared__ unsigned s_epoch;
+    __shared__ int s_warp[SX_BLOCK / 32];
+    __shared__ int s_base;
+    __shared__ unsigned s_flags;
+    sx_ticket(st, &s_tile, &s_epoch);
+    const int tile = s_tile;
+    const unsigned epoch = s_epoch;
+    const long long base_idx = (long long)tile * SX_BLOCK * SX_LEN_ITEMS + (long long)threadIdx.x * SX_LEN_ITEMS;
+    int v[SX_LEN_ITEMS];
+    int sum = 0;
+#pragma unroll
+    for (int i = 0; i < SX_LEN_ITEMS; ++i) {
+        const long long idx = base_idx + i;
+        v[i] = idx < n ? (e[idx] - b[idx]) : 0;
+        sum += v[i];
+    }
+    int total;
+    const int ex = sx_block_exclusive_scan(sum, s_warp, &total);
+    if (threadIdx.x < 32) {
+        unsigned f = 0u;
+        const int base = sx_lookback_warp(st, tile, epoch, total, f);
+        if (threadIdx.x == 0) {
+            s_base = base;
+            s_flags = f;
+        }
+    }
+    __syncthreads();
+    int run = s_base + ex;
+#pragma unroll
+    for (int i = 0; i < SX_LEN_ITEMS; ++i) {
+        const long long idx = base_idx + i;
+        if (idx < n) out[idx] = run;
+        run += v[i];
+        if (idx == n - 1) out[n] = run;
+    }
+    if (n == 0 && tile == 0 && threadIdx.x == 0) out[0] = 0;
+    sx_retire(st, epoch, s_flags, result);
+}
+
+cudaError_t sx_cell_offsets_launch(const int* b, const int* e, long long n, int* out, int* result, const SxScanState& st,
+                                   cudaStream_t stream)
+{
+    const long long per = (long long)SX_BLOCK * SX_LEN_ITEMS;
+    const int tiles = (int)((n + per - 1) / per > 0 ? (n + per - 1) / per : 1);
+    cudaError_t err = cudaMemsetAsync(st.counters, 0, 16 + (size_t)tiles * 8, stream);
+    if (err != cudaSuccess) return err;
+    sx_cell_offsets_kernel<<<tiles, SX_BLOCK, 0, stream>>>(b, e, n, out, result, st);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Prolongation of a set (multilevel.py:213-264): [b*r, e*r) on rows
+// row*r + 0..r-1, for occupied rows only, in the same order.  `ord` holds
+// the exclusive scan of the occupied-row flags.
+// ---------------------------------------------------------------------------
+__global__ void sx_occupied_kernel(const int* __restrict__ off, int rows, int* __restrict__ flags)
+{
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < rows; q += gridDim.x * blockDim.x)
+        flags[q] = off[q + 1] > off[q] ? 1 : 0;
+}
+
+__global__ void sx_prolong_set_rows_kernel(const int* __restrict__ rows_in, const int* __restrict__ off, int rows,
+                                           const int* __restrict__ ord, int r, int* __restrict__ rows_out,
+                                           int* __restrict__ off_out)
+{
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < rows; q += gridDim.x * blockDim.x) {
+        const int n_q = off[q + 1] - off[q];
+        if (n_q > 0) {
+            const int p = ord[q];
+            for (int k = 0; k < r; ++k) {
+                rows_out[p * r + k] = rows_in[q] * r + k;
+                off_out[p * r + k] = r * off[q] + k * n_q;
+            }
+        }
+        if (q == rows - 1) off_out[ord[rows] * r] = r * off[rows];
+    }
+}
+
+__global__ void sx_prolong_set_intervals_kernel(const int* __restrict__ b, const int* __restrict__ e,
+                                                const int* __restrict__ off, int rows, int n, int r,
+                                                int* __restrict__ ob, int* __restrict__ oe, int* result)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int q = sx_row_of(off, rows, i);
+        const int n_q = off[q + 1] - off[q];
+        if (i + 1 < off[q + 1] && b[i + 1] < b[i]) atomicOr(&result[1], 1);
+        const int bi = b[i] * r, ei = e[i] * r;
+        const int base = r * off[q] + (i - off[q]);
+        for (int k = 0; k < r; ++k) {
+            ob[base + k * n_q] = bi;
+            oe[base + k * n_q] = ei;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Field prolongation (kernels.py:384-455): piecewise-constant injection onto
+// the prolonged set.  Every coarse row must be occupied (the caller checks,
+// as the reference's alignment check does).  Coarse interval i (ordinal o
+// in row ordinal p) maps in sub-row d to the fine interval
+// f = fine_off[p*r + d] + o, and fine cell k of f takes coarse cell k / r.
+// One warp handles one coarse interval.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void sx_prolong_field_kernel(const int* __restrict__ off, int rows, const int* __restrict__ coff, int n,
+                                        const int* __restrict__ foff_rows, const int* __restrict__ fcoff, int r,
+                                        const T* __restrict__ cv, T* __restrict__ fv)
+{
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    const long long ncells = coff[n];
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
+        const int cb = coff[i];
+        if (coff[i + 1] - cb <= 0) continue;
+        const int p = sx_row_of(off, rows, i);
+        const int o = i - off[p];
+        for (int d = 0; d < r; ++d) {
+            const int f = foff_rows[p * r + d] + o;
+            const int fs = fcoff[f];
+            const int fw = fcoff[f + 1] - fs;
+            // Rows whose begins decrease are re-sorted on the fine level, so
+            // fine interval f may be wider than coarse interval i; the
+            // reference then reads past i, and past the array at its end.
+            // Here reads stay inside the array (0 beyond it).
+            for (int t = lane; t < fw; t += 32) {
+                const long long src = (long long)cb + t / r;
+                fv[fs + t] = src < ncells ? cv[src] : (T)0;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Field restriction (kernels.py:458-599 and multilevel.py:410-479).  The
+// coarse set is restrict_set(fine).  For coarse interval i (row ordinal p)
+// and sub-row dy, the fine interval is fine_off[p*r + dy] + (i -
+// coarse_off[p]).
+// Checks, with the reference's error order (flag bits):
+//   1  the fine row count differs from coarse rows x r
+//   2  fine rows are not coarse_row*r + dy
+//   8  a fine interval is not [r*cb, r*ce)
+// The reduction keeps the reference's order: sub-row outer, column inner,
+// stop early at the fine interval's end; mean = sum * norm.
+// ---------------------------------------------------------------------------
+__global__ void sx_restrict_check_kernel(const int* __restrict__ crows, int crow_count, const int* __restrict__ coff_rows,
+                                         const int* __restrict__ cb, const int* __restrict__ ce, int cn,
+                                         const int* __restrict__ frows, int frow_count, const int* __restrict__ foff_rows,
+                                         const int* __restrict__ fb, const int* __restrict__ fe, int fn, int r,
+                                         int* __restrict__ flags)
+{
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int stride = gridDim.x * blockDim.x;
+    if (tid == 0 && frow_count != crow_count * r) atomicOr(flags, 1);
+    if (frow_count != crow_count * r) return;
+    for (long long j = tid; j < (long long)crow_count * r; j += stride) {
+        const int p = (int)(j / r), dy = (int)(j % r);
+        if (frows[j] != crows[p] * r + dy) atomicOr(flags, 2);
+    }
+    for (long long j = tid; j < (long long)cn * r; j += stride) {
+        const int i = (int)(j / r), dy = (int)(j % r);
+        const int p = sx_row_of(coff_rows, crow_count, i);
+        const long long f = (long long)foff_rows[p * r + dy] + (i - coff_rows[p]);
+        if (f < 0 || f >= fn) {
+            atomicOr(flags, 8);
+            continue;
+        }
+        if (fb[f] != cb[i] * r || fe[f] != ce[i] * r) atomicOr(flags, 8);
+    }
+}
+
+template <typename T>
+__global__ void sx_restrict_field_kernel(const int* __restrict__ coff_rows, int crow_count, const int* __restrict__ ccoff,
+                                         int cn, const int* __restrict__ foff_rows, const int* __restrict__ fcoff, int r,
+                                         int reducer, T norm, const T* __restrict__ fv, T* __restrict__ cv)
+{
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < cn; i += warps) {
+        const int p = sx_row_of(coff_rows, crow_count, i);
+        const int cb = ccoff[i];
+        const int w = ccoff[i + 1] - cb;
+        if (w <= 0) continue;
+        const int ordinal = i - coff_rows[p];
+        for (int k = lane; k < w; k += 32) {
+            T acc = (T)0, lo = (T)0, hi = (T)0;
+            bool have = false;
+            for (int dy = 0; dy < r; ++dy) {
+                const int f = foff_rows[p * r + dy] + ordinal;
+                const int fend = fcoff[f + 1];
+                const int start = fcoff[f] + k * r;
+                for (int dx = 0; dx < r; ++dx) {
+                    const int idx = start + dx;
+                    if (idx >= fend) break;
+                    const T v = fv[idx];
+                    if (reducer == 2) {
+                        if (!have || v < lo) lo = v;
+                    } else if (reducer == 3) {
+                        if (!have || v > hi) hi = v;
+                    } else {
+                        acc = sx_add(acc, v);
+                    }
+                    have = true;
+                }
+            }
+            cv[cb + k] = reducer == 0 ? sx_mul(acc, norm) : reducer == 1 ? acc : reducer == 2 ? lo : hi;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Subset gather / scatter (fields.py:127-294): copy the cells of each subset
+// interval between a subset field and a superset field with the same
+// coordinates.  A binary search finds the superset interval, then the walk
+// goes across superset intervals in the reference's way (cells of the
+// subset that the superset lacks are skipped).  `pos` maps each subset
+// interval to its superset row ordinal.  One warp per subset interval: lane
+// 0 walks, and the warp copies each piece.
+// ---------------------------------------------------------------------------
+template <typename E>
+__global__ void sx_subset_copy_kernel(int scatter, int n, const int* __restrict__ pos, const int* __restrict__ sb,
+                                      const int* __restrict__ se, const int* __restrict__ scoff,
+                                      const int* __restrict__ uoff, const int* __restrict__ ub,
+                                      const int* __restrict__ ue, const int* __restrict__ ucoff, int urows,
+                                      E* __restrict__ sub, E* __restrict__ sup)
+{
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
+        const int row = pos[i];
+        if (row < 0 || row >= urows) continue;
+        const int start = sb[i], stop = se[i];
+        if (stop <= start) continue;
+        const int rs = uoff[row], rt = uoff[row + 1];
+        if (rs >= rt) continue;
+        int idx = rs;
+        if (lane == 0) {
+            int lo = rs, hi = rt - 1;
+            bool found = false;
+            while (lo <= hi) {
+                const int mid = (lo + hi) >> 1;
+                if (start < ub[mid]) hi = mid - 1;
+                else if (start >= ue[mid]) lo = mid + 1;
+                else {
+                    idx = mid;
+                    found = true;
+                    break;
+                }
+            }
+            if (!found) idx = lo;
+            if (idx < rs) idx = rs;
+        }
+        idx = __shfl_sync(0xFFFFFFFFu, idx, 0);
+        int cur = start, done = 0;
+        const int sub_base = scoff[i];
+        while (cur < stop && idx < rt) {
+            const int b = ub[idx], e = ue[idx];
+            if (cur < b) {
+                cur = b;
+                continue;
+            }
+            const int stop2 = stop < e ? stop : e;
+            const int len = stop2 - cur;
+            if (len > 0) {
+                const long long sp = (long long)ucoff[idx] + (cur - b);
+                const long long dp = (long long)sub_base + done;
+                for (int t = lane; t < len; t += 32) {
+                    if (scatter) sup[sp + t] = sub[dp + t];
+                    else sub[dp + t] = sup[sp + t];
+                }
+                done += len;
+                cur = stop2;
+            }
+            if (cur >= e) ++idx;
+            if (len == 0 && cur < stop) ++cur;
+        }
+    }
+}
+
+// Superset row ordinal of each subset interval (searchsorted), or a flag
+// when the row is missing (fields.py:310-316).
+__global__ void sx_subset_rows_kernel(const int* __restrict__ soff, const int* __restrict__ srows, int srow_count,
+                                      int sn, const int* __restrict__ urows, int urow_count, int* __restrict__ pos,
+                                      int* __restrict__ flags)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < sn; i += gridDim.x * blockDim.x) {
+        const int p = sx_row_of(soff, srow_count, i);
+        const int row = srows[p];
+        int lo = 0, hi = urow_count;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (urows[mid] < row) lo = mid + 1; else hi = mid;
+        }
+        if (lo >= urow_count || urows[lo] != row) atomicOr(flags, 1);
+        pos[i] = lo;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// First-order upwind with zero exterior (interval_stencil.py:16-113).
+// A cell outside [0, width) x [0, height), or outside the set, reads as 0.
+// `lookup[row id]` gives the row ordinal or -1.  Blocks take runs of 256
+// consecutive cells.  Thread 0 locates the block's first interval and row,
+// and each thread walks forward to its own cell.  Neighbours inside the
+// cell's own interval are read directly; the others are found by binary
+// search in their row.
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T sx_sample(int row, int x, int height, int width, const int* __restrict__ lookup,
+                                       const int* __restrict__ off, const int* __restrict__ b,
+                                       const int* __restrict__ e, const int* __restrict__ coff,
+                                       const T* __restrict__ v)
+{
+    if (row < 0 || row >= height || x < 0 || x >= width) return (T)0;
+    const int ord = lookup[row];
+    if (ord < 0) return (T)0;
+    int lo = off[ord], hi = off[ord + 1] - 1;
+    while (lo <= hi) {
+        const int mid = (lo + hi) >> 1;
+        if (x < b[mid]) hi = mid - 1;
+        else if (x >= e[mid]) lo = mid + 1;
+        else return v[coff[mid] + (x - b[mid])];
+    }
+    return (T)0;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) sx_upwind_kernel(const int* __restrict__ rows, const int* __restrict__ rid,
+                                                        const int* __restrict__ off,
+                                                        int row_count, const int* __restrict__ b,
+                                                        const int* __restrict__ e, const int* __restrict__ coff, int n,
+                                                        const int* __restrict__ lookup, const T* __restrict__ v,
+                                                        T* __restrict__ out, int width, int height, T a, T bb, T dt,
+                                                        T dx, T dy, int direct, long long value_count)
+{
+    __shared__ int s_i, s_p;
+    const long long cells = coff[n] < value_count ? (long long)coff[n] : value_count;
+    for (long long c0 = (long long)blockIdx.x * blockDim.x; c0 < cells; c0 += (long long)gridDim.x * blockDim.x) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int lo = 0, hi = n - 1;  // last interval with coff <= c0
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (coff[mid] <= c0) lo = mid; else hi = mid - 1;
+            }
+            s_i = lo;
+            s_p = sx_row_of(off, row_count, lo);
+        }
+        __syncthreads();
+        const long long c = c0 + threadIdx.x;
+        if (c >= cells) continue;
+        int i = s_i, p = s_p;
+        while (coff[i + 1] <= c) ++i;  // skips empty intervals too
+        while (off[p + 1] <= i) ++p;
+        const int row = rid ? rid[i] : rows[p];
+        const int ib = b[i], ie = e[i];
+        const int x = ib + (int)(c - coff[i]);
+        const T center = v[c];
+        // Inside the cell's own interval of a row whose intervals are sorted
+        // and disjoint, the search below would return this interval, so the
+        // neighbour is read directly.
+        T left, right;
+        if (direct && x - 1 >= ib) left = (x - 1 >= 0 && x - 1 < width) ? v[c - 1] : (T)0;
+        else left = sx_sample<T>(row, x - 1, height, width, lookup, off, b, e, coff, v);
+        if (direct && x + 1 < ie) right = (x + 1 >= 0 && x + 1 < width) ? v[c + 1] : (T)0;
+        else right = sx_sample<T>(row, x + 1, height, width, lookup, off, b, e, coff, v);
+        const T down = sx_sample<T>(row - 1, x, height, width, lookup, off, b, e, coff, v);
+        const T up = sx_sample<T>(row + 1, x, height, width, lookup, off, b, e, coff, v);
+        const T du_dx = a >= (T)0 ? sx_div(sx_sub(center, left), dx) : sx_div(sx_sub(right, center), dx);
+        const T du_dy = bb >= (T)0 ? sx_div(sx_sub(center, down), dy) : sx_div(sx_sub(up, center), dy);
+        out[c] = sx_sub(center, sx_mul(dt, sx_add(sx_mul(a, du_dx), sx_mul(bb, du_dy))));
+    }
+}
+
+__global__ void sx_row_lookup_kernel(const int* __restrict__ rows, int row_count, int height, int* __restrict__ lookup,
+                                     int* __restrict__ flags)
+{
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < row_count; p += gridDim.x * blockDim.x) {
+        const int r = rows[p];
+        if (r < 0 || r >= height) {
+            atomicOr(flags, 1);
+            continue;
+        }
+        lookup[r] = p;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Gradient magnitude and threshold run-length encoding on a full
+// width x height grid (regrid.py:20-124,172-223).  The gradient uses
+// central differences inside and one-sided ones at the borders, with no
+// /dx, and is sqrt(gx*gx + gy*gy).  A run is a stretch of
+// value >= threshold.  One warp per row, 32 columns per step: a ballot
+// gives the mask, and the run starts and stops come from the mask and the
+// carry bit.  Each run end is written once (see DESIGN.md 5.2 for the
+// reference's double write).
+// ---------------------------------------------------------------------------
+template <bool GRAD>
+__device__ __forceinline__ bool sx_pred(const float* __restrict__ d, int x, int y, int width, int height, float thr)
+{
+    const long long idx = (long long)y * width + x;
+    if (!GRAD) return d[idx] >= thr;
+    const float c = d[idx];
+    float gx = 0.0f, gy = 0.0f;
+    if (width > 1) {
+        if (x == 0) gx = __fsub_rn(d[idx + 1], c);
+        else if (x == width - 1) gx = __fsub_rn(c, d[idx - 1]);
+        else gx = __fmul_rn(__fsub_rn(d[idx + 1], d[idx - 1]), 0.5f);
+    }
+    if (height > 1) {
+        if (y == 0) gy = __fsub_rn(d[idx + width], c);
+        else if (y == height - 1) gy = __fsub_rn(c, d[idx - width]);
+        else gy = __fmul_rn(__fsub_rn(d[idx + width], d[idx - width]), 0.5f);
+    }
+    return __fsqrt_rn(__fadd_rn(__fmul_rn(gx, gx), __fmul_rn(gy, gy))) >= thr;
+}
+
+template <bool GRAD>
+__global__ void sx_threshold_rle_kernel(const float* __restrict__ d, int width, int height, float thr,
+                                        int* __restrict__ counts, const int* __restrict__ offsets,
+                                        int* __restrict__ ob, int* __restrict__ oe)
+{
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int y = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; y < height; y += warps) {
+        unsigned prev = 0u;
+        int n = 0;
+        const int base_out = ob ? offsets[y] : 0;
+        for (int base = 0; base < width; base += 32) {
+            const int x = base + lane;
+            const bool on = x < width && sx_pred<GRAD>(d, x, y, width, height, thr);
+            const unsigned m = __ballot_sync(0xFFFFFFFFu, on);
+            const unsigned starts = m & ~((m << 1) | prev);
+            const unsigned stops = ((m << 1) | prev) & ~m & ((width - base >= 32) ? 0xFFFFFFFFu : ((1u << (width - base)) - 1u));
+            if (ob) {
+                const unsigned below = (1u << lane) - 1u;
+                if ((starts >> lane) & 1u) ob[base_out + n + __popc(starts & below)] = x;
+                // a stop at bit j closes the run that started before it
+                if ((stops >> lane) & 1u) oe[base_out + n + __popc(starts & below) - 1] = x;
+            }
+            n += __popc(starts);
+            prev = (width - base >= 32) ? (m >> 31) & 1u : (m >> (width - base - 1)) & 1u;
+        }
+        if (ob && prev && lane == 0) oe[base_out + n - 1] = width;
+        if (counts && lane == 0) counts[y] = n;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Compensated (Neumaier) sum in FP64 of a float or double array, in two
+// stages: per-block partial (sum, compensation) pairs, then one block that
+// combines them in a fixed order.  The result is deterministic.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void sx_neumaier(double& s, double& c, double v)
+{
+    const double t = __dadd_rn(s, v);
+    if (fabs(s) >= fabs(v)) c = __dadd_rn(c, __dadd_rn(__dsub_rn(s, t), v));
+    else c = __dadd_rn(c, __dadd_rn(__dsub_rn(v, t), s));
+    s = t;
+}
+
+template <typename T>
+__global__ void sx_mass_partial_kernel(const T* __restrict__ v, long long n, double* __restrict__ part)
+{
+    __shared__ double ss[SX_BLOCK], sc[SX_BLOCK];
+    double s = 0.0, c = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        sx_neumaier(s, c, (double)v[i]);
+    ss[threadIdx.x] = s;
+    sc[threadIdx.x] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double S = 0.0, C = 0.0;
+        for (int t = 0; t < (int)blockDim.x; ++t) {
+            sx_neumaier(S, C, ss[t]);
+            C = __dadd_rn(C, sc[t]);
+        }
+        part[2 * blockIdx.x] = S;
+        part[2 * blockIdx.x + 1] = C;
+    }
+}
+
+__global__ void sx_mass_final_kernel(const double* __restrict__ part, int parts, double scale, double* __restrict__ out)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        double S = 0.0, C = 0.0;
+        for (int t = 0; t < parts; ++t) {
+            sx_neumaier(S, C, part[2 * t]);
+            C = __dadd_rn(C, part[2 * t + 1]);
+        }
+        out[0] = __dmul_rn(__dadd_rn(S, C), scale);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Row shape check: OR of SX_ROWS_* bits over all adjacent interval pairs.
+// ---------------------------------------------------------------------------
+__global__ void sx_check_rows_kernel(const int* __restrict__ b, const int* __restrict__ e, const int* __restrict__ off,
+                                     int rows, long long n, int* flags)
+{
+    unsigned f = 0u;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int bi = b[i], ei = e[i];
+        if (ei <= bi) f |= 4u;
+        const int q = sx_row_of(off, rows, (int)i);
+        if (i + 1 < off[q + 1]) {
+            const int nb = b[i + 1], ne = e[i + 1];
+            if (nb < bi) f |= 1u;
+            if (nb < ei) f |= 2u;
+            else if (nb == ei) f |= 8u;
+            if (ne < ei) f |= 16u;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) f |= __shfl_xor_sync(0xFFFFFFFFu, f, o);
+    if ((threadIdx.x & 31) == 0 && f) atomicOr(flags, (int)f);
+}
+
+cudaError_t sx_check_rows_launch(const int* b, const int* e, const int* off, int rows, long long n, int* flags,
+                                 cudaStream_t stream)
+{
+    cudaError_t err = cudaMemsetAsync(flags, 0, sizeof(int), stream);
+    if (err != cudaSuccess || n <= 0 || rows <= 0) return err;
+    long long g = (n + 255) / 256;
+    if (g > 148 * 32) g = 148 * 32;
+    sx_check_rows_kernel<<<(int)g, 256, 0, stream>>>(b, e, off, rows, n, flags);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Cell lookup (interval_field.py:162-297): global interval index holding
+// (row, col), or -1.  Binary search over the row ids, then over the row's
+// intervals (same search order as the reference).
+// ---------------------------------------------------------------------------
+__global__ void sx_locate_cells_kernel(const int* __restrict__ rows, const int* __restrict__ off, const int* __restrict__ b,
+                                       const int* __restrict__ e, int row_count, const int* __restrict__ qr,
+                                       const int* __restrict__ qc, long long q, int* __restrict__ out)
+{
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < q; t += (long long)gridDim.x * blockDim.x) {
+        int found = -1;
+        if (row_count > 0) {
+            const int row = qr[t], col = qc[t];
+            int lo = 0, hi = row_count - 1, pos = -1;
+            while (lo <= hi) {
+                const int mid = (lo + hi) >> 1;
+                const int v = rows[mid];
+                if (v == row) {
+                    pos = mid;
+                    break;
+                }
+                if (v < row) lo = mid + 1; else hi = mid - 1;
+            }
+            if (pos >= 0) {
+                lo = off[pos];
+                hi = off[pos + 1] - 1;
+                while (lo <= hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (col < b[mid]) hi = mid - 1;
+                    else if (col >= e[mid]) lo = mid + 1;
+                    else {
+                        found = mid;
+                        break;
+                    }
+                }
+            }
+        }
+        out[t] = found;
+    }
+}
+
+cudaError_t sx_locate_cells_launch(const int* rows, const int* off, const int* b, const int* e, int row_count,
+                                   const int* qr, const int* qc, long long q, int* out, cudaStream_t stream)
+{
+    if (q <= 0) return cudaSuccess;
+    long long g = (q + 255) / 256;
+    if (g > 148 * 64) g = 148 * 64;
+    sx_locate_cells_kernel<<<(int)g, 256, 0, stream>>>(rows, off, b, e, row_count, qr, qc, q, out);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Host launchers
+// ---------------------------------------------------------------------------
+static int sx_grid(long long work, int block, int cap = 65535 * 8)
+{
+    long long g = (work + block - 1) / block;
+    if (g < 1) g = 1;
+    if (g > cap) g = cap;
+    return (int)g;
+}
+
+cudaError_t sx_prolong_set_launch(const int* rows_in, const int* off, const int* b, const int* e, int rows, int n, int r,
+                                  int* occupied, int* ord, int* result, const SxScanState& st, int* rows_out,
+                                  int* off_out, int* ob, int* oe, cudaStream_t stream)
+{
+    sx_occupied_kernel<<<sx_grid(rows, 256), 256, 0, stream>>>(off, rows, occupied);
+    cudaError_t err = sx_scan_i32_launch(occupied, rows, ord, result, st, stream);
+    if (err != cudaSuccess) return err;
+    sx_prolong_set_rows_kernel<<<sx_grid(rows, 256), 256, 0, stream>>>(rows_in, off, rows, ord, r, rows_out, off_out);
+    if (n > 0)
+        sx_prolong_set_intervals_kernel<<<sx_grid(n, 256), 256, 0, stream>>>(b, e, off, rows, n, r, ob, oe, result);
+    return cudaGetLastError();
+}
+
+cudaError_t sx_prolong_field_launch(const int* off, int rows, const int* coff, int n, const int* foff_rows,
+                                    const int* fcoff, int r, const void* cv, void* fv, int dbl, cudaStream_t stream)
+{
+    const int grid = sx_grid((long long)n * 32, 256);
+    if (dbl)
+        sx_prolong_field_kernel<double><<<grid, 256, 0, stream>>>(off, rows, coff, n, foff_rows, fcoff, r,
+                                                                  (const double*)cv, (double*)fv);
+    else
+        sx_prolong_field_kernel<float><<<grid, 256, 0, stream>>>(off, rows, coff, n, foff_rows, fcoff, r,
+                                                                 (const float*)cv, (float*)fv);
+    return cudaGetLastError();
+}
+
+cudaError_t sx_restrict_check_launch(const int* crows, int crow_count, const int* coff_rows, const int* cb,
+                                     const int* ce, int cn, const int* frows, int frow_count, const int* foff_rows,
+                                     const int* fb, const int* fe, int fn, int r, int* flags, cudaStream_t stream)
+{
+    long long work = (long long)(crow_count > cn ? crow_count : cn) * r;
+    sx_restrict_check_kernel<<<sx_grid(work, 256), 256, 0, stream>>>(crows, crow_count, coff_rows, cb, ce, cn, frows,
+                                                                     frow_count, foff_rows, fb, fe, fn, r, flags);
+    return cudaGetLastError();
+}
+
+cudaError_t sx_restrict_field_launch(const int* coff_rows, int crow_count, const int* ccoff, int cn,
+                                     const int* foff_rows, const int* fcoff, int r, int reducer, double norm,
+                                     const void* fv, void* cv, int dbl, cudaStream_t stream)
+{
+    const int grid = sx_grid((long long)cn * 32, 256);
+    if (dbl)
+        sx_restrict_field_kernel<double><<<grid, 256, 0, stream>>>(coff_rows, crow_count, ccoff, cn, foff_rows, fcoff, r,
+                                                                   reducer, norm, (const double*)fv, (double*)cv);
+    else
+        sx_restrict_field_kernel<float><<<grid, 256, 0, stream>>>(coff_rows, crow_count, ccoff, cn, foff_rows, fcoff, r,
+                                                                  reducer, (float)norm, (const float*)fv, (float*)cv);
+    return cudaGetLastError();
+}
+
+cudaError_t sx_subset_rows_launch(const int* soff, const int* srows, int srow_count, int sn, const int* urows,
+                                  int urow_count, int* pos, int* flags, cudaStream_t stream)
+{
+    if (sn <= 0) return cudaSuccess;
+    sx_subset_rows_kernel<<<sx_grid(sn, 256), 256, 0, stream>>>(soff, srows, srow_count, sn, urows, urow_count, pos,
+                                                                 flags);
+    return cudaGetLastError();
+}
+
+cudaError_t sx_subset_copy_launch(int scatter, int n, const int* pos, const int* sb, const int* se, const int* scoff,
+                                  const int* uoff, const int* ub, const int* ue, const int* ucoff, int urows,
+                                  void* sub, void* sup, int elem_size, cudaStream_t stream)
+{
+    if (n <= 0) return cudaSuccess;
+    const int grid = sx_grid((long long)n * 32, 256);
+    switch (elem_size) {
+        case 1:
+            sx_subset_copy_kernel<unsigned char><<<grid, 256, 0, stream>>>(scatter, n, pos, sb, se, scoff, uoff, ub, ue,
+                                                                           ucoff, urows, (unsigned char*)sub,
+                                                                           (unsigned char*)sup);
+            break;
+        case 4:
+            sx_subset_copy_kernel<unsigned int><<<grid, 256, 0, stream>>>(scatter, n, pos, sb, se, scoff, uoff, ub, ue,
+                                                                          ucoff, urows, (unsigned int*)sub,
+                                                                          (unsigned int*)sup);
+            break;
+        case 8:
+            sx_subset_copy_kernel<unsigned long long><<<grid, 256, 0, stream>>>(scatter, n, pos, sb, se, scoff, uoff, ub,
+                                                                                ue, ucoff, urows,
+                                                                                (unsigned long long*)sub,
+                                                                                (unsigned long long*)sup);
+            break;
+        default:
+            return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t sx_row_lookup_launch(const int* rows, int row_count, int height, int* lookup, int* flags,
+                                 cudaStream_t stream)
+{
+    cudaError_t err = cudaMemsetAsync(lookup, 0xFF, (size_t)height * sizeof(int), stream);
+    if (err != cudaSuccess) return err;
+    if (row_count > 0)
+        sx_row_lookup_kernel<<<sx_grid(row_count, 256), 256, 0, stream>>>(rows, row_count, height, lookup, flags);
+    return cudaGetLastError();
+}
+
+cudaError_t sx_upwind_launch(const int* rows, const int* rid, const int* off, int row_count, const int* b, const int* e, const int* coff,
+                             int n, long long cells, const int* lookup, const void* v, void* out, int width, int height,
+                             double a, double bb, double dt, double dx, double dy, int direct, int dbl,
+                             cudaStream_t stream)
+{
+    if (n <= 0 || cells <= 0) return cudaSuccess;
+    const int grid = sx_grid(cells, 256, 148 * 16);
+    if (dbl)
+        sx_upwind_kernel<double><<<grid, 256, 0, stream>>>(rows, rid, off, row_count, b, e, coff, n, lookup, (const double*)v,
+                                                           (double*)out, width, height, a, bb, dt, dx, dy, direct, cells);
+    else
+        sx_upwind_kernel<float><<<grid, 256, 0, stream>>>(rows, rid, off, row_count, b, e, coff, n, lookup, (const float*)v,
+                                                          (float*)out, width, height, (float)a, (float)bb, (float)dt,
+                                                          (float)dx, (float)dy, direct, cells);
+    return cudaGetLastError();
+}
+
+cudaError_t sx_threshold_launch(const float* d, int width, int height, float thr, int grad, int* counts,
+                                const int* offsets, int* ob, int* oe, cudaStream_t stream)
+{
+    const int grid = sx_grid((long long)height * 32, 256);
+    if (grad) sx_threshold_rle_kernel<true><<<grid, 256, 0, stream>>>(d, width, height, thr, counts, offsets, ob, oe);
+    else sx_threshold_rle_kernel<false><<<grid, 256, 0, stream>>>(d, width, height, thr, counts, offsets, ob, oe);
+    return cudaGetLastError();
+}
+
+cudaError_t sx_mass_launch(const void* v, long long n, int dbl, double scale, double* part, int parts, double* out,
+                           cudaStream_t stream)
+{
+    if (dbl) sx_mass_partial_kernel<double><<<parts, SX_BLOCK, 0, stream>>>((const double*)v, n, part);
+    else sx_mass_partial_kernel<float><<<parts, SX_BLOCK, 0, stream>>>((const float*)v, n, part);
+    sx_mass_final_kernel<<<1, 32, 0, stream>>>(part, parts, scale, out);
+    return cudaGetLastError();
+}

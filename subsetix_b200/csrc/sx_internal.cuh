@@ -7,8 +7,10 @@
 struct SxLeafDev {
     const int* begin;
     const int* end;
-    const int* off;  // aligned row offsets, length rows + 1
-    int widen;       // begin - widen, end + widen on load (0 for set operations)
+    const int* off;      // aligned row offsets, length rows + 1 (row y = [off[y], off[y+1]))
+    const int* off_end;  // when set, row y = [off[y], off_end[y]) instead
+    int widen;           // begin - widen, end + widen on load (0 for set operations)
+    int scale;           // > 1: [floor(b/scale), ceil(e/scale)) on load (restriction)
 };
 
 struct SxBoolArgs {
@@ -41,6 +43,8 @@ struct SxRowList {
     int count;
     int shift;
     int skip_empty;
+    int div;    // >= 1: row v maps to output row floor((v + shift) / div)
+    int phase;  // ranges: output row y reads source row y * div + phase - shift
 };
 
 struct SxAlignArgs {
@@ -52,7 +56,8 @@ struct SxAlignArgs {
     int* wcount;       // [nwords]
     int* wprefix;      // [nwords + 1]
     int* rows_out;     // capacity = sum of counts
-    int* aligned[SX_MAX_LEAVES * 2];  // per list, [rows_out + 1]; null to skip
+    int* aligned[SX_MAX_LEAVES * 2];      // per list, [rows_out + 1]; null to skip
+    int* aligned_end[SX_MAX_LEAVES * 2];  // per list, [rows_out]; when set, explicit [start, stop) ranges
     int* result;       // [0] rows_out count, [1] flags
 };
 
@@ -71,3 +76,37 @@ cudaError_t sx_align_launch(SxAlignArgs& A, int out_capacity, const SxScanState&
 
 // Records `msg` as the calling thread's sx_last_error() text and returns `code`.
 int sx_set_error(int code, const char* msg);
+
+// Interval fields (sx_fields.cu)
+cudaError_t sx_check_rows_launch(const int* b, const int* e, const int* off, int rows, long long n, int* flags,
+                                 cudaStream_t stream);
+cudaError_t sx_cell_offsets_launch(const int* b, const int* e, long long n, int* out, int* result, const SxScanState& st,
+                                   cudaStream_t stream);
+cudaError_t sx_prolong_set_launch(const int* rows_in, const int* off, const int* b, const int* e, int rows, int n, int r,
+                                  int* occupied, int* ord, int* result, const SxScanState& st, int* rows_out,
+                                  int* off_out, int* ob, int* oe, cudaStream_t stream);
+cudaError_t sx_prolong_field_launch(const int* off, int rows, const int* coff, int n, const int* foff_rows,
+                                    const int* fcoff, int r, const void* cv, void* fv, int dbl, cudaStream_t stream);
+cudaError_t sx_restrict_check_launch(const int* crows, int crow_count, const int* coff_rows, const int* cb,
+                                     const int* ce, int cn, const int* frows, int frow_count, const int* foff_rows,
+                                     const int* fb, const int* fe, int fn, int r, int* flags, cudaStream_t stream);
+cudaError_t sx_restrict_field_launch(const int* coff_rows, int crow_count, const int* ccoff, int cn,
+                                     const int* foff_rows, const int* fcoff, int r, int reducer, double norm,
+                                     const void* fv, void* cv, int dbl, cudaStream_t stream);
+cudaError_t sx_subset_rows_launch(const int* soff, const int* srows, int srow_count, int sn, const int* urows,
+                                  int urow_count, int* pos, int* flags, cudaStream_t stream);
+cudaError_t sx_subset_copy_launch(int scatter, int n, const int* pos, const int* sb, const int* se, const int* scoff,
+                                  const int* uoff, const int* ub, const int* ue, const int* ucoff, int urows,
+                                  void* sub, void* sup, int elem_size, cudaStream_t stream);
+cudaError_t sx_row_lookup_launch(const int* rows, int row_count, int height, int* lookup, int* flags,
+                                 cudaStream_t stream);
+cudaError_t sx_upwind_launch(const int* rows, const int* rid, const int* off, int row_count, const int* b, const int* e, const int* coff,
+                             int n, long long cells, const int* lookup, const void* v, void* out, int width, int height,
+                             double a, double bb, double dt, double dx, double dy, int direct, int dbl,
+                             cudaStream_t stream);
+cudaError_t sx_threshold_launch(const float* d, int width, int height, float thr, int grad, int* counts,
+                                const int* offsets, int* ob, int* oe, cudaStream_t stream);
+cudaError_t sx_mass_launch(const void* v, long long n, int dbl, double scale, double* part, int parts, double* out,
+                           cudaStream_t stream);
+cudaError_t sx_locate_cells_launch(const int* rows, const int* off, const int* b, const int* e, int row_count,
+                                   const int* qr, const int* qc, long long q, int* out, cudaStream_t stream);

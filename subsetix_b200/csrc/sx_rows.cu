@@ -29,7 +29,9 @@ __global__ void sx_align_mark_kernel(SxAlignArgs A)
     const SxRowList L = A.list[l];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L.count; i += gridDim.x * blockDim.x) {
         if (L.skip_empty && L.off[i + 1] <= L.off[i]) continue;
-        const long long v = (long long)L.rows[i] + L.shift - A.row_min;
+        long long u = (long long)L.rows[i] + L.shift;
+        if (L.div > 1) u = u >= 0 ? u / L.div : -((-u + L.div - 1) / L.div);  // floor division
+        const long long v = u - A.row_min;
         if (v < 0 || v >= A.nbits) continue;  // excluded by the caller's bounds
         atomicOr(&A.bitmap[v >> 5], 1u << (v & 31));
     }
@@ -63,13 +65,19 @@ __global__ void sx_align_offsets_kernel(SxAlignArgs A)
     int* dst = A.aligned[l];
     if (dst == nullptr) return;
     const SxRowList L = A.list[l];
+    int* dst_end = A.aligned_end[l];
     const int rout = A.result[0];
+    const long long div = L.div > 1 ? L.div : 1;
     for (int y = blockIdx.x * blockDim.x + threadIdx.x; y <= rout; y += gridDim.x * blockDim.x) {
+        // The closing offset stops after the last output row, so source rows
+        // beyond row_max do not leak into it.
         int pos;
-        if (y == rout) {
+        long long key = 0;
+        if (y == rout && rout == 0) {
             pos = L.count;
         } else {
-            const long long key = (long long)A.rows_out[y] - L.shift;
+            key = y == rout ? ((long long)A.rows_out[rout - 1] + 1) * div + L.phase - L.shift
+                            : (long long)A.rows_out[y] * div + L.phase - L.shift;
             int lo = 0, hi = L.count;
             while (lo < hi) {
                 const int mid = (lo + hi) >> 1;
@@ -77,7 +85,10 @@ __global__ void sx_align_offsets_kernel(SxAlignArgs A)
             }
             pos = lo;
         }
-        dst[y] = L.count > 0 ? L.off[pos] : 0;
+        const int start = L.count > 0 ? L.off[pos] : 0;
+        dst[y] = start;
+        if (dst_end && y < rout)
+            dst_end[y] = (pos < L.count && (long long)L.rows[pos] == key) ? L.off[pos + 1] : start;
     }
 }
 

@@ -217,8 +217,26 @@ __device__ __forceinline__ int sx_sweep_table(const SxBoolArgs& A, const int* s,
     return n;
 }
 
-// One row, K row-shifted views of one set, widened by A.leaf[l].widen:
-// union with merge semantics (touching runs join).
+// Begin/end of one interval after the leaf's coordinate transform: widened
+// by `widen` ([b - w, e + w)), or coarsened by `scale` ([floor(b/r), ceil(e/r))).
+__device__ __forceinline__ int sx_floordiv(int a, int r) { return a >= 0 ? a / r : -((-a + r - 1) / r); }
+
+__device__ __forceinline__ int sx_tb(const SxLeafDev& L, int i)
+{
+    const int b = __ldg(L.begin + i);
+    return L.scale > 1 ? sx_floordiv(b, L.scale) : b - L.widen;
+}
+
+__device__ __forceinline__ int sx_te(const SxLeafDev& L, int i)
+{
+    const int e = __ldg(L.end + i);
+    return L.scale > 1 ? -sx_floordiv(-e, L.scale) : e + L.widen;
+}
+
+// One row, K views of interval sets (row-shifted, widened or coarsened):
+// their union with the reference's merge semantics (touching runs join).
+// Begins and ends of a view must each be non-decreasing; every event at a
+// coordinate is applied before the run state is examined.
 template <int K, bool WRITE>
 __device__ __forceinline__ int sx_sweep_union(const SxBoolArgs& A, const int* s, const int* cnt, int* out_b, int* out_e,
                                               long long pos, bool& bad, bool& over)
@@ -229,9 +247,8 @@ __device__ __forceinline__ int sx_sweep_union(const SxBoolArgs& A, const int* s,
     for (int l = 0; l < K; ++l) {
         qb[l] = 0;
         qe[l] = 0;
-        const int w = A.leaf[l].widen;
-        hb[l] = cnt[l] > 0 ? __ldg(A.leaf[l].begin + s[l]) - w : INT_MAX;
-        he[l] = cnt[l] > 0 ? __ldg(A.leaf[l].end + s[l]) + w : INT_MAX;
+        hb[l] = cnt[l] > 0 ? sx_tb(A.leaf[l], s[l]) : INT_MAX;
+        he[l] = cnt[l] > 0 ? sx_te(A.leaf[l], s[l]) : INT_MAX;
         rem += 2 * cnt[l];
     }
     int active = 0;
@@ -247,27 +264,26 @@ __device__ __forceinline__ int sx_sweep_union(const SxBoolArgs& A, const int* s,
         const bool was = active > 0;
 #pragma unroll
         for (int l = 0; l < K; ++l) {
-            const int w = A.leaf[l].widen;
             // ends before begins: an element whose begin has not been taken at
             // an earlier coordinate is empty (or reversed) and breaks the contract
-            if (qe[l] < cnt[l] && he[l] == c) {
+            while (qe[l] < cnt[l] && he[l] == c) {
                 --active;
                 --rem;
                 if (qe[l] >= qb[l]) bad = true;
                 const int qn = ++qe[l];
                 if (qn < cnt[l]) {
-                    const int v = __ldg(A.leaf[l].end + s[l] + qn) + w;
-                    if (v <= c) bad = true;
+                    const int v = sx_te(A.leaf[l], s[l] + qn);
+                    if (v < c) bad = true;
                     he[l] = v;
                 }
             }
-            if (qb[l] < cnt[l] && hb[l] == c) {
+            while (qb[l] < cnt[l] && hb[l] == c) {
                 ++active;
                 --rem;
                 const int qn = ++qb[l];
                 if (qn < cnt[l]) {
-                    const int v = __ldg(A.leaf[l].begin + s[l] + qn) - w;
-                    if (v <= c) bad = true;
+                    const int v = sx_tb(A.leaf[l], s[l] + qn);
+                    if (v < c) bad = true;
                     hb[l] = v;
                 }
             }
@@ -312,7 +328,7 @@ __global__ void __launch_bounds__(32 * SX_SWEEP_WARPS) sx_sweep_kernel(SxBoolArg
 #pragma unroll
     for (int l = 0; l < K; ++l) {
         const int a = active ? A.leaf[l].off[row] : 0;
-        const int b = active ? A.leaf[l].off[row + 1] : 0;
+        const int b = active ? (A.leaf[l].off_end ? A.leaf[l].off_end[row] : A.leaf[l].off[row + 1]) : 0;
         s[l] = a;
         lim[l] = MODE == MODE_TABLE ? 2 * (b - a) : (b - a);
     }

@@ -1,0 +1,277 @@
+"""Morphology, multilevel sets and interval fields on the GPU.
+
+Interval outputs are compared bit for bit (begin, end, row_offsets, rows)
+with fixtures generated by the reference itself, and with the oracle on
+larger seeded inputs.  Float32 field values must match the reference's bit
+for bit; float64 values must match the FP64 oracle bit for bit (both follow
+the same operation order without contraction).
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from tests.golden_io import error, get_set, has, load
+from tests.gpu_util import assert_same, dev_set, host, iset, rand_set
+
+pytestmark = pytest.mark.gpu
+
+sc = pytest.importorskip("subsetix_b200.subsetix_cupy")
+
+MORPH = "morph.npz"
+ML = "multilevel.npz"
+STENCIL = "stencil_regrid.npz"
+
+
+def _cases(data, prefix):
+    return sorted({k.split("/")[0] for k in data if k.startswith(prefix) and k.split("/")[0][len(prefix):].isdigit()},
+                  key=lambda s: int(s[len(prefix):]))
+
+
+# ---------------------------------------------------------------- morphology
+
+def test_morphology_fixtures(cuda_device):
+    data = load(MORPH)
+    checked = 0
+    for case in _cases(data, "m"):
+        S = dev_set(get_set(data, f"{case}/S"))
+        for hx, hy in [(0, 0), (2, 0), (0, 1), (1, 1), (3, 2), (1, 4)]:
+            assert_same(sc.dilate_interval_set(S, halo_x=hx, halo_y=hy), get_set(data, f"{case}/dilate_{hx}_{hy}"),
+                        f"{case} dilate {hx},{hy}")
+            checked += 1
+        for w, h in [(8, 6), (16, 12), (1, 3)]:
+            assert_same(sc.clip_interval_set(S, width=w, height=h), get_set(data, f"{case}/clip_{w}_{h}"),
+                        f"{case} clip {w},{h}")
+            assert_same(sc.erode_interval_set(S, halo_x=1, halo_y=1, width=w, height=h),
+                        get_set(data, f"{case}/erode_{w}_{h}"), f"{case} erode {w},{h}")
+            assert_same(sc.ghost_zones(S, halo_x=1, halo_y=1, width=w, height=h),
+                        get_set(data, f"{case}/ghost_{w}_{h}"), f"{case} ghost {w},{h}")
+            checked += 3
+    assert checked >= 60 * 15
+
+
+def test_morphology_config1(cuda_device):
+    data = load(MORPH)
+    A = dev_set(get_set(data, "cfg1/A"))
+    for hx, hy in [(1, 1), (2, 2), (4, 4), (3, 0)]:
+        assert_same(sc.dilate_interval_set(A, halo_x=hx, halo_y=hy), get_set(data, f"cfg1/dilate_{hx}_{hy}"))
+        assert_same(sc.erode_interval_set(A, halo_x=hx, halo_y=hy, width=256, height=256),
+                    get_set(data, f"cfg1/erode_{hx}_{hy}"))
+
+
+@pytest.mark.parametrize("hx,hy", [(1, 1), (2, 4), (0, 6), (3, 9), (5, 0)])
+def test_dilate_random_against_oracle(cuda_device, hx, hy):
+    h = rand_set(2048, 40.0, seed=hx * 10 + hy, row_stride=3)
+    got = sc.dilate_interval_set(dev_set(h), halo_x=hx, halo_y=hy)
+    exp = O.dilate(iset(h), hx, hy)
+    assert_same(got, exp)
+
+
+def test_clip_erode_random_against_oracle(cuda_device):
+    h = rand_set(1024, 12.0, seed=5, row_stride=1, row0=-50)
+    S = dev_set(h)
+    W, H = 4000, 900
+    assert_same(sc.clip_interval_set(S, width=W, height=H), O.clip(iset(h), W, H))
+    assert_same(sc.erode_interval_set(S, 2, 1, width=W, height=H), O.erode(iset(h), 2, 1, width=W, height=H))
+    assert_same(sc.ghost_zones(S, 1, 2, width=W, height=H), O.ghost_zones(iset(h), 1, 2, width=W, height=H))
+
+
+def test_morphology_errors(cuda_device):
+    S = sc.build_interval_set(row_offsets=[0, 1], begin=[0], end=[3])
+    with pytest.raises(ValueError):
+        sc.dilate_interval_set(S, halo_x=-1)
+    with pytest.raises(ValueError):
+        sc.clip_interval_set(S, width=0, height=3)
+    with pytest.raises(ValueError):
+        sc.clip_interval_set(S, width=3, height=-1)
+    with pytest.raises(TypeError):
+        sc.translate_interval_set(S, dx=1.5)
+    with pytest.raises(ValueError):
+        sc.interior_for_direction(S, 0, 0)
+
+
+def _compact(s):
+    """Occupied rows with merged intervals (the reference's compaction)."""
+    return O.build_from_rows(O.interval_rows(s), s.begin, s.end)
+
+
+def _translate(s, dx, dy):
+    return O.ISet(s.begin + dx, s.end + dx, s.row_offsets.copy(), s.rows + dy)
+
+
+def test_translate_and_boundaries(cuda_device):
+    h = rand_set(256, 6.0, seed=9, row_stride=1)
+    S = dev_set(h)
+    s = iset(h)
+    t = sc.translate_interval_set(S, dx=3, dy=-2)
+    assert_same(t, _translate(s, 3, -2))
+    interior = _compact(O.intersection(s, _translate(s, -1, 0)))
+    assert_same(sc.interior_for_direction(S, 1, 0), interior)
+    assert_same(sc.boundary_for_direction(S, 1, 0), _compact(O.difference(s, interior)))
+    inner = s
+    for dx, dy in ((1, 0), (-1, 0), (0, 1), (0, -1)):
+        inner = O.intersection(inner, _translate(s, -dx, -dy))
+    assert_same(sc.boundary_layer(S), _compact(O.difference(s, _compact(inner))))
+
+
+# ---------------------------------------------------------------- multilevel sets
+
+def test_prolong_restrict_set_fixtures(cuda_device):
+    data = load(ML)
+    for case in _cases(data, "p"):
+        S = dev_set(get_set(data, f"{case}/S"))
+        for r in (1, 2, 3, 4):
+            assert_same(sc.prolong_set(S, r), get_set(data, f"{case}/prolong_{r}"), f"{case} prolong {r}")
+            assert_same(sc.restrict_set(S, r), get_set(data, f"{case}/restrict_{r}"), f"{case} restrict {r}")
+    S = sc.build_interval_set(row_offsets=[0, 1], begin=[0], end=[3])
+    assert sc.prolong_set(S, 1) is S
+
+
+@pytest.mark.parametrize("r", [2, 3, 4, 8, 12])
+def test_prolong_restrict_random_against_oracle(cuda_device, r):
+    h = rand_set(3000, 20.0, seed=r, row_stride=2)
+    S = dev_set(h)
+    assert_same(sc.prolong_set(S, r), O.prolong_set(iset(h), r))
+    assert_same(sc.restrict_set(S, r), O.restrict_set(iset(h), r))
+    # restrict(prolong(S)) is S with touching intervals merged
+    assert_same(sc.restrict_set(sc.prolong_set(S, r), r), O.restrict_set(O.prolong_set(iset(h), r), r))
+
+
+# ---------------------------------------------------------------- fields
+
+def _field(h, values, dtype=torch.float32):
+    S = dev_set(h)
+    f = sc.create_interval_field(S, fill_value=0.0, dtype=np.float32 if dtype == torch.float32 else np.float64)
+    f.values.copy_(torch.as_tensor(np.asarray(values), device="cuda").to(dtype))
+    return f
+
+
+def _vals(x):
+    return torch.as_tensor(x).cpu().numpy()
+
+
+def test_field_fixtures(cuda_device):
+    data = load(ML)
+    n_fine = n_err = 0
+    for case in _cases(data, "f"):
+        h = get_set(data, f"{case}/S")
+        f = _field(h, data[f"{case}/values"])
+        for r in (2, 3):
+            err = error(data, f"{case}/fine_{r}")
+            if err is not None:
+                with pytest.raises(ValueError):
+                    sc.prolong_field(f, r)
+                n_err += 1
+                continue
+            fine = sc.prolong_field(f, r)
+            assert_same(fine.interval_set, get_set(data, f"{case}/fine_{r}"))
+            np.testing.assert_array_equal(_vals(fine.values), data[f"{case}/fine_{r}/values"])
+            noisy = sc.IntervalField(interval_set=fine.interval_set,
+                                     values=torch.as_tensor(data[f"{case}/noisy_{r}"], device="cuda"),
+                                     interval_cell_offsets=fine.interval_cell_offsets)
+            for red in ("mean", "sum", "min", "max"):
+                key = f"{case}/restrict_{r}_{red}"
+                if error(data, key) is not None:
+                    with pytest.raises(ValueError):
+                        sc.restrict_field(noisy, r, reducer=red)
+                    continue
+                out = sc.restrict_field(noisy, r, reducer=red)
+                assert_same(out.interval_set, get_set(data, key))
+                assert out.values.dtype == torch.float32
+                np.testing.assert_array_equal(_vals(out.values), data[f"{key}/values"], err_msg=key)
+            n_fine += 1
+    assert n_fine >= 20 and n_err >= 1
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+def test_field_random_against_oracle(cuda_device, dtype):
+    rng = np.random.default_rng(3)
+    h = rand_set(1500, 10.0, seed=11, row_stride=1, min_per_row=1)
+    npd = np.float32 if dtype == torch.float32 else np.float64
+    s = iset(h)
+    cf = O.create_field(s, 0.0, npd)
+    cf.values[...] = rng.standard_normal(cf.values.size).astype(npd)
+    f = _field(h, cf.values, dtype)
+    for r in (2, 4):
+        fine = sc.prolong_field(f, r, dtype=npd)
+        exp = O.prolong_field(cf, r, dtype=npd)
+        assert_same(fine.interval_set, exp.iset)
+        np.testing.assert_array_equal(_vals(fine.values), exp.values)
+        noisy_vals = rng.standard_normal(exp.values.size).astype(npd)
+        noisy = sc.IntervalField(interval_set=fine.interval_set, values=torch.as_tensor(noisy_vals, device="cuda"),
+                                 interval_cell_offsets=fine.interval_cell_offsets)
+        for red in ("mean", "sum", "min", "max"):
+            got = sc.restrict_field(noisy, r, reducer=red, dtype=npd)
+            want = O.restrict_field(O.Field(exp.iset, noisy_vals, exp.offsets), r, red, dtype=npd)
+            assert_same(got.interval_set, want.iset)
+            np.testing.assert_array_equal(_vals(got.values), want.values, err_msg=red)
+
+
+def test_restrict_field_misaligned_raises(cuda_device):
+    h = rand_set(64, 3.0, seed=2, row_stride=1, min_per_row=1)
+    f = _field(h, np.ones(int(np.sum(h[1] - h[0])), np.float32))
+    with pytest.raises(ValueError):
+        sc.restrict_field(f, 2)
+    with pytest.raises(NameError):
+        sc.restrict_field(f, 1)
+
+
+def test_cell_access(cuda_device):
+    S = sc.build_interval_set(row_offsets=[0, 2, 3], begin=[0, 6, 1], end=[4, 9, 5])
+    f = sc.create_interval_field(S, fill_value=1.5, dtype=np.float32)
+    assert f.cell_count == 11
+    assert sc.set_cell(f, 0, 7, 4.0)
+    assert not sc.set_cell(f, 0, 5, 4.0)
+    assert float(sc.get_cell(f, 0, 7)) == 4.0
+    assert sc.get_cell(f, 1, 0) is None
+    with pytest.raises(IndexError):
+        sc.get_cell(f, 5, 0)
+    rows = torch.tensor([0, 0, 1, 1, 2, -1], dtype=torch.int32, device="cuda")
+    cols = torch.tensor([3, 4, 4, 5, 0, 0], dtype=torch.int32, device="cuda")
+    idx = sc.locate_interval_cells(f, rows, cols)
+    assert idx.cpu().tolist() == [0, -1, 2, -1, -1, -1]
+
+
+# ---------------------------------------------------------------- upwind
+
+def test_upwind_fixtures(cuda_device):
+    data = load(STENCIL)
+    cases = _cases(data, "u")
+    assert len(cases) == 15
+    for case in cases:
+        h = get_set(data, f"{case}/S")
+        f = _field(h, data[f"{case}/values"])
+        width, height, a, b, dt, dx, dy = data[f"{case}/params"].tolist()
+        out = sc.step_upwind_interval(f, width=int(width), height=int(height), a=a, b=b, dt=dt, dx=dx, dy=dy)
+        np.testing.assert_array_equal(_vals(out), data[f"{case}/out"], err_msg=case)
+        buf = torch.empty_like(f.values)
+        res = sc.step_upwind_interval(f, width=int(width), height=int(height), a=a, b=b, dt=dt, dx=dx, dy=dy, out=buf)
+        assert res is buf
+        np.testing.assert_array_equal(_vals(buf), data[f"{case}/out"])
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+def test_upwind_random_against_oracle(cuda_device, dtype):
+    npd = np.float32 if dtype == torch.float32 else np.float64
+    rng = np.random.default_rng(7)
+    W = H = 1024
+    for seed, touching in ((1, False), (2, True)):
+        h = rand_set(H, 30.0, seed=seed, row_stride=1, max_col=W, touching=touching, row0=0)
+        s = iset(h)
+        cf = O.create_field(s, 0.0, npd)
+        cf.values[...] = rng.uniform(0, 1, cf.values.size).astype(npd)
+        f = _field(h, cf.values, dtype)
+        for a, b in ((1.0, 0.5), (-0.3, -0.8)):
+            got = sc.step_upwind_interval(f, width=W, height=H, a=a, b=b, dt=0.2 / W, dx=1.0 / W, dy=1.0 / H)
+            exp = O.upwind(cf, width=W, height=H, a=a, b=b, dt=0.2 / W, dx=1.0 / W, dy=1.0 / H, dtype=npd)
+            np.testing.assert_array_equal(_vals(got), exp)
+
+
+def test_upwind_rows_out_of_range(cuda_device):
+    S = sc.build_interval_set(row_offsets=[0, 1, 2], begin=[0, 0], end=[2, 2], rows=[0, 5])
+    f = sc.create_interval_field(S, fill_value=1.0, dtype=np.float32)
+    with pytest.raises(ValueError):
+        sc.step_upwind_interval(f, width=4, height=4, a=1.0, b=1.0, dt=0.1, dx=1.0, dy=1.0)
+    with pytest.raises(ValueError):
+        sc.step_upwind_interval(f, width=0, height=4, a=1.0, b=1.0, dt=0.1, dx=1.0, dy=1.0)
