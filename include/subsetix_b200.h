@@ -331,6 +331,8 @@ int sx_upwind_f64(const int32_t* rows, const int32_t* row_offsets, int32_t row_c
  * (exclusive scan of counts), out_begin/out_end written. */
 int sx_threshold_rle(const float* values, int32_t width, int32_t height, float threshold, int gradient, int32_t* counts,
                      const int32_t* offsets, int32_t* out_begin, int32_t* out_end, void* stream);
+/* Gradient magnitude of a full grid, same formula (regrid.py:172-274, K14). */
+int sx_gradient_magnitude(const float* values, int32_t width, int32_t height, float* out, void* stream);
 int sx_gradient_threshold_rle(const float* values, int32_t width, int32_t height, float threshold, int32_t* counts,
                               const int32_t* offsets, int32_t* out_begin, int32_t* out_end, void* stream);
 
@@ -339,6 +341,24 @@ int sx_gradient_threshold_rle(const float* values, int32_t width, int32_t height
 int sx_locate_cells(const int32_t* rows, const int32_t* row_offsets, const int32_t* begin, const int32_t* end,
                     int32_t row_count, const int32_t* query_rows, const int32_t* query_cols, int64_t count,
                     int32_t* out, void* stream);
+
+/* Runs of cells whose value equals *target (host pointer to one value of
+ * the field's type), per interval; runs never cross intervals
+ * (subsetix_amr2/fields.py:39-100).  Count pass (out_begin NULL): counts[n]
+ * runs per interval.  Write pass: run_offsets[n] (exclusive scan of the
+ * counts) and the intervals' begins give [begin + first, begin + last + 1).
+ * Types: SX_VALUE_F32, F64, I8 (also uint8 and bool), I32, I64. */
+#define SX_VALUE_F32 0
+#define SX_VALUE_F64 1
+#define SX_VALUE_I8 2
+#define SX_VALUE_I32 3
+#define SX_VALUE_I64 4
+int sx_value_runs(int type, const void* values, const int32_t* cell_offsets, int64_t n, const void* target,
+                  int32_t* counts, const int32_t* run_offsets, const int32_t* begin, int32_t* out_begin,
+                  int32_t* out_end, void* stream);
+
+/* dst[p] = src[index[p]] for p < count (row offsets of derived sets). */
+int sx_gather_i32(const int32_t* index, int32_t count, const int32_t* src, int32_t* dst, void* stream);
 
 /* Compensated (Neumaier) FP64 sum of n values times `scale`, in a fixed
  * order (deterministic).  partials: 2 * parts doubles of scratch, parts in

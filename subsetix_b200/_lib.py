@@ -105,10 +105,14 @@ _SIGNATURES = {
                                      c_vp]),
     "sx_threshold_rle": (ctypes.c_int, [c_vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_float, ctypes.c_int, c_vp,
                                         c_vp, c_vp, c_vp, c_vp]),
+    "sx_gradient_magnitude": (ctypes.c_int, [c_vp, ctypes.c_int32, ctypes.c_int32, c_vp, c_vp]),
     "sx_gradient_threshold_rle": (ctypes.c_int, [c_vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_float, c_vp, c_vp,
                                                  c_vp, c_vp, c_vp]),
     "sx_locate_cells": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, ctypes.c_int32, c_vp, c_vp, ctypes.c_int64, c_vp,
                                        c_vp]),
+    "sx_value_runs": (ctypes.c_int, [ctypes.c_int, c_vp, c_vp, ctypes.c_int64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
+                                     c_vp]),
+    "sx_gather_i32": (ctypes.c_int, [c_vp, ctypes.c_int32, c_vp, c_vp, c_vp]),
     "sx_mass_integral": (ctypes.c_int, [ctypes.c_int, c_vp, ctypes.c_int64, ctypes.c_double, c_vp, ctypes.c_int, c_vp,
                                         c_vp]),
     "sx_mass_integral_f64": (ctypes.c_int, [c_vp, ctypes.c_int64, ctypes.c_double, c_vp, ctypes.c_int, c_vp, c_vp]),

@@ -477,6 +477,16 @@ int sx_threshold_rle(const float* values, int32_t width, int32_t height, float t
     return SX_OK;
 }
 
+int sx_gradient_magnitude(const float* values, int32_t width, int32_t height, float* out, void* stream)
+{
+    if (width <= 0 || height <= 0) return fail(SX_ERR_INVALID, "sx_gradient_magnitude: width and height must be positive");
+    if ((long long)width * height > INT32_MAX) return fail(SX_ERR_INVALID, "sx_gradient_magnitude: grid too large");
+    if (!values || !out) return fail(SX_ERR_INVALID, "sx_gradient_magnitude: null argument");
+    cudaError_t err = sx_gradient_launch(values, width, height, out, (cudaStream_t)stream);
+    if (err != cudaSuccess) return cuda_fail(err, "sx_gradient_magnitude");
+    return SX_OK;
+}
+
 int sx_gradient_threshold_rle(const float* values, int32_t width, int32_t height, float threshold, int32_t* counts,
                               const int32_t* offsets, int32_t* out_begin, int32_t* out_end, void* stream)
 {
@@ -494,6 +504,33 @@ int sx_locate_cells(const int32_t* rows, const int32_t* row_offsets, const int32
     cudaError_t err = sx_locate_cells_launch(rows, row_offsets, begin, end, row_count, query_rows, query_cols, count,
                                              out, (cudaStream_t)stream);
     if (err != cudaSuccess) return cuda_fail(err, "sx_locate_cells");
+    return SX_OK;
+}
+
+int sx_value_runs(int type, const void* values, const int32_t* cell_offsets, int64_t n, const void* target,
+                  int32_t* counts, const int32_t* run_offsets, const int32_t* begin, int32_t* out_begin,
+                  int32_t* out_end, void* stream)
+{
+    if (type < SX_VALUE_F32 || type > SX_VALUE_I64) return fail(SX_ERR_INVALID, "sx_value_runs: type %d", type);
+    if (n < 0 || n > INT32_MAX) return fail(SX_ERR_INVALID, "sx_value_runs: bad size");
+    if (!target) return fail(SX_ERR_INVALID, "sx_value_runs: null target");
+    if (n == 0) return SX_OK;
+    if (!cell_offsets || (!out_begin && !counts)) return fail(SX_ERR_INVALID, "sx_value_runs: null argument");
+    if (out_begin && (!out_end || !run_offsets || !begin))
+        return fail(SX_ERR_INVALID, "sx_value_runs: write mode needs run offsets and begins");
+    cudaError_t err = sx_value_runs_launch(type, values, cell_offsets, (int)n, target, out_begin ? nullptr : counts,
+                                           run_offsets, begin, out_begin, out_end, (cudaStream_t)stream);
+    if (err != cudaSuccess) return cuda_fail(err, "sx_value_runs");
+    return SX_OK;
+}
+
+int sx_gather_i32(const int32_t* index, int32_t count, const int32_t* src, int32_t* dst, void* stream)
+{
+    if (count < 0) return fail(SX_ERR_INVALID, "sx_gather_i32: negative count");
+    if (count == 0) return SX_OK;
+    if (!index || !src || !dst) return fail(SX_ERR_INVALID, "sx_gather_i32: null argument");
+    cudaError_t err = sx_gather_i32_launch(index, count, src, dst, (cudaStream_t)stream);
+    if (err != cudaSuccess) return cuda_fail(err, "sx_gather_i32");
     return SX_OK;
 }
 

@@ -628,6 +628,131 @@ cudaError_t sx_locate_cells_launch(const int* rows, const int* off, const int* b
 }
 
 // ---------------------------------------------------------------------------
+// Runs of cells equal to a target value, per interval
+// (subsetix_amr2/fields.py:39-100).  Runs never cross an interval boundary.
+// One warp per interval, 32 cells per step with a ballot, as in the
+// threshold RLE.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void sx_value_runs_kernel(const T* __restrict__ v, const int* __restrict__ coff, int n, T target,
+                                     int* __restrict__ counts, const int* __restrict__ run_off,
+                                     const int* __restrict__ b, int* __restrict__ ob, int* __restrict__ oe)
+{
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
+        const int c0 = coff[i];
+        const int w = coff[i + 1] - c0;
+        const int base_out = ob ? run_off[i] : 0;
+        const int x0 = ob ? b[i] : 0;
+        unsigned prev = 0u;
+        int k = 0;
+        for (int base = 0; base < w; base += 32) {
+            const int t = base + lane;
+            const bool on = t < w && v[c0 + t] == target;
+            const unsigned m = __ballot_sync(0xFFFFFFFFu, on);
+            const unsigned valid = (w - base >= 32) ? 0xFFFFFFFFu : ((1u << (w - base)) - 1u);
+            const unsigned starts = m & ~((m << 1) | prev);
+            const unsigned stops = ((m << 1) | prev) & ~m & valid;
+            if (ob) {
+                const unsigned below = (1u << lane) - 1u;
+                if ((starts >> lane) & 1u) ob[base_out + k + __popc(starts & below)] = x0 + t;
+                if ((stops >> lane) & 1u) oe[base_out + k + __popc(starts & below) - 1] = x0 + t;
+            }
+            k += __popc(starts);
+            prev = (w - base >= 32) ? (m >> 31) & 1u : (m >> (w - base - 1)) & 1u;
+        }
+        if (ob && prev && lane == 0) oe[base_out + k - 1] = x0 + w;
+        if (counts && lane == 0) counts[i] = w > 0 ? k : 0;
+    }
+}
+
+__global__ void sx_gather_i32_kernel(const int* __restrict__ idx, int count, const int* __restrict__ src,
+                                     int* __restrict__ dst)
+{
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < count; p += gridDim.x * blockDim.x) dst[p] = src[idx[p]];
+}
+
+cudaError_t sx_value_runs_launch(int type, const void* v, const int* coff, int n, const void* target, int* counts,
+                                 const int* run_off, const int* b, int* ob, int* oe, cudaStream_t stream)
+{
+    if (n <= 0) return cudaSuccess;
+    long long g = ((long long)n * 32 + 255) / 256;
+    if (g > 148 * 64) g = 148 * 64;
+    const int grid = (int)g;
+    switch (type) {
+        case 0:
+            sx_value_runs_kernel<float><<<grid, 256, 0, stream>>>((const float*)v, coff, n, *(const float*)target,
+                                                                  counts, run_off, b, ob, oe);
+            break;
+        case 1:
+            sx_value_runs_kernel<double><<<grid, 256, 0, stream>>>((const double*)v, coff, n, *(const double*)target,
+                                                                   counts, run_off, b, ob, oe);
+            break;
+        case 2:
+            sx_value_runs_kernel<signed char><<<grid, 256, 0, stream>>>((const signed char*)v, coff, n,
+                                                                        *(const signed char*)target, counts, run_off,
+                                                                        b, ob, oe);
+            break;
+        case 3:
+            sx_value_runs_kernel<int><<<grid, 256, 0, stream>>>((const int*)v, coff, n, *(const int*)target, counts,
+                                                                run_off, b, ob, oe);
+            break;
+        case 4:
+            sx_value_runs_kernel<long long><<<grid, 256, 0, stream>>>((const long long*)v, coff, n,
+                                                                      *(const long long*)target, counts, run_off, b,
+                                                                      ob, oe);
+            break;
+        default:
+            return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t sx_gather_i32_launch(const int* idx, int count, const int* src, int* dst, cudaStream_t stream)
+{
+    if (count <= 0) return cudaSuccess;
+    long long g = (count + 255) / 256;
+    if (g > 148 * 64) g = 148 * 64;
+    sx_gather_i32_kernel<<<(int)g, 256, 0, stream>>>(idx, count, src, dst);
+    return cudaGetLastError();
+}
+
+// Gradient magnitude of a full width x height grid into a float32 array
+// (regrid.py:172-274); the same per-cell formula as the fused RLE.
+__global__ void sx_gradient_kernel(const float* __restrict__ d, int width, int height, float* __restrict__ out)
+{
+    const long long cells = (long long)width * height;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < cells;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int y = (int)(idx / width), x = (int)(idx - (long long)y * width);
+        const float c = d[idx];
+        float gx = 0.0f, gy = 0.0f;
+        if (width > 1) {
+            if (x == 0) gx = __fsub_rn(d[idx + 1], c);
+            else if (x == width - 1) gx = __fsub_rn(c, d[idx - 1]);
+            else gx = __fmul_rn(__fsub_rn(d[idx + 1], d[idx - 1]), 0.5f);
+        }
+        if (height > 1) {
+            if (y == 0) gy = __fsub_rn(d[idx + width], c);
+            else if (y == height - 1) gy = __fsub_rn(c, d[idx - width]);
+            else gy = __fmul_rn(__fsub_rn(d[idx + width], d[idx - width]), 0.5f);
+        }
+        out[idx] = __fsqrt_rn(__fadd_rn(__fmul_rn(gx, gx), __fmul_rn(gy, gy)));
+    }
+}
+
+cudaError_t sx_gradient_launch(const float* d, int width, int height, float* out, cudaStream_t stream)
+{
+    const long long cells = (long long)width * height;
+    if (cells <= 0) return cudaSuccess;
+    long long g = (cells + 255) / 256;
+    if (g > 148 * 32) g = 148 * 32;
+    sx_gradient_kernel<<<(int)g, 256, 0, stream>>>(d, width, height, out);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 // Host launchers
 // ---------------------------------------------------------------------------
 static int sx_grid(long long work, int block, int cap = 65535 * 8)

@@ -110,3 +110,7 @@ cudaError_t sx_mass_launch(const void* v, long long n, int dbl, double scale, do
                            cudaStream_t stream);
 cudaError_t sx_locate_cells_launch(const int* rows, const int* off, const int* b, const int* e, int row_count,
                                    const int* qr, const int* qc, long long q, int* out, cudaStream_t stream);
+cudaError_t sx_value_runs_launch(int type, const void* v, const int* coff, int n, const void* target, int* counts,
+                                 const int* run_off, const int* b, int* ob, int* oe, cudaStream_t stream);
+cudaError_t sx_gather_i32_launch(const int* idx, int count, const int* src, int* dst, cudaStream_t stream);
+cudaError_t sx_gradient_launch(const float* d, int width, int height, float* out, cudaStream_t stream);
