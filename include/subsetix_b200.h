@@ -91,9 +91,11 @@ typedef struct sx_leaf {
 } sx_leaf;
 
 /* Launch tuning for sx_bool_eval; NULL or zero fields select automatic values.
- * kernel: 1 = global-memory sweep, 2 = shared-memory staged sweep (table mode);
- * blocks_per_sm: residency cap of the global sweep; staging_cap: elements per
- * warp of the staged sweep.  Results never depend on the tuning. */
+ * kernel: 1 = global-memory sweep, 2 = shared-memory staged sweep, 3 =
+ * merge-path tile kernel (table mode; the default); blocks_per_sm: residency
+ * cap of the global sweep; staging_cap: elements per warp of the staged
+ * sweep, or keys per tile of the merge-path kernel.  Results never depend on
+ * the tuning. */
 typedef struct sx_tuning {
     int32_t kernel;
     int32_t blocks_per_sm;

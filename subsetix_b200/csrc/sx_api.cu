@@ -93,7 +93,7 @@ int sx_bool_eval(const sx_leaf* leaves, int k, int32_t rows, const uint32_t* tab
     A.capacity = capacity;
     A.result = result;
     if (tuning) {
-        if (tuning->kernel < 0 || tuning->kernel > 2 || tuning->blocks_per_sm < 0 || tuning->staging_cap < 0)
+        if (tuning->kernel < 0 || tuning->kernel > 3 || tuning->blocks_per_sm < 0 || tuning->staging_cap < 0)
             return fail(SX_ERR_INVALID, "sx_bool_eval: bad tuning");
         A.tune_kernel = tuning->kernel;
         A.tune_blocks_per_sm = tuning->blocks_per_sm;

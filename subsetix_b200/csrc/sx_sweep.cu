@@ -582,6 +582,477 @@ __global__ void __launch_bounds__(32 * SX_SMEM_WARPS) sx_sweep_smem_kernel(SxBoo
 
 static size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+// ---------------------------------------------------------------------------
+// Merge-path form of the table sweep (the main path for set algebra).
+//
+// A block of SXM_THREADS threads owns one tile of 32 aligned rows.  Every
+// boundary of every leaf in the tile becomes a key (row, x, leaf) in shared
+// memory: 32 bits (row << 27 | (x - xmin) << 3 | leaf) when the tile's
+// coordinates span less than 2^24, else 64 bits (row << 40 | (x + 2^31) << 8
+// | leaf).  Each leaf's keys are already sorted (rows are consecutive and,
+// on canonical leaves, boundaries rise inside a row), so the tile's keys are
+// merged pairwise with balanced merge paths: every thread merges the same
+// number of keys, whatever the row lengths.  An exclusive XOR-scan of
+// (1 << leaf) over the merged keys gives the membership state after each
+// boundary.  At the last key of each (row, x) group, f(state) is compared
+// with f before the group; a change is an output boundary.  Output
+// boundaries alternate begin/end and never cross rows (every row ends with
+// all leaves outside, and f(0) = 0).
+//
+// One pass over the inputs: the output boundaries are kept in shared memory
+// while the block scans their count and the tile's global base comes from
+// the look-back, then they are written out.
+//
+// Contract: each leaf's boundaries must rise strictly inside a row
+// (non-empty, non-touching, sorted intervals); otherwise SXF_CONTRACT.  A
+// tile whose keys do not fit in shared memory is swept by its first warp
+// with the one-lane-per-row sweep above (same results, slower).
+// ---------------------------------------------------------------------------
+#define SXM_THREADS 256
+#define SXM_WARPS (SXM_THREADS / 32)
+#define SXM_TR 32
+
+template <typename KeyT>
+struct SxmKey;
+
+template <>
+struct SxmKey<unsigned> {
+    static constexpr unsigned MAX = 0xFFFFFFFFu;
+    __device__ static unsigned make(int r, int x, int l, int xmin)
+    {
+        return ((unsigned)r << 27) | ((unsigned)(x - xmin) << 3) | (unsigned)l;
+    }
+    __device__ static unsigned group(unsigned k) { return k >> 3; }
+    __device__ static int row(unsigned k) { return (int)(k >> 27); }
+    __device__ static int x(unsigned k, int xmin) { return xmin + (int)((k >> 3) & 0xFFFFFFu); }
+    __device__ static unsigned tag(unsigned k) { return k & 7u; }
+};
+
+template <>
+struct SxmKey<unsigned long long> {
+    static constexpr unsigned long long MAX = 0xFFFFFFFFFFFFFFFFull;
+    __device__ static unsigned long long make(int r, int x, int l, int)
+    {
+        return ((unsigned long long)r << 40) | ((unsigned long long)((unsigned)x ^ 0x80000000u) << 8) |
+               (unsigned long long)l;
+    }
+    __device__ static unsigned long long group(unsigned long long k) { return k >> 8; }
+    __device__ static int row(unsigned long long k) { return (int)(k >> 40); }
+    __device__ static int x(unsigned long long k, int) { return (int)((unsigned)(k >> 8) ^ 0x80000000u); }
+    __device__ static unsigned tag(unsigned long long k) { return (unsigned)(k & 7ull); }
+};
+
+// Block-wide exclusive sum (all SXM_THREADS threads call it).
+__device__ __forceinline__ int sxm_block_excl_sum(int v, int* s_warp, int* total)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_warp[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        const int w = lane < SXM_WARPS ? s_warp[lane] : 0;
+        int wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xFFFFFFFFu, wi, o);
+            if (lane >= o) wi += y;
+        }
+        if (lane < SXM_WARPS) s_warp[lane] = wi - w;
+        if (lane == SXM_WARPS - 1) s_warp[SXM_WARPS] = wi;
+    }
+    __syncthreads();
+    const int r = s_warp[wid] + incl - v;
+    *total = s_warp[SXM_WARPS];
+    __syncthreads();
+    return r;
+}
+
+// Block-wide exclusive XOR scan.
+__device__ __forceinline__ unsigned sxm_block_excl_xor(unsigned v, int* s_warp)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    unsigned incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= o) incl ^= y;
+    }
+    if (lane == 31) s_warp[wid] = (int)incl;
+    __syncthreads();
+    if (wid == 0) {
+        const unsigned w = lane < SXM_WARPS ? (unsigned)s_warp[lane] : 0u;
+        unsigned wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(0xFFFFFFFFu, wi, o);
+            if (lane >= o) wi ^= y;
+        }
+        if (lane < SXM_WARPS) s_warp[lane] = (int)(wi ^ w);
+    }
+    __syncthreads();
+    const unsigned r = (unsigned)s_warp[wid] ^ incl ^ v;
+    __syncthreads();
+    return r;
+}
+
+struct SxmTile {
+    int off[SX_TABLE_MAX_LEAVES][SXM_TR + 1];
+    const int* lb[SX_TABLE_MAX_LEAVES];
+    const int* le[SX_TABLE_MAX_LEAVES];
+    int ls[SX_TABLE_MAX_LEAVES], ll[SX_TABLE_MAX_LEAVES], lbuf[SX_TABLE_MAX_LEAVES];
+    int nl;
+    int warp[SXM_WARPS + 1];
+    unsigned tab[8];
+    int rowcnt[SXM_TR];
+    int xmin, xmax;
+    int tile, base;
+    unsigned flags;
+};
+
+// Keys, merges and output boundaries of one tile with key type KeyT.
+// Returns the number of output boundaries of this thread; they are left in
+// `emits` (this thread's slots [c0, c0 + n)); *excl receives this thread's
+// exclusive position among the tile's output boundaries and *total the
+// tile's count.  All threads of the block call it.
+// Key buffers per tile: two, or three for K = 3, 6, 7, where the merge tree
+// (odd lists stay in place) would otherwise read and write one buffer.
+template <int K>
+struct SxmBuffers {
+    static constexpr int n = (K == 3 || K == 6 || K == 7) ? 3 : 2;
+};
+
+template <int K, typename KeyT>
+__device__ __forceinline__ int sxm_tile(SxmTile& S, unsigned char* smem, int cap_bytes, int nrows, int T,
+                                        const int* start, const int* len, unsigned& bad, KeyT*& emits, int& c0,
+                                        int* excl, int* total)
+{
+    using Key = SxmKey<KeyT>;
+    constexpr int NB = SxmBuffers<K>::n;
+    const int tid = threadIdx.x;
+    const int capk = cap_bytes / (NB * (int)sizeof(KeyT));
+    KeyT* buf[NB];
+#pragma unroll
+    for (int q = 0; q < NB; ++q) buf[q] = (KeyT*)smem + q * capk;
+    const int xmin = S.xmin;
+    const int nint = T >> 1;
+    // 1a. row of every interval of the tile, one byte each (in buffer 1)
+    unsigned char* rowmap = (unsigned char*)buf[1];
+    for (int t = tid; t < K * nrows; t += SXM_THREADS) {
+        const int l = t / nrows, r = t - l * nrows;
+        int sl = 0;
+#pragma unroll
+        for (int q = 1; q < K; ++q)
+            if (l == q) sl = start[q];
+        const int o0 = S.off[l][0];
+        for (int g = S.off[l][r]; g < S.off[l][r + 1]; ++g) rowmap[(sl >> 1) + g - o0] = (unsigned char)r;
+    }
+    __syncthreads();
+    // 1b. keys, one thread per interval: list l's keys sit at [start[l], start[l] + len[l])
+    for (int e = tid; e < nint; e += SXM_THREADS) {
+        int l = 0, sl = 0, el = len[0];
+#pragma unroll
+        for (int q = 1; q < K; ++q)
+            if (2 * e >= start[q]) {
+                l = q;
+                sl = start[q];
+                el = start[q] + len[q];
+            }
+        const int g = S.off[l][0] + e - (sl >> 1);
+        const int r = rowmap[e];
+        const int b = __ldg(S.lb[l] + g), en = __ldg(S.le[l] + g);
+        bool ok = b < en;
+        if (2 * e + 2 < el && rowmap[e + 1] == r) ok = ok && en < __ldg(S.lb[l] + g + 1);
+        if (!ok) bad = 1u;
+        buf[0][2 * e] = Key::make(r, b, l, xmin);
+        buf[0][2 * e + 1] = Key::make(r, en, l, xmin);
+    }
+    if (tid == 0) {
+#pragma unroll
+        for (int l = 0; l < K; ++l) {
+            S.ls[l] = start[l];
+            S.ll[l] = len[l];
+            S.lbuf[l] = 0;
+        }
+        S.nl = K;
+    }
+    __syncthreads();
+    // 2. pairwise merges; a list without a partner stays where it is
+    c0 = (int)(((long long)T * tid) / SXM_THREADS);
+    const int c1 = (int)(((long long)T * (tid + 1)) / SXM_THREADS);
+    while (S.nl > 1) {
+        const int nl = S.nl;
+        const int np = nl >> 1;  // merged pairs; list nl-1 waits when nl is odd
+        const int M = S.ls[2 * np - 1] + S.ll[2 * np - 1];  // pairs cover [0, M)
+        const int m0 = (int)(((long long)M * tid) / SXM_THREADS);
+        const int m1 = (int)(((long long)M * (tid + 1)) / SXM_THREADS);
+        int k = m0;
+        int p = 0;
+        while (k < m1) {
+            while (p + 1 < np && k >= S.ls[2 * (p + 1)]) ++p;
+            const int a0 = S.ls[2 * p], la = S.ll[2 * p], lb = S.ll[2 * p + 1];
+            const int ba = S.lbuf[2 * p], bb = S.lbuf[2 * p + 1];
+            const int bo = (ba != 0 && bb != 0) ? 0 : ((ba != 1 && bb != 1) ? 1 : 2);
+            const KeyT* A_ = buf[0];
+            const KeyT* B_ = buf[0];
+            KeyT* D_ = buf[0];
+#pragma unroll
+            for (int q = 1; q < NB; ++q) {
+                if (ba == q) A_ = buf[q];
+                if (bb == q) B_ = buf[q];
+                if (bo == q) D_ = buf[q];
+            }
+            const int b0 = a0 + la;
+            const int pend = min(m1, a0 + la + lb);
+            const int d = k - a0;
+            int lo = max(0, d - lb), hi = min(d, la);
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (A_[a0 + mid] < B_[b0 + d - 1 - mid]) lo = mid + 1; else hi = mid;
+            }
+            int i = lo, j = d - lo;
+            KeyT ka = i < la ? A_[a0 + i] : Key::MAX;
+            KeyT kb = j < lb ? B_[b0 + j] : Key::MAX;
+            for (; k < pend; ++k) {
+                const bool ta = ka < kb;
+                D_[k] = ta ? ka : kb;
+                if (ta) {
+                    ++i;
+                    ka = i < la ? A_[a0 + i] : Key::MAX;
+                } else {
+                    ++j;
+                    kb = j < lb ? B_[b0 + j] : Key::MAX;
+                }
+            }
+        }
+        __syncthreads();
+        if (tid == 0) {
+            for (int q = 0; q < np; ++q) {
+                const int ba = S.lbuf[2 * q], bb = S.lbuf[2 * q + 1];
+                S.ls[q] = S.ls[2 * q];
+                S.ll[q] = S.ll[2 * q] + S.ll[2 * q + 1];
+                S.lbuf[q] = (ba != 0 && bb != 0) ? 0 : ((ba != 1 && bb != 1) ? 1 : 2);
+            }
+            if (nl & 1) {
+                S.ls[np] = S.ls[nl - 1];
+                S.ll[np] = S.ll[nl - 1];
+                S.lbuf[np] = S.lbuf[nl - 1];
+            }
+            S.nl = np + (nl & 1);
+        }
+        __syncthreads();
+    }
+    const int mb = S.lbuf[0];
+    const KeyT* m = buf[0];
+    emits = buf[1];
+#pragma unroll
+    for (int q = 1; q < NB; ++q)
+        if (mb == q) m = buf[q];
+    if (mb == 1) emits = buf[0];
+    // 3. states: XOR of (1 << leaf) before this thread's chunk
+    unsigned x = 0u;
+    for (int i = c0; i < c1; ++i) x ^= 1u << Key::tag(m[i]);
+    unsigned s = sxm_block_excl_xor(x, S.warp);
+    // 4. output boundaries of the chunk, kept in `emits` at [c0, c0 + n)
+    int n = 0;
+    if (c0 < c1) {
+        unsigned gstate = s;  // state before the (row, x) group holding c0
+        {
+            const KeyT g = Key::group(m[c0]);
+            int gs = c0;
+            while (gs > 0 && Key::group(m[gs - 1]) == g) {
+                --gs;
+                gstate ^= 1u << Key::tag(m[gs]);
+            }
+        }
+        bool fprev = (S.tab[gstate >> 5] >> (gstate & 31u)) & 1u;
+        KeyT cur = m[c0];
+        for (int i = c0; i < c1; ++i) {
+            const KeyT nxt = (i + 1 < T) ? m[i + 1] : Key::MAX;
+            s ^= 1u << Key::tag(cur);
+            if (Key::group(nxt) != Key::group(cur)) {
+                const bool fa = (S.tab[s >> 5] >> (s & 31u)) & 1u;
+                if (fa != fprev) {
+                    emits[c0 + n] = cur;
+                    ++n;
+                    if (fa) atomicAdd(&S.rowcnt[Key::row(cur)], 1);
+                    fprev = fa;
+                }
+            }
+            cur = nxt;
+        }
+    }
+    *excl = sxm_block_excl_sum(n, S.warp, total);
+    return n;
+}
+
+template <int K, typename KeyT>
+__device__ __forceinline__ void sxm_write(const SxBoolArgs& A, const SxmTile& S, const KeyT* emits, int c0, int n,
+                                          int excl, int base, bool& over)
+{
+    using Key = SxmKey<KeyT>;
+    const long long cap = A.capacity;
+    for (int q = 0; q < n; ++q) {
+        const KeyT key = emits[c0 + q];
+        const int p = excl + q;
+        const long long o = (long long)base + (p >> 1);
+        if (o < cap) {
+            if (p & 1) A.out_end[o] = Key::x(key, S.xmin); else A.out_begin[o] = Key::x(key, S.xmin);
+        } else {
+            over = true;
+        }
+    }
+}
+
+template <int K>
+__global__ void __launch_bounds__(SXM_THREADS) sx_merge_kernel(SxBoolArgs A, SxSweepState st, int tiles,
+                                                                 int cap_bytes)
+{
+    extern __shared__ __align__(16) unsigned char sxm_smem[];
+    __shared__ SxmTile S;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    if (tid == 0) {
+        S.tile = (int)atomicAdd(&st.counters[0], 1u);
+        S.flags = 0u;
+        S.xmin = INT_MAX;
+        S.xmax = INT_MIN;
+    }
+    if (tid < 8) S.tab[tid] = A.table[tid];
+    if (tid < SXM_TR) S.rowcnt[tid] = 0;
+    if (tid < K) {
+        S.lb[tid] = A.leaf[tid].begin;
+        S.le[tid] = A.leaf[tid].end;
+    }
+    __syncthreads();
+    const int tile = S.tile;
+    const int r0 = tile * SXM_TR;
+    const int nrows = min(SXM_TR, A.rows - r0);
+    for (int t = tid; t < K * (nrows + 1); t += SXM_THREADS) {
+        const int l = t / (nrows + 1), r = t - l * (nrows + 1);
+        S.off[l][r] = A.leaf[l].off[r0 + r];
+    }
+    __syncthreads();
+    // coordinate span of the tile: first begin and last end of every leaf row
+    for (int t = tid; t < K * nrows; t += SXM_THREADS) {
+        const int l = t / nrows, r = t - l * nrows;
+        const int g0 = S.off[l][r], g1 = S.off[l][r + 1];
+        if (g1 > g0) {
+            atomicMin(&S.xmin, min(__ldg(S.lb[l] + g0), __ldg(S.le[l] + g0)));
+            atomicMax(&S.xmax, max(__ldg(S.le[l] + g1 - 1), __ldg(S.lb[l] + g1 - 1)));
+        }
+    }
+    int len[K], start[K];
+    int T = 0;
+#pragma unroll
+    for (int l = 0; l < K; ++l) {
+        len[l] = 2 * (S.off[l][nrows] - S.off[l][0]);
+        start[l] = T;
+        T += len[l];
+    }
+    __syncthreads();
+    const bool narrow = (long long)S.xmax - (long long)S.xmin < (1ll << 24);
+    constexpr int NB = SxmBuffers<K>::n;
+    const int mode = (narrow && 4ll * NB * T <= cap_bytes) ? 1 : ((8ll * NB * T <= cap_bytes) ? 2 : 0);
+    unsigned bad = 0u;
+    int count = 0, n = 0, excl = 0, c0 = 0;
+    unsigned* e32 = nullptr;
+    unsigned long long* e64 = nullptr;
+    if (mode == 1) {
+        int total;
+        n = sxm_tile<K, unsigned>(S, sxm_smem, cap_bytes, nrows, T, start, len, bad, e32, c0, &excl, &total);
+        count = total >> 1;
+    } else if (mode == 2) {
+        int total;
+        n = sxm_tile<K, unsigned long long>(S, sxm_smem, cap_bytes, nrows, T, start, len, bad, e64, c0, &excl, &total);
+        count = total >> 1;
+    }
+    if (__syncthreads_or(bad)) {
+        if (tid == 0) S.flags |= SXF_CONTRACT;
+    }
+    // fallback tile: one lane per row over global memory
+    int lane_count = 0;
+    int s_row[K], lim_row[K];
+    if (mode == 0 && wid == 0) {
+        const bool act = lane < nrows;
+#pragma unroll
+        for (int l = 0; l < K; ++l) {
+            const int a = act ? S.off[l][lane] : 0;
+            const int b = act ? S.off[l][lane + 1] : 0;
+            s_row[l] = a;
+            lim_row[l] = 2 * (b - a);
+        }
+        bool fb_bad = false, fb_over = false;
+        if (act) lane_count = sx_sweep_table<K, false>(A, s_row, lim_row, nullptr, nullptr, 0, fb_bad, fb_over);
+        if (__any_sync(0xFFFFFFFFu, fb_bad) && lane == 0) S.flags |= SXF_CONTRACT;
+        int tot = lane_count;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xFFFFFFFFu, tot, o);
+        count = tot;
+    }
+    // look-back for the tile's base
+    if (wid == 0) {
+        unsigned f = 0u;
+        const int base = sx_hier_lookback(st, tile, tiles, count, f);
+        if (lane == 0) {
+            S.base = base;
+            if (f) S.flags |= f;
+        }
+    }
+    __syncthreads();
+    const int base = S.base;
+    bool over = false;
+    if (mode != 0) {
+        if (mode == 1) sxm_write<K, unsigned>(A, S, e32, c0, n, excl, base, over);
+        else sxm_write<K, unsigned long long>(A, S, e64, c0, n, excl, base, over);
+        if (wid == 0) {
+            const int c = lane < nrows ? S.rowcnt[lane] : 0;
+            int incl = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            if (lane < nrows) A.out_off[r0 + lane + 1] = base + incl;
+            if (tile == 0 && lane == 0) A.out_off[0] = 0;
+        }
+    } else if (wid == 0) {
+        int incl = lane_count;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane < nrows) {
+            bool fb_bad = false;
+            if (lane_count > 0)
+                sx_sweep_table<K, true>(A, s_row, lim_row, A.out_begin, A.out_end, (long long)base + incl - lane_count,
+                                        fb_bad, over);
+            A.out_off[r0 + lane + 1] = base + incl;
+        }
+        if (tile == 0 && lane == 0) A.out_off[0] = 0;
+    }
+    if (__syncthreads_or(over)) {
+        if (tid == 0) S.flags |= SXF_CAPACITY;
+    }
+    if (tid == 0) {
+        const unsigned flags = S.flags;
+        if (flags) atomicOr(&st.counters[3], flags);
+        __threadfence();
+        const unsigned prev = atomicAdd(&st.counters[1], 1u);
+        if (prev == (unsigned)tiles - 1u) {
+            __threadfence();
+            const unsigned long long last = sx_ld_status(&st.tile_status[tiles - 1]);
+            const unsigned fl = atomicExch(&st.counters[3], 0u);
+            A.result[0] = (int)(unsigned)(last & 0xFFFFFFFFull);
+            A.result[1] = (int)fl;
+        }
+    }
+}
+
 size_t sx_sweep_state_bytes(long long tiles)
 {
     const long long groups = (tiles + SX_GROUP - 1) / SX_GROUP;
@@ -660,6 +1131,41 @@ static int sx_pick_ecap(long long elems, long long tiles)
     return (int)e;
 }
 
+
+template <int K>
+static cudaError_t sx_merge_launch_k(const SxBoolArgs& A, const SxSweepState& st, int tiles, int cap_bytes,
+                                     cudaStream_t stream)
+{
+    static int configured = 0;  // largest dynamic shared memory set for this instantiation
+    if (cap_bytes > configured) {
+        cudaError_t err =
+            cudaFuncSetAttribute(sx_merge_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap_bytes);
+        if (err != cudaSuccess) return err;
+        configured = cap_bytes;
+    }
+    sx_merge_kernel<K><<<tiles, SXM_THREADS, cap_bytes, stream>>>(A, st, tiles, cap_bytes);
+    return cudaGetLastError();
+}
+
+// Shared memory per tile: two (or three) key buffers of 32-bit keys with
+// room for 1.25x the average tile plus slack, in steps of 2 KiB, between
+// 8 KiB and 96 KiB.  `requested` (keys) overrides the average.
+static int sx_merge_cap(long long leaf_intervals, long long tiles, int requested, int nbuf)
+{
+    long long keys;
+    if (requested > 0) {
+        keys = requested;
+    } else {
+        const long long avg = tiles > 0 ? (2 * leaf_intervals + tiles - 1) / tiles : 0;
+        keys = avg + avg / 4 + 256;
+    }
+    long long bytes = 4ll * nbuf * keys;
+    bytes = (bytes + 2047) / 2048 * 2048;
+    if (bytes < 8192) bytes = 8192;
+    if (bytes > 98304) bytes = 98304;
+    return (int)bytes;
+}
+
 cudaError_t sx_sweep_launch(const SxBoolArgs& A, bool union_mode, void* workspace, cudaStream_t stream)
 {
     const long long tiles = sx_sweep_tiles(A.rows);
@@ -687,11 +1193,23 @@ cudaError_t sx_sweep_launch(const SxBoolArgs& A, bool union_mode, void* workspac
     // resident), global sweep with a residency cap of 3 blocks per SM for
     // heavy tiles (measured best on the 4096x4096 shape expression).
     SxBoolArgs B = A;
-    if (B.tune_kernel == 0) {
-        const long long avg = (A.capacity + tiles - 1) / tiles;
-        B.tune_kernel = avg <= 1024 ? 2 : 1;
-        if (B.tune_kernel == 1 && B.tune_blocks_per_sm == 0) B.tune_blocks_per_sm = 3;
+    if (B.tune_kernel == 0) B.tune_kernel = 3;
+    if (B.tune_kernel == 3) {
+        const int nbuf = (A.k == 3 || A.k == 6 || A.k == 7) ? 3 : 2;
+        const int cap = sx_merge_cap(A.capacity, tiles, A.tune_staging_cap, nbuf);
+        switch (A.k) {
+            case 1: return sx_merge_launch_k<1>(A, st, t, cap, stream);
+            case 2: return sx_merge_launch_k<2>(A, st, t, cap, stream);
+            case 3: return sx_merge_launch_k<3>(A, st, t, cap, stream);
+            case 4: return sx_merge_launch_k<4>(A, st, t, cap, stream);
+            case 5: return sx_merge_launch_k<5>(A, st, t, cap, stream);
+            case 6: return sx_merge_launch_k<6>(A, st, t, cap, stream);
+            case 7: return sx_merge_launch_k<7>(A, st, t, cap, stream);
+            case 8: return sx_merge_launch_k<8>(A, st, t, cap, stream);
+            default: return cudaErrorInvalidValue;
+        }
     }
+    if (B.tune_kernel == 1 && B.tune_blocks_per_sm == 0) B.tune_blocks_per_sm = 3;
     if (B.tune_kernel == 1) {
         const SxBoolArgs& A = B;
         switch (A.k) {

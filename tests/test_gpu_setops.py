@@ -226,3 +226,36 @@ def test_shapes_4096_expression(cuda_device):
     leaves_h = {n: iset(h) for n, h in zip("ABCDE", ops)}
     leaves_d = {n: dev_set(h) for n, h in zip("ABCDE", ops)}
     assert_same(sc.evaluate(_build(EXPRS["e0"], leaves_d)), O.evaluate(EXPRS["e0"], leaves_h), "shapes4096")
+
+
+def test_wide_coordinate_span_vs_oracle(cuda_device):
+    # tiles whose coordinates span more than 2^24 take the 64-bit key path
+    rng = np.random.default_rng(12)
+    hs = []
+    for _ in range(5):
+        b, e, off, rid = _random_canonical(rng, 700, 0, 5.0)
+        hs.append(((b.astype(np.int64) * 40000).astype(np.int32), (e.astype(np.int64) * 40000).astype(np.int32),
+                   off, rid))
+    leaves_h = {n: iset(h) for n, h in zip("ABCDE", hs)}
+    leaves_d = {n: dev_set(h) for n, h in zip("ABCDE", hs)}
+    for name, spec in EXPRS.items():
+        assert_same(sc.evaluate(_build(spec, leaves_d)), O.evaluate(spec, leaves_h), name)
+
+
+@pytest.mark.parametrize("tuning", [{"kernel": 1}, {"kernel": 1, "blocks_per_sm": 6}, {"kernel": 2},
+                                    {"kernel": 3, "staging_cap": 256}, {"kernel": 3, "staging_cap": 12000}])
+def test_tuning_never_changes_results(cuda_device, tuning):
+    from subsetix_b200 import _core
+
+    ops = synth.shape_operands(1024)
+    leaves_h = {n: iset(h) for n, h in zip("ABCDE", ops)}
+    leaves_d = {n: dev_set(h) for n, h in zip("ABCDE", ops)}
+    saved = dict(_core.TUNING)
+    try:
+        _core.TUNING.clear()
+        _core.TUNING.update(tuning)
+        got = sc.evaluate(_build(EXPRS["e0"], leaves_d))
+    finally:
+        _core.TUNING.clear()
+        _core.TUNING.update(saved)
+    assert_same(got, O.evaluate(EXPRS["e0"], leaves_h), str(tuning))
