@@ -146,7 +146,7 @@ def peak_hbm():
 
 def traffic_per_launch(copies: int):
     """DRAM bytes of one fused launch, from the committed ncu summary (scaled by copies)."""
-    path = os.path.join(REPO, "profiles", "sx_sweep_kernel_shapes4096.md")
+    path = os.path.join(REPO, "profiles", "sx_merge_kernel_shapes4096.md")
     try:
         for line in open(path):
             if line.startswith("traffic_bytes_per_copy:"):
@@ -338,7 +338,7 @@ def main():
         "gpu_launches": args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic_per_launch(args.copies),
-                     "peak_source": peak_kind, "algorithmic_bytes": algo, "kernel": "sx_sweep_kernel<5,MODE_TABLE>",
+                     "peak_source": peak_kind, "algorithmic_bytes": algo, "kernel": "sx_merge_kernel<5>",
                      "kernel_ms": kernel_ms},
         "clocks": clocks.summary(),
     }

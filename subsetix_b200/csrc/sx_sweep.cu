@@ -784,7 +784,10 @@ __device__ __forceinline__ int sxm_tile(SxmTile& S, unsigned char* smem, int cap
     // 2. pairwise merges; a list without a partner stays where it is
     c0 = (int)(((long long)T * tid) / SXM_THREADS);
     const int c1 = (int)(((long long)T * (tid + 1)) / SXM_THREADS);
+    unsigned xacc = 0u;  // XOR of (1 << leaf) over this thread's last merged range
+    const bool single = S.nl == 1;
     while (S.nl > 1) {
+        xacc = 0u;
         const int nl = S.nl;
         const int np = nl >> 1;  // merged pairs; list nl-1 waits when nl is odd
         const int M = S.ls[2 * np - 1] + S.ll[2 * np - 1];  // pairs cover [0, M)
@@ -819,7 +822,9 @@ __device__ __forceinline__ int sxm_tile(SxmTile& S, unsigned char* smem, int cap
             KeyT kb = j < lb ? B_[b0 + j] : Key::MAX;
             for (; k < pend; ++k) {
                 const bool ta = ka < kb;
-                D_[k] = ta ? ka : kb;
+                const KeyT kk = ta ? ka : kb;
+                D_[k] = kk;
+                xacc ^= 1u << Key::tag(kk);
                 if (ta) {
                     ++i;
                     ka = i < la ? A_[a0 + i] : Key::MAX;
@@ -853,10 +858,11 @@ __device__ __forceinline__ int sxm_tile(SxmTile& S, unsigned char* smem, int cap
     for (int q = 1; q < NB; ++q)
         if (mb == q) m = buf[q];
     if (mb == 1) emits = buf[0];
-    // 3. states: XOR of (1 << leaf) before this thread's chunk
-    unsigned x = 0u;
-    for (int i = c0; i < c1; ++i) x ^= 1u << Key::tag(m[i]);
-    unsigned s = sxm_block_excl_xor(x, S.warp);
+    // 3. states: XOR of (1 << leaf) before this thread's chunk.  The last
+    // merge round covered all T keys with the same split as [c0, c1).
+    if (single)
+        for (int i = c0; i < c1; ++i) xacc ^= 1u << Key::tag(m[i]);
+    unsigned s = sxm_block_excl_xor(xacc, S.warp);
     // 4. output boundaries of the chunk, kept in `emits` at [c0, c0 + n)
     int n = 0;
     if (c0 < c1) {
@@ -869,13 +875,14 @@ __device__ __forceinline__ int sxm_tile(SxmTile& S, unsigned char* smem, int cap
                 gstate ^= 1u << Key::tag(m[gs]);
             }
         }
-        bool fprev = (S.tab[gstate >> 5] >> (gstate & 31u)) & 1u;
+        const unsigned tab0 = S.tab[0];
+        bool fprev = K <= 5 ? ((tab0 >> gstate) & 1u) : ((S.tab[gstate >> 5] >> (gstate & 31u)) & 1u);
         KeyT cur = m[c0];
         for (int i = c0; i < c1; ++i) {
             const KeyT nxt = (i + 1 < T) ? m[i + 1] : Key::MAX;
             s ^= 1u << Key::tag(cur);
             if (Key::group(nxt) != Key::group(cur)) {
-                const bool fa = (S.tab[s >> 5] >> (s & 31u)) & 1u;
+                const bool fa = K <= 5 ? ((tab0 >> s) & 1u) : ((S.tab[s >> 5] >> (s & 31u)) & 1u);
                 if (fa != fprev) {
                     emits[c0 + n] = cur;
                     ++n;
