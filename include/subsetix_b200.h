@@ -362,6 +362,34 @@ int sx_value_runs(int type, const void* values, const int32_t* cell_offsets, int
 /* dst[p] = src[index[p]] for p < count (row offsets of derived sets). */
 int sx_gather_i32(const int32_t* index, int32_t count, const int32_t* src, int32_t* dst, void* stream);
 
+/* ---------------------------------------------------------------------------
+ * Two-level AMR on full grids, batched: arrays are [batch][height][width]
+ * (coarse) and [batch][height*ratio][width*ratio] (fine).  In the
+ * reference's AMR2Simulation both levels are full rectangles, and these are
+ * its interval kernels specialised to that case, with the same results:
+ *   sx_upwind_full      step_upwind_interval on a full grid
+ *                       (subsetix_cupy/interval_stencil.py:59-219); in != out;
+ *   sx_amr_sync_full    synchronize_interval_fields(..., reducer="mean",
+ *                       fill_fine_outside=True, copy=False)
+ *                       (subsetix_amr2/fields.py:570-612): coarse cells with
+ *                       action 1 (REFINE) take the mean of their fine block,
+ *                       the others are copied into it;
+ *   sx_amr_regrid_full  the regrid of simulation.py:289-304: gradient tag
+ *                       (regrid.py:336-350) then two-level grading with
+ *                       `padding` (regrid.py:404-442; mode 0 von Neumann,
+ *                       1 Moore), written as action bytes (1 REFINE, 0 KEEP)
+ *                       like ActionField.set_from_interval_set.  `tags` is
+ *                       scratch of batch*width*height bytes; threshold is
+ *                       max(refine_threshold, epsilon) rounded to float32.
+ * No counterpart in the reference for the batching.
+ * ------------------------------------------------------------------------- */
+int sx_upwind_full(int dtype, const void* values, void* out, int32_t width, int32_t height, int32_t batch, double a,
+                   double b, double dt, double dx, double dy, void* stream);
+int sx_amr_sync_full(int dtype, void* coarse, void* fine, const int8_t* actions, int32_t width, int32_t height,
+                     int32_t batch, int32_t ratio, void* stream);
+int sx_amr_regrid_full(int dtype, const void* coarse, uint8_t* tags, int8_t* actions, int32_t width, int32_t height,
+                       int32_t batch, float threshold, int32_t padding, int mode, void* stream);
+
 /* Compensated (Neumaier) FP64 sum of n values times `scale`, in a fixed
  * order (deterministic).  partials: 2 * parts doubles of scratch, parts in
  * [1, 4096].  No reference counterpart (the reference has no mass

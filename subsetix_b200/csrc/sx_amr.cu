@@ -1,0 +1,200 @@
+// Two-level AMR step on full grids, batched over independent simulations.
+//
+// In the reference's AMR2Simulation both levels are full rectangles: the
+// coarse field covers [0, W) x [0, H) and the fine field [0, rW) x [0, rH),
+// one interval per row (subsetix_amr2/simulation.py:159-213).  On such sets
+// the interval kernels reduce to dense ones, and this file runs them
+// directly on [batch][rows][cols] arrays:
+//
+//   sx_upwind_full     the upwind update of interval_stencil.py:59-113 with
+//                      zero exterior (cells outside the grid read 0);
+//   sx_amr_sync_full   synchronize_interval_fields with the mean reducer and
+//                      copy=False (fields.py:570-612): a coarse cell marked
+//                      REFINE takes the mean of its r x r fine block, summed
+//                      sub-row outer, column inner, times 1/r^2
+//                      (kernels.py:458-527); any other coarse cell is copied
+//                      into its fine block (kernels.py:384-418).  Refine and
+//                      coarse-only cells partition the grid, so one pass per
+//                      coarse cell does both halves;
+//   sx_amr_tag_full    the gradient tag of regrid.py:172-223,336-350: the
+//                      field is read as float32, the gradient has central
+//                      differences inside and one-sided ones at the edges,
+//                      and a cell is tagged when sqrt(gx^2 + gy^2) >=
+//                      threshold;
+//   sx_amr_grade_full  enforce_two_level_grading_set (regrid.py:404-442) as
+//                      a cell set: a coarse cell is refined when a tagged
+//                      cell lies within `padding` along a row or a column
+//                      (von Neumann) or within the (2p+1)^2 box (Moore),
+//                      clipped to the grid.  The action byte is REFINE (1)
+//                      or KEEP (0), as ActionField.set_from_interval_set
+//                      writes it (fields.py:520-546).
+//
+// Float formulas use explicit round-to-nearest operations, so results are
+// bit-identical to the interval kernels (and to the reference) on the same
+// inputs, in float32 and in float64.
+
+#include "sx_internal.cuh"
+
+__device__ __forceinline__ float sxa_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float sxa_sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float sxa_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float sxa_div(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ double sxa_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sxa_sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double sxa_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double sxa_div(double a, double b) { return __ddiv_rn(a, b); }
+
+// One thread per cell; x fastest.  blockIdx.z is the batch entry.
+template <typename T>
+__global__ void __launch_bounds__(256) sx_upwind_full_kernel(const T* __restrict__ in, T* __restrict__ out, int W,
+                                                             int H, T a, T b, T dt, T dx, T dy)
+{
+    const long long plane = (long long)W * H;
+    const T* v = in + plane * blockIdx.z;
+    T* o = out + plane * blockIdx.z;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= W) return;
+    const long long idx = (long long)y * W + x;
+    const T c = v[idx];
+    const T l = x > 0 ? v[idx - 1] : (T)0;
+    const T r = x + 1 < W ? v[idx + 1] : (T)0;
+    const T d = y > 0 ? v[idx - W] : (T)0;
+    const T u = y + 1 < H ? v[idx + W] : (T)0;
+    const T du_dx = a >= (T)0 ? sxa_div(sxa_sub(c, l), dx) : sxa_div(sxa_sub(r, c), dx);
+    const T du_dy = b >= (T)0 ? sxa_div(sxa_sub(c, d), dy) : sxa_div(sxa_sub(u, c), dy);
+    o[idx] = sxa_sub(c, sxa_mul(dt, sxa_add(sxa_mul(a, du_dx), sxa_mul(b, du_dy))));
+}
+
+// One thread per coarse cell.  R is the refinement ratio (template for the
+// common 2, runtime otherwise).
+template <typename T, int RT>
+__global__ void __launch_bounds__(256) sx_amr_sync_full_kernel(T* __restrict__ coarse, T* __restrict__ fine,
+                                                               const signed char* __restrict__ actions, int W, int H,
+                                                               int rr, T norm)
+{
+    const int R = RT > 0 ? RT : rr;
+    const int b = blockIdx.z;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= W) return;
+    const long long plane = (long long)W * H;
+    const long long ci = plane * b + (long long)y * W + x;
+    const int FW = W * R;
+    T* f = fine + plane * R * R * b + ((long long)y * R) * FW + (long long)x * R;
+    if (actions[ci] == 1) {
+        T acc = (T)0;
+        for (int dy = 0; dy < R; ++dy)
+            for (int dx = 0; dx < R; ++dx) acc = sxa_add(acc, f[(long long)dy * FW + dx]);
+        coarse[ci] = sxa_mul(acc, norm);
+    } else {
+        const T c = coarse[ci];
+        for (int dy = 0; dy < R; ++dy)
+            for (int dx = 0; dx < R; ++dx) f[(long long)dy * FW + dx] = c;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) sx_amr_tag_full_kernel(const T* __restrict__ in, unsigned char* __restrict__ tags,
+                                                              int W, int H, float thr)
+{
+    const long long plane = (long long)W * H;
+    const T* v = in + plane * blockIdx.z;
+    unsigned char* t = tags + plane * blockIdx.z;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= W) return;
+    const long long idx = (long long)y * W + x;
+    const float c = (float)v[idx];
+    float gx = 0.0f, gy = 0.0f;
+    if (W > 1) {
+        if (x == 0) gx = __fsub_rn((float)v[idx + 1], c);
+        else if (x == W - 1) gx = __fsub_rn(c, (float)v[idx - 1]);
+        else gx = __fmul_rn(__fsub_rn((float)v[idx + 1], (float)v[idx - 1]), 0.5f);
+    }
+    if (H > 1) {
+        if (y == 0) gy = __fsub_rn((float)v[idx + W], c);
+        else if (y == H - 1) gy = __fsub_rn(c, (float)v[idx - W]);
+        else gy = __fmul_rn(__fsub_rn((float)v[idx + W], (float)v[idx - W]), 0.5f);
+    }
+    t[idx] = __fsqrt_rn(__fadd_rn(__fmul_rn(gx, gx), __fmul_rn(gy, gy))) >= thr ? 1 : 0;
+}
+
+// mode 0: von Neumann (row or column within p), 1: Moore (box), 2: no grading
+__global__ void __launch_bounds__(256) sx_amr_grade_full_kernel(const unsigned char* __restrict__ tags,
+                                                               signed char* __restrict__ actions, int W, int H, int p,
+                                                               int mode)
+{
+    const long long plane = (long long)W * H;
+    const unsigned char* t = tags + plane * blockIdx.z;
+    signed char* a = actions + plane * blockIdx.z;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= W) return;
+    bool on = t[(long long)y * W + x] != 0;
+    if (!on && mode != 2) {
+        const int x0 = max(0, x - p), x1 = min(W - 1, x + p);
+        const int y0 = max(0, y - p), y1 = min(H - 1, y + p);
+        if (mode == 1) {
+            for (int yy = y0; yy <= y1 && !on; ++yy)
+                for (int xx = x0; xx <= x1; ++xx)
+                    if (t[(long long)yy * W + xx]) {
+                        on = true;
+                        break;
+                    }
+        } else {
+            for (int xx = x0; xx <= x1 && !on; ++xx) on = t[(long long)y * W + xx] != 0;
+            for (int yy = y0; yy <= y1 && !on; ++yy) on = t[(long long)yy * W + x] != 0;
+        }
+    }
+    a[(long long)y * W + x] = on ? 1 : 0;
+}
+
+static dim3 sxa_grid(int W, int H, int batch) { return dim3((unsigned)((W + 255) / 256), (unsigned)H, (unsigned)batch); }
+
+cudaError_t sx_upwind_full_launch(int dbl, const void* in, void* out, int W, int H, int batch, double a, double b,
+                                  double dt, double dx, double dy, cudaStream_t stream)
+{
+    const dim3 g = sxa_grid(W, H, batch);
+    if (dbl)
+        sx_upwind_full_kernel<double><<<g, 256, 0, stream>>>((const double*)in, (double*)out, W, H, a, b, dt, dx, dy);
+    else
+        sx_upwind_full_kernel<float><<<g, 256, 0, stream>>>((const float*)in, (float*)out, W, H, (float)a, (float)b,
+                                                            (float)dt, (float)dx, (float)dy);
+    return cudaGetLastError();
+}
+
+cudaError_t sx_amr_sync_full_launch(int dbl, void* coarse, void* fine, const signed char* actions, int W, int H,
+                                    int batch, int ratio, cudaStream_t stream)
+{
+    const dim3 g = sxa_grid(W, H, batch);
+    const double norm = 1.0 / ((double)ratio * ratio);
+    if (dbl) {
+        if (ratio == 2)
+            sx_amr_sync_full_kernel<double, 2><<<g, 256, 0, stream>>>((double*)coarse, (double*)fine, actions, W, H, 2,
+                                                                      norm);
+        else
+            sx_amr_sync_full_kernel<double, 0><<<g, 256, 0, stream>>>((double*)coarse, (double*)fine, actions, W, H,
+                                                                      ratio, norm);
+    } else {
+        if (ratio == 2)
+            sx_amr_sync_full_kernel<float, 2><<<g, 256, 0, stream>>>((float*)coarse, (float*)fine, actions, W, H, 2,
+                                                                     (float)norm);
+        else
+            sx_amr_sync_full_kernel<float, 0><<<g, 256, 0, stream>>>((float*)coarse, (float*)fine, actions, W, H, ratio,
+                                                                     (float)norm);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t sx_amr_regrid_full_launch(int dbl, const void* coarse, unsigned char* tags, signed char* actions, int W,
+                                      int H, int batch, float threshold, int padding, int mode, cudaStream_t stream)
+{
+    const dim3 g = sxa_grid(W, H, batch);
+    if (dbl)
+        sx_amr_tag_full_kernel<double><<<g, 256, 0, stream>>>((const double*)coarse, tags, W, H, threshold);
+    else
+        sx_amr_tag_full_kernel<float><<<g, 256, 0, stream>>>((const float*)coarse, tags, W, H, threshold);
+    sx_amr_grade_full_kernel<<<g, 256, 0, stream>>>(tags, actions, W, H, padding, padding <= 0 ? 2 : mode);
+    return cudaGetLastError();
+}

@@ -534,6 +534,56 @@ int sx_gather_i32(const int32_t* index, int32_t count, const int32_t* src, int32
     return SX_OK;
 }
 
+static int full_grid_check(const char* what, int W, int H, int batch)
+{
+    if (W <= 0 || H <= 0 || batch <= 0) return fail(SX_ERR_INVALID, "%s: width, height and batch must be positive", what);
+    if (H > 65535 || batch > 65535) return fail(SX_ERR_INVALID, "%s: height and batch must not exceed 65535", what);
+    if ((long long)W * H * batch > (1ll << 40)) return fail(SX_ERR_INVALID, "%s: grid too large", what);
+    return SX_OK;
+}
+
+int sx_upwind_full(int dtype, const void* values, void* out, int32_t width, int32_t height, int32_t batch, double a,
+                   double b, double dt, double dx, double dy, void* stream)
+{
+    if (dtype != SX_F32 && dtype != SX_F64) return fail(SX_ERR_INVALID, "sx_upwind_full: dtype %d", dtype);
+    int rc = full_grid_check("sx_upwind_full", width, height, batch);
+    if (rc != SX_OK) return rc;
+    if (!values || !out || values == out) return fail(SX_ERR_INVALID, "sx_upwind_full: need distinct input and output");
+    cudaError_t err = sx_upwind_full_launch(dtype == SX_F64, values, out, width, height, batch, a, b, dt, dx, dy,
+                                            (cudaStream_t)stream);
+    if (err != cudaSuccess) return cuda_fail(err, "sx_upwind_full");
+    return SX_OK;
+}
+
+int sx_amr_sync_full(int dtype, void* coarse, void* fine, const int8_t* actions, int32_t width, int32_t height,
+                     int32_t batch, int32_t ratio, void* stream)
+{
+    if (dtype != SX_F32 && dtype != SX_F64) return fail(SX_ERR_INVALID, "sx_amr_sync_full: dtype %d", dtype);
+    int rc = full_grid_check("sx_amr_sync_full", width, height, batch);
+    if (rc != SX_OK) return rc;
+    if (ratio < 1 || (long long)width * ratio > INT32_MAX || (long long)height * ratio > INT32_MAX)
+        return fail(SX_ERR_INVALID, "sx_amr_sync_full: bad ratio");
+    if (!coarse || !fine || !actions) return fail(SX_ERR_INVALID, "sx_amr_sync_full: null argument");
+    cudaError_t err = sx_amr_sync_full_launch(dtype == SX_F64, coarse, fine, (const signed char*)actions, width, height,
+                                              batch, ratio, (cudaStream_t)stream);
+    if (err != cudaSuccess) return cuda_fail(err, "sx_amr_sync_full");
+    return SX_OK;
+}
+
+int sx_amr_regrid_full(int dtype, const void* coarse, uint8_t* tags, int8_t* actions, int32_t width, int32_t height,
+                       int32_t batch, float threshold, int32_t padding, int mode, void* stream)
+{
+    if (dtype != SX_F32 && dtype != SX_F64) return fail(SX_ERR_INVALID, "sx_amr_regrid_full: dtype %d", dtype);
+    int rc = full_grid_check("sx_amr_regrid_full", width, height, batch);
+    if (rc != SX_OK) return rc;
+    if (mode != 0 && mode != 1) return fail(SX_ERR_INVALID, "sx_amr_regrid_full: mode must be 0 (von Neumann) or 1 (Moore)");
+    if (!coarse || !tags || !actions) return fail(SX_ERR_INVALID, "sx_amr_regrid_full: null argument");
+    cudaError_t err = sx_amr_regrid_full_launch(dtype == SX_F64, coarse, tags, (signed char*)actions, width, height,
+                                                batch, threshold, padding, mode, (cudaStream_t)stream);
+    if (err != cudaSuccess) return cuda_fail(err, "sx_amr_regrid_full");
+    return SX_OK;
+}
+
 int sx_mass_integral(int dtype, const void* values, int64_t n, double scale, double* partials, int parts, double* out,
                      void* stream)
 {

@@ -114,3 +114,11 @@ cudaError_t sx_value_runs_launch(int type, const void* v, const int* coff, int n
                                  const int* run_off, const int* b, int* ob, int* oe, cudaStream_t stream);
 cudaError_t sx_gather_i32_launch(const int* idx, int count, const int* src, int* dst, cudaStream_t stream);
 cudaError_t sx_gradient_launch(const float* d, int width, int height, float* out, cudaStream_t stream);
+
+// Full-grid two-level AMR (sx_amr.cu)
+cudaError_t sx_upwind_full_launch(int dbl, const void* in, void* out, int W, int H, int batch, double a, double b,
+                                  double dt, double dx, double dy, cudaStream_t stream);
+cudaError_t sx_amr_sync_full_launch(int dbl, void* coarse, void* fine, const signed char* actions, int W, int H,
+                                    int batch, int ratio, cudaStream_t stream);
+cudaError_t sx_amr_regrid_full_launch(int dbl, const void* coarse, unsigned char* tags, signed char* actions, int W,
+                                      int H, int batch, float threshold, int padding, int mode, cudaStream_t stream);

@@ -1,0 +1,111 @@
+"""The fused full-grid AMR engine against AMR2Simulation, the reference's fixtures and the FP64 oracle."""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from tests.golden_io import get_set, load
+from tests.gpu_util import assert_same, host
+
+pytestmark = pytest.mark.gpu
+
+amr = pytest.importorskip("subsetix_b200.subsetix_amr2")
+from subsetix_b200.subsetix_amr2.fused import FusedTwoLevelAMR  # noqa: E402
+
+
+def _vals(x):
+    return torch.as_tensor(x).cpu().numpy()
+
+
+def _gauss(res, sigma=0.1, cx=0.5, cy=0.5):
+    xs = (np.arange(res) + 0.5) / res
+    gx, gy = np.meshgrid(xs, xs)
+    return np.exp(-((gx - cx) ** 2 + (gy - cy) ** 2) / (2 * sigma ** 2))
+
+
+def _square(res):
+    sim = amr.AMR2Simulation(amr.SimulationConfig(coarse_resolution=res, velocity=(1.0, 0.5), cfl=0.5))
+    sim.initialize_square(squares=[amr.SquareSpec(center=(0.35, 0.4), half_width=(0.15, 0.1))])
+    return sim.state.coarse_field.values.reshape(res, res).clone()
+
+
+@pytest.mark.parametrize("tag", ["sq32", "sq24", "gauss32"])
+@pytest.mark.parametrize("graph", [False, True])
+def test_fused_matches_reference_fixtures(cuda_device, tag, graph):
+    data = load("amr.npz")
+    res, steps, every, vx, vy, dt = data[f"{tag}/params"].tolist()
+    res, steps, every = int(res), int(steps), int(every)
+    u0 = _square(res) if tag.startswith("sq") else torch.as_tensor(_gauss(res).astype(np.float32), device="cuda")
+    eng = FusedTwoLevelAMR(u0, velocity=(vx, vy), cfl=0.5, refine_threshold=0.05, grading=1)
+    assert eng.dt == dt
+    np.testing.assert_array_equal(_vals(eng.fine_values).reshape(-1), data[f"{tag}/fine0"])
+    assert_same(eng.refine_set(), get_set(data, f"{tag}/refine0"))
+    eng.run(steps, regrid_every=every, graph=graph)
+    np.testing.assert_array_equal(_vals(eng.coarse_values).reshape(-1), data[f"{tag}/coarse"])
+    np.testing.assert_array_equal(_vals(eng.fine_values).reshape(-1), data[f"{tag}/fine"])
+    assert_same(eng.refine_set(), get_set(data, f"{tag}/refine"))
+
+
+@pytest.mark.parametrize("mode,pad", [("von_neumann", 2), ("moore", 1), ("moore", 0)])
+def test_fused_matches_amr2simulation(cuda_device, mode, pad):
+    res, steps, every = 40, 9, 2
+    u0 = torch.as_tensor(_gauss(res, 0.08, 0.4, 0.55).astype(np.float32), device="cuda")
+    cfg = amr.SimulationConfig(coarse_resolution=res, velocity=(-0.7, 0.4), cfl=0.5, refine_threshold=0.03,
+                               grading=pad, grading_mode=mode)
+    sim = amr.AMR2Simulation(cfg)
+    from subsetix_b200.subsetix_cupy import create_interval_field, full_interval_set
+
+    f = create_interval_field(full_interval_set(res, res), fill_value=0.0, dtype=np.float32)
+    f.values.copy_(u0.reshape(-1))
+    sim.set_initial_field(f)
+    state, _ = sim.run(steps=steps, regrid_every=every)
+    eng = FusedTwoLevelAMR(u0, velocity=(-0.7, 0.4), cfl=0.5, refine_threshold=0.03, grading=pad, grading_mode=mode)
+    eng.run(steps, regrid_every=every, graph=True)
+    np.testing.assert_array_equal(_vals(eng.coarse_values).reshape(-1), _vals(state.coarse_field.values))
+    np.testing.assert_array_equal(_vals(eng.fine_values).reshape(-1), _vals(state.fine_field.values))
+    assert_same(eng.refine_set(), host(state.actions.refine_set()))
+
+
+def test_fused_fp64_matches_oracle(cuda_device):
+    res, steps, every = 48, 12, 4
+    u0 = _gauss(res, 0.07)
+    ref = O.AMR2(res, (1.0, 0.5), cfl=0.5, threshold=0.05, grading_pad=1, dtype=np.float64)
+    ref.init(u0)
+    ref.run(steps, every)
+    eng = FusedTwoLevelAMR(torch.as_tensor(u0, device="cuda"), velocity=(1.0, 0.5), cfl=0.5, dtype=torch.float64)
+    eng.run(steps, regrid_every=every, graph=True)
+    np.testing.assert_array_equal(_vals(eng.coarse_values).reshape(-1), ref.coarse.values)
+    np.testing.assert_array_equal(_vals(eng.fine_values).reshape(-1), ref.fine.values)
+
+
+def test_fused_batch_equals_single_runs(cuda_device):
+    res = 32
+    inits = [_gauss(res, s, cx, 0.5).astype(np.float32) for s, cx in ((0.06, 0.3), (0.1, 0.5), (0.08, 0.7))]
+    batch = torch.as_tensor(np.stack(inits), device="cuda")
+    eng = FusedTwoLevelAMR(batch, velocity=(1.0, 0.5), cfl=0.5)
+    eng.run(7, regrid_every=3)
+    for i, u0 in enumerate(inits):
+        one = FusedTwoLevelAMR(torch.as_tensor(u0, device="cuda"), velocity=(1.0, 0.5), cfl=0.5)
+        one.run(7, regrid_every=3, graph=False)
+        np.testing.assert_array_equal(_vals(eng.coarse_values[i]), _vals(one.coarse_values[0]))
+        np.testing.assert_array_equal(_vals(eng.fine_values[i]), _vals(one.fine_values[0]))
+
+
+def test_fused_fp32_error_and_mass(cuda_device):
+    res, steps, every = 128, 40, 10
+    u0 = _gauss(res, 0.05)
+    e64 = FusedTwoLevelAMR(torch.as_tensor(u0, device="cuda"), velocity=(1.0, 0.5), cfl=0.5, dtype=torch.float64)
+    e32 = FusedTwoLevelAMR(torch.as_tensor(u0.astype(np.float32), device="cuda"), velocity=(1.0, 0.5), cfl=0.5)
+    m0 = float(e64.mass()[0])
+    e64.run(steps, every)
+    e32.run(steps, every)
+    a = _vals(e32.fine_values).astype(np.float64)
+    b = _vals(e64.fine_values)
+    rel_l2 = np.linalg.norm(a - b) / np.linalg.norm(b)
+    assert rel_l2 <= 1e-5, rel_l2
+    m64, m32 = float(e64.mass()[0]), float(e32.mass()[0])
+    assert abs(m32 - m64) <= 1e-5 * abs(m64)
+    assert abs(m64 - m0) <= 1e-2 * abs(m0)  # zero-exterior upwind loses mass only at the boundary
+    assert abs(float(e64.restriction_defect()[0])) <= 1e-12
+    assert abs(float(e32.restriction_defect()[0])) <= 1e-5 * abs(m32)
