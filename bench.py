@@ -53,6 +53,7 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=5)
     p.add_argument("--cpu-seconds", type=float, default=10.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-amr", action="store_true", help="skip the two-level AMR step section")
     return p.parse_args()
 
 
@@ -219,6 +220,71 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def amr_section(device, steps: int = 200, every: int = 10, res: int = 1024):
+    """Two-level AMR advection, Gaussian blob exp(-r^2 / (2 * 0.05^2)) on a res^2 coarse grid.
+
+    Velocity (1.0, 0.5), CFL 0.5, regrid with 2:1 grading every `every`
+    steps, `steps` steps.  FP32 with CUDA-graph replay against FP64 without
+    graphs (the plain FP64 step) and FP64 with graphs; FP32 error against
+    the FP64 run, compensated FP64 mass integrals and restriction defect.
+    """
+    import torch
+
+    from subsetix_b200.subsetix_amr2.fused import FusedTwoLevelAMR
+
+    xs = (np.arange(res) + 0.5) / res
+    gx, gy = np.meshgrid(xs, xs)
+    u0 = np.exp(-((gx - 0.5) ** 2 + (gy - 0.5) ** 2) / (2 * 0.05 ** 2))
+
+    def make(dtype, fused):
+        return FusedTwoLevelAMR(torch.as_tensor(u0, dtype=dtype, device=device), velocity=(1.0, 0.5), cfl=0.5,
+                                refine_threshold=0.05, grading=1, dtype=dtype, fused=fused)
+
+    stream = torch.cuda.current_stream(device)
+    runs = {}
+    # "plain": separate upwind/upwind/sync launches, no graph; "graph": one fused
+    # step kernel per step, replayed from a CUDA graph
+    for name, dtype, graph in (("fp32_graph", torch.float32, True), ("fp64_plain", torch.float64, False),
+                               ("fp64_graph", torch.float64, True), ("fp32_plain", torch.float32, False)):
+        warm = make(dtype, graph)
+        warm.run(3 * every, every, graph=graph)
+        eng = make(dtype, graph)
+        if graph:
+            eng.prepare_graphs()
+        mass0 = float(eng.mass()[0])
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        eng.run(steps, every, graph=graph)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        runs[name] = (eng, e0.elapsed_time(e1), mass0)
+    cells = res * res + (2 * res) * (2 * res)
+    ref, _, mass0_64 = runs["fp64_plain"]
+    out = {"workload": f"two-level AMR {res}x{res} coarse, x2 fine, gaussian sigma 0.05, velocity (1.0,0.5), "
+                       f"CFL 0.5, {steps} steps, regrid+grading every {every}",
+           "cells_per_step": cells, "steps": steps}
+    peak, _ = peak_hbm()
+    for name, (eng, ms, m0) in runs.items():
+        es = 8 if eng.dtype == torch.float64 else 4
+        # algorithmic bytes per step: every coarse value and fine block read and
+        # written once plus the action byte; the regrid reads the coarse level
+        # and writes tag and action bytes once per period
+        algo = res * res * (10 * es + 1) + res * res * (es + 3) / every
+        out[name] = {"ms_per_step": ms / steps, "gcell_updates_per_s": cells * steps / (ms / 1e3) / 1e9,
+                     "hbm_gbs": algo / (ms / steps / 1e3) / 1e9, "hbm_frac": algo / (ms / steps / 1e3) / 1e9 / peak,
+                     "mass_final": float(eng.mass()[0]), "mass_initial": m0,
+                     "restriction_defect": float(eng.restriction_defect()[0])}
+    for lvl in ("coarse_values", "fine_values"):
+        b = getattr(ref, lvl).double()
+        a = getattr(runs["fp32_graph"][0], lvl).double()
+        out[f"fp32_rel_l2_{lvl.split('_')[0]}"] = float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
+        out[f"fp32_linf_{lvl.split('_')[0]}"] = float((a - b).abs().max())
+    out["speedup_fp32_graph_vs_fp64_plain"] = out["fp64_plain"]["ms_per_step"] / out["fp32_graph"]["ms_per_step"]
+    out["fp64_reference"] = "the FP64 run of the same kernels (bit-identical to the FP64 oracle at test sizes)"
+    return out
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -342,6 +408,8 @@ def main():
                      "kernel_ms": kernel_ms},
         "clocks": clocks.summary(),
     }
+    if not args.no_amr:
+        line["amr_step"] = amr_section(device)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         one = [synth_one for synth_one in workload(1)]
         line["cpu_baseline"] = cpu_baseline(one, args.cpu_seconds, True)

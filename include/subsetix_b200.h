@@ -387,6 +387,12 @@ int sx_upwind_full(int dtype, const void* values, void* out, int32_t width, int3
                    double b, double dt, double dx, double dy, void* stream);
 int sx_amr_sync_full(int dtype, void* coarse, void* fine, const int8_t* actions, int32_t width, int32_t height,
                      int32_t batch, int32_t ratio, void* stream);
+/* One fixed-geometry step for ratio 2 in one pass: sx_upwind_full on both
+ * levels followed by sx_amr_sync_full, value for value (a coarse cell's
+ * synchronisation reads only its own new value and its fine block's). */
+int sx_amr_step_full(int dtype, const void* coarse_in, const void* fine_in, void* coarse_out, void* fine_out,
+                     const int8_t* actions, int32_t width, int32_t height, int32_t batch, double a, double b,
+                     double dt, double dx_coarse, double dy_coarse, double dx_fine, double dy_fine, void* stream);
 int sx_amr_regrid_full(int dtype, const void* coarse, uint8_t* tags, int8_t* actions, int32_t width, int32_t height,
                        int32_t batch, float threshold, int32_t padding, int mode, void* stream);
 

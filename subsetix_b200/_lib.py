@@ -118,6 +118,9 @@ _SIGNATURES = {
                                       ctypes.c_double, c_vp]),
     "sx_amr_sync_full": (ctypes.c_int, [ctypes.c_int, c_vp, c_vp, c_vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                         ctypes.c_int32, c_vp]),
+    "sx_amr_step_full": (ctypes.c_int, [ctypes.c_int, c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.c_int32, ctypes.c_int32,
+                                        ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                        ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double, c_vp]),
     "sx_amr_regrid_full": (ctypes.c_int, [ctypes.c_int, c_vp, c_vp, c_vp, ctypes.c_int32, ctypes.c_int32,
                                           ctypes.c_int32, ctypes.c_float, ctypes.c_int32, ctypes.c_int, c_vp]),
     "sx_mass_integral": (ctypes.c_int, [ctypes.c_int, c_vp, ctypes.c_int64, ctypes.c_double, c_vp, ctypes.c_int, c_vp,

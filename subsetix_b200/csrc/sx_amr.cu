@@ -94,6 +94,78 @@ __global__ void __launch_bounds__(256) sx_amr_sync_full_kernel(T* __restrict__ c
     }
 }
 
+// Whole fixed-geometry step for ratio 2: upwind of the coarse cell and of
+// its 2 x 2 fine block (from the previous values, zero exterior), then the
+// synchronisation of that coarse cell with its block.  A step's
+// synchronisation of a coarse cell reads only that cell's and that block's
+// new values, so this equals upwind(coarse); upwind(fine); sync, value for
+// value.  in/out are distinct buffers.
+template <typename T>
+__device__ __forceinline__ T sxa_upwind_cell(T c, T l, T r, T d, T u, T a, T b, T dt, T dx, T dy)
+{
+    const T du_dx = a >= (T)0 ? sxa_div(sxa_sub(c, l), dx) : sxa_div(sxa_sub(r, c), dx);
+    const T du_dy = b >= (T)0 ? sxa_div(sxa_sub(c, d), dy) : sxa_div(sxa_sub(u, c), dy);
+    return sxa_sub(c, sxa_mul(dt, sxa_add(sxa_mul(a, du_dx), sxa_mul(b, du_dy))));
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) sx_amr_step_full_kernel(const T* __restrict__ cin, const T* __restrict__ fin,
+                                                               T* __restrict__ cout, T* __restrict__ fout,
+                                                               const signed char* __restrict__ actions, int W, int H,
+                                                               T a, T b, T dt, T dxc, T dyc, T dxf, T dyf, T norm)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= W) return;
+    const long long plane = (long long)W * H;
+    const int FW = 2 * W, FH = 2 * H;
+    const T* C = cin + plane * blockIdx.z;
+    const T* F = fin + 4 * plane * blockIdx.z;
+    const long long ci = (long long)y * W + x;
+    // coarse cell
+    const T c = C[ci];
+    const T cl = x > 0 ? C[ci - 1] : (T)0;
+    const T cr = x + 1 < W ? C[ci + 1] : (T)0;
+    const T cd = y > 0 ? C[ci - W] : (T)0;
+    const T cu = y + 1 < H ? C[ci + W] : (T)0;
+    const T cn = sxa_upwind_cell(c, cl, cr, cd, cu, a, b, dt, dxc, dyc);
+    // fine block: rows 2y-1 .. 2y+2, columns 2x-1 .. 2x+2
+    const int fx = 2 * x, fy = 2 * y;
+    T v[4][4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int yy = fy - 1 + j;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int xx = fx - 1 + i;
+            const bool corner = (j == 0 || j == 3) && (i == 0 || i == 3);
+            v[j][i] = (!corner && yy >= 0 && yy < FH && xx >= 0 && xx < FW) ? F[(long long)yy * FW + xx] : (T)0;
+        }
+    }
+    T fn[2][2];
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+            fn[j][i] = sxa_upwind_cell(v[j + 1][i + 1], v[j + 1][i], v[j + 1][i + 2], v[j][i + 1], v[j + 2][i + 1], a, b,
+                                       dt, dxf, dyf);
+    T* CO = cout + plane * blockIdx.z;
+    T* FO = fout + 4 * plane * blockIdx.z;
+    if (actions[plane * blockIdx.z + ci] == 1) {
+        T acc = sxa_add(sxa_add(sxa_add(sxa_add((T)0, fn[0][0]), fn[0][1]), fn[1][0]), fn[1][1]);
+        CO[ci] = sxa_mul(acc, norm);
+    } else {
+        CO[ci] = cn;
+        fn[0][0] = fn[0][1] = fn[1][0] = fn[1][1] = cn;
+    }
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+        T* row = FO + (long long)(fy + j) * FW + fx;
+        row[0] = fn[j][0];
+        row[1] = fn[j][1];
+    }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) sx_amr_tag_full_kernel(const T* __restrict__ in, unsigned char* __restrict__ tags,
                                                               int W, int H, float thr)
@@ -196,5 +268,22 @@ cudaError_t sx_amr_regrid_full_launch(int dbl, const void* coarse, unsigned char
     else
         sx_amr_tag_full_kernel<float><<<g, 256, 0, stream>>>((const float*)coarse, tags, W, H, threshold);
     sx_amr_grade_full_kernel<<<g, 256, 0, stream>>>(tags, actions, W, H, padding, padding <= 0 ? 2 : mode);
+    return cudaGetLastError();
+}
+
+cudaError_t sx_amr_step_full_launch(int dbl, const void* cin, const void* fin, void* cout, void* fout,
+                                    const signed char* actions, int W, int H, int batch, double a, double b, double dt,
+                                    double dxc, double dyc, double dxf, double dyf, cudaStream_t stream)
+{
+    const dim3 g = sxa_grid(W, H, batch);
+    if (dbl)
+        sx_amr_step_full_kernel<double><<<g, 256, 0, stream>>>((const double*)cin, (const double*)fin, (double*)cout,
+                                                               (double*)fout, actions, W, H, a, b, dt, dxc, dyc, dxf,
+                                                               dyf, 0.25);
+    else
+        sx_amr_step_full_kernel<float><<<g, 256, 0, stream>>>((const float*)cin, (const float*)fin, (float*)cout,
+                                                              (float*)fout, actions, W, H, (float)a, (float)b,
+                                                              (float)dt, (float)dxc, (float)dyc, (float)dxf,
+                                                              (float)dyf, 0.25f);
     return cudaGetLastError();
 }

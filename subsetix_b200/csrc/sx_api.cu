@@ -570,6 +570,26 @@ int sx_amr_sync_full(int dtype, void* coarse, void* fine, const int8_t* actions,
     return SX_OK;
 }
 
+int sx_amr_step_full(int dtype, const void* coarse_in, const void* fine_in, void* coarse_out, void* fine_out,
+                     const int8_t* actions, int32_t width, int32_t height, int32_t batch, double a, double b,
+                     double dt, double dx_coarse, double dy_coarse, double dx_fine, double dy_fine, void* stream)
+{
+    if (dtype != SX_F32 && dtype != SX_F64) return fail(SX_ERR_INVALID, "sx_amr_step_full: dtype %d", dtype);
+    int rc = full_grid_check("sx_amr_step_full", width, height, batch);
+    if (rc != SX_OK) return rc;
+    if ((long long)width * 2 > INT32_MAX || (long long)height * 2 > INT32_MAX)
+        return fail(SX_ERR_INVALID, "sx_amr_step_full: grid too large");
+    if (!coarse_in || !fine_in || !coarse_out || !fine_out || !actions)
+        return fail(SX_ERR_INVALID, "sx_amr_step_full: null argument");
+    if (coarse_in == coarse_out || fine_in == fine_out)
+        return fail(SX_ERR_INVALID, "sx_amr_step_full: outputs must not alias inputs");
+    cudaError_t err = sx_amr_step_full_launch(dtype == SX_F64, coarse_in, fine_in, coarse_out, fine_out,
+                                              (const signed char*)actions, width, height, batch, a, b, dt, dx_coarse,
+                                              dy_coarse, dx_fine, dy_fine, (cudaStream_t)stream);
+    if (err != cudaSuccess) return cuda_fail(err, "sx_amr_step_full");
+    return SX_OK;
+}
+
 int sx_amr_regrid_full(int dtype, const void* coarse, uint8_t* tags, int8_t* actions, int32_t width, int32_t height,
                        int32_t batch, float threshold, int32_t padding, int mode, void* stream)
 {

@@ -122,3 +122,6 @@ cudaError_t sx_amr_sync_full_launch(int dbl, void* coarse, void* fine, const sig
                                     int batch, int ratio, cudaStream_t stream);
 cudaError_t sx_amr_regrid_full_launch(int dbl, const void* coarse, unsigned char* tags, signed char* actions, int W,
                                       int H, int batch, float threshold, int padding, int mode, cudaStream_t stream);
+cudaError_t sx_amr_step_full_launch(int dbl, const void* cin, const void* fin, void* cout, void* fout,
+                                    const signed char* actions, int W, int H, int batch, double a, double b, double dt,
+                                    double dxc, double dyc, double dxf, double dyf, cudaStream_t stream);

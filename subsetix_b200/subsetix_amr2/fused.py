@@ -7,10 +7,11 @@ both levels as full rectangles and runs, per step,
 
 On full rectangles every interval kernel of that loop is a dense one, so
 ``FusedTwoLevelAMR`` runs the same loop on ``[batch, rows, cols]`` arrays
-with four kernels: ``sx_upwind_full`` (both levels), ``sx_amr_sync_full``
-(restriction into refined coarse cells and prolongation into the rest, in
-one pass), and ``sx_amr_regrid_full`` (gradient tag and grading into action
-bytes).  The results are bit-identical to ``AMR2Simulation`` on the same
+with ``sx_upwind_full`` (both levels), ``sx_amr_sync_full`` (restriction
+into refined coarse cells and prolongation into the rest, in one pass) and
+``sx_amr_regrid_full`` (gradient tag and grading into action bytes).  For
+ratio 2 the upwind of both levels and the synchronisation run as one kernel
+per step (``sx_amr_step_full``, ``fused=True``).  The results are bit-identical to ``AMR2Simulation`` on the same
 initial field, in float32 and in float64.  The first synchronisation of a
 step always follows the previous step's last one with nothing in between,
 so it recomputes identical values and is skipped.
@@ -53,7 +54,7 @@ class FusedTwoLevelAMR:
 
     def __init__(self, coarse0: torch.Tensor, *, velocity: Sequence[float], cfl: float = 0.9,
                  refine_threshold: float = 0.05, grading: int = 1, grading_mode: str = "von_neumann", ratio: int = 2,
-                 dtype: torch.dtype = torch.float32, epsilon: float = 1e-8):
+                 dtype: torch.dtype = torch.float32, epsilon: float = 1e-8, fused: bool = True):
         if dtype not in (torch.float32, torch.float64):
             raise TypeError("dtype must be torch.float32 or torch.float64")
         if grading_mode not in _MODES:
@@ -70,6 +71,7 @@ class FusedTwoLevelAMR:
             raise ValueError("AMR2Simulation grids are square")
         self.device = c0.device
         self.dtype = dtype
+        self.fused = bool(fused) and int(ratio) == 2
         self.code = _lib.SX_F64 if dtype == torch.float64 else _lib.SX_F32
         self.ratio = int(ratio)
         self.velocity = (float(velocity[0]), float(velocity[1]))
@@ -127,11 +129,24 @@ class FusedTwoLevelAMR:
                "sx_upwind_full")
         self.cur = nxt
 
+    def _fused_advance_sync(self) -> None:
+        lib = _lib.load()
+        a, b = self.velocity
+        nxt = 1 - self.cur
+        _check(lib.sx_amr_step_full(self.code, ptr(self.coarse[self.cur]), ptr(self.fine[self.cur]),
+                                    ptr(self.coarse[nxt]), ptr(self.fine[nxt]), ptr(self.actions), self.width,
+                                    self.height, self.batch, a, b, self.dt, self.dx_coarse, self.dy_coarse,
+                                    self.dx_fine, self.dy_fine, self._stream()), "sx_amr_step_full")
+        self.cur = nxt
+
     def _step_body(self, regrid: bool) -> None:
         if regrid:
             self._regrid()
-        self._advance()
-        self._sync()
+        if self.fused:
+            self._fused_advance_sync()
+        else:
+            self._advance()
+            self._sync()
 
     # ------------------------------------------------------------------ public
     def step(self, regrid_every: int = 1) -> None:

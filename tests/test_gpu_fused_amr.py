@@ -31,13 +31,13 @@ def _square(res):
 
 
 @pytest.mark.parametrize("tag", ["sq32", "sq24", "gauss32"])
-@pytest.mark.parametrize("graph", [False, True])
-def test_fused_matches_reference_fixtures(cuda_device, tag, graph):
+@pytest.mark.parametrize("graph,fused", [(False, False), (False, True), (True, True), (True, False)])
+def test_fused_matches_reference_fixtures(cuda_device, tag, graph, fused):
     data = load("amr.npz")
     res, steps, every, vx, vy, dt = data[f"{tag}/params"].tolist()
     res, steps, every = int(res), int(steps), int(every)
     u0 = _square(res) if tag.startswith("sq") else torch.as_tensor(_gauss(res).astype(np.float32), device="cuda")
-    eng = FusedTwoLevelAMR(u0, velocity=(vx, vy), cfl=0.5, refine_threshold=0.05, grading=1)
+    eng = FusedTwoLevelAMR(u0, velocity=(vx, vy), cfl=0.5, refine_threshold=0.05, grading=1, fused=fused)
     assert eng.dt == dt
     np.testing.assert_array_equal(_vals(eng.fine_values).reshape(-1), data[f"{tag}/fine0"])
     assert_same(eng.refine_set(), get_set(data, f"{tag}/refine0"))
@@ -73,10 +73,12 @@ def test_fused_fp64_matches_oracle(cuda_device):
     ref = O.AMR2(res, (1.0, 0.5), cfl=0.5, threshold=0.05, grading_pad=1, dtype=np.float64)
     ref.init(u0)
     ref.run(steps, every)
-    eng = FusedTwoLevelAMR(torch.as_tensor(u0, device="cuda"), velocity=(1.0, 0.5), cfl=0.5, dtype=torch.float64)
-    eng.run(steps, regrid_every=every, graph=True)
-    np.testing.assert_array_equal(_vals(eng.coarse_values).reshape(-1), ref.coarse.values)
-    np.testing.assert_array_equal(_vals(eng.fine_values).reshape(-1), ref.fine.values)
+    for fused in (True, False):
+        eng = FusedTwoLevelAMR(torch.as_tensor(u0, device="cuda"), velocity=(1.0, 0.5), cfl=0.5, dtype=torch.float64,
+                               fused=fused)
+        eng.run(steps, regrid_every=every, graph=True)
+        np.testing.assert_array_equal(_vals(eng.coarse_values).reshape(-1), ref.coarse.values)
+        np.testing.assert_array_equal(_vals(eng.fine_values).reshape(-1), ref.fine.values)
 
 
 def test_fused_batch_equals_single_runs(cuda_device):
