@@ -111,3 +111,36 @@ def test_fused_fp32_error_and_mass(cuda_device):
     assert abs(m64 - m0) <= 1e-2 * abs(m0)  # zero-exterior upwind loses mass only at the boundary
     assert abs(float(e64.restriction_defect()[0])) <= 1e-12
     assert abs(float(e32.restriction_defect()[0])) <= 1e-5 * abs(m32)
+
+
+def test_batched_uneven_sets_against_oracle(cuda_device):
+    from subsetix_b200 import synth
+    from subsetix_b200.batch import SetBatch, batched_binary, batched_upwind
+    from tests.gpu_util import dev_set, iset
+
+    sides, sets_a = synth.batched_uneven_sets(count=24, seed=3, side_hi=1024)
+    _, sets_b = synth.batched_uneven_sets(count=24, seed=4, side_hi=1024)
+    A = SetBatch.from_sets([dev_set(h) for h in sets_a], sides)
+    B = SetBatch.from_sets([dev_set(h) for h in sets_b], sides)
+    uni = batched_binary(A, B, "union").split()
+    inter = batched_binary(A, B, "intersection").split()
+    for i in range(len(sides)):
+        assert_same(uni[i], O.union(iset(sets_a[i]), iset(sets_b[i])), f"union {i}")
+        assert_same(inter[i], O.intersection(iset(sets_a[i]), iset(sets_b[i])), f"intersection {i}")
+    # one FP32 upwind step of every set's field in one launch
+    rng = np.random.default_rng(1)
+    fields, values = [], []
+    for h, side in zip(sets_a, sides):
+        s = iset(h)
+        f = O.create_field(s, 0.0, np.float32)
+        f.values[...] = rng.uniform(0, 1, f.values.size).astype(np.float32)
+        fields.append((f, side))
+        values.append(f.values)
+    vals = torch.as_tensor(np.concatenate(values), device="cuda")
+    W = max(sides)
+    got = _vals(batched_upwind(A, vals, width=W, a=1.0, b=-0.5, dt=1e-4, dx=1e-3, dy=1e-3))
+    pos = 0
+    for f, side in fields:
+        exp = O.upwind(f, width=side, height=side, a=1.0, b=-0.5, dt=1e-4, dx=1e-3, dy=1e-3)
+        np.testing.assert_array_equal(got[pos:pos + exp.size], exp)
+        pos += exp.size
