@@ -54,6 +54,7 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=10.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-amr", action="store_true", help="skip the two-level AMR step section")
+    p.add_argument("--no-autotune", action="store_true", help="use the automatic launch choice")
     return p.parse_args()
 
 
@@ -326,6 +327,12 @@ def main():
         return _core.bool_eval_async(specs, R, table, _lib.MODE_TABLE, device, out=(ob, oe), result=res_buf,
                                      offsets=off_buf)
 
+    tuning = {}
+    if not args.no_autotune:
+        from subsetix_b200 import autotune
+
+        tuning = autotune.tune_bool_eval(specs, R, table, device)
+
     # correctness guard + output size for the roofline bytes
     _, _, ooff, result = step()
     total, flags = (int(x) for x in result.cpu())
@@ -398,7 +405,8 @@ def main():
         "dtype": "int32", "data": "synthetic",
         "config": {"workload": f"shapes4096 ((A|B)-(C&D))^E x{args.copies} stacked copies per rank",
                    "copies": args.copies, "input_intervals_per_step": n_in, "output_intervals": total,
-                   "rows": R, "l2": "inputs larger than L2 (no flush)", "parallelism": f"independent batch per rank x{world}"},
+                   "rows": R, "l2": "inputs larger than L2 (no flush)", "parallelism": f"independent batch per rank x{world}",
+                   "tuning": {k: v for k, v in tuning.items() if k != "ms"}},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e_ms},
         "gpu_launches": args.steps,

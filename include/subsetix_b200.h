@@ -324,6 +324,20 @@ int sx_upwind_f64(const int32_t* rows, const int32_t* row_offsets, int32_t row_c
                   const double* values, double* out, int32_t width, int32_t height, double a, double b, double dt,
                   double dx, double dy, int direct, void* stream);
 
+/* Adjoint of sx_upwind for fixed velocity and dt (no reference
+ * counterpart).  grad_out = dL/du' in, grad_in = dL/du out (may not alias),
+ * values = the step's input u; grad_velocity[2] (device doubles) receives
+ * (dL/da, dL/db) with dt held fixed, summed in a fixed order.  The
+ * transpose follows the forward's neighbour rules exactly (zero exterior,
+ * cells outside the set read 0).  scratch: sx_upwind_adjoint_scratch_bytes
+ * bytes of device memory. */
+size_t sx_upwind_adjoint_scratch_bytes(int64_t cells);
+int sx_upwind_adjoint(int dtype, const int32_t* rows, const int32_t* row_offsets, int32_t row_count,
+                      const int32_t* begin, const int32_t* end, const int32_t* cell_offsets, int64_t n, int64_t cells,
+                      const int32_t* lookup, const void* grad_out, const void* values, void* grad_in, int32_t width,
+                      int32_t height, double a, double b, double dt, double dx, double dy, int direct,
+                      double* grad_velocity, void* scratch, size_t scratch_bytes, void* stream);
+
 /* Threshold run-length encoding of a full width x height float32 grid
  * (subsetix_amr2/regrid.py:20-124 K11/K12, and regrid.py:172-223 K14 when
  * gradient = 1): a run is a stretch of value >= threshold, where value is

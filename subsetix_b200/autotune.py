@@ -1,0 +1,96 @@
+"""Launch autotuner for the row-sweep set algebra (sx_bool_eval).
+
+The candidates are the kernel kinds of ``sx_tuning``: the merge-path tile
+kernel with several key capacities per tile (how many boundaries a block
+stages, i.e. the work per warp), and the one-lane-per-row sweep with
+several residency caps.  Each candidate is timed with CUDA events on the
+caller's workload; the fastest is cached under a key of the workload's
+shape (leaf count, row count, mean boundaries per 32-row tile, bucketed by
+powers of two) and installed in ``_core.TUNING`` so later evaluations use
+it.  Results never depend on the tuning; only speed does.
+"""
+
+from __future__ import annotations
+
+import json
+import math
+import os
+from typing import Dict, List, Optional, Sequence
+
+import torch
+
+from . import _core, _lib
+
+_CACHE: Dict[str, dict] = {}
+
+
+def workload_key(sizes: Sequence[int], rows: int) -> str:
+    k = len(sizes)
+    tiles = max(1, (int(rows) + 31) // 32)
+    per_tile = 2 * sum(int(s) for s in sizes) / tiles
+    return f"k{k}-r{int(math.log2(max(rows, 1)))}-t{int(math.log2(max(per_tile, 1.0)))}"
+
+
+def candidates(sizes: Sequence[int], rows: int) -> List[dict]:
+    tiles = max(1, (int(rows) + 31) // 32)
+    avg = 2 * sum(int(s) for s in sizes) / tiles
+    out = []
+    for f in (1.1, 1.25, 1.5, 2.0):
+        out.append({"kernel": 3, "staging_cap": int(avg * f + 256)})
+    for b in (3, 5, 8):
+        out.append({"kernel": 1, "blocks_per_sm": b})
+    return out
+
+
+def tune_bool_eval(leaves, rows: int, table: Sequence[int], device, *, mode: int = _lib.MODE_TABLE,
+                   repeats: int = 5, install: bool = True, cache_path: Optional[str] = None) -> dict:
+    """Time every candidate on ``leaves`` and return (and install) the fastest tuning."""
+    sizes = [int(leaf[0].numel()) for leaf in leaves]
+    key = workload_key(sizes, rows)
+    if key in _CACHE:
+        best = _CACHE[key]
+    else:
+        cap = max(1, sum(sizes))
+        ob = torch.empty(cap, dtype=torch.int32, device=device)
+        oe = torch.empty(cap, dtype=torch.int32, device=device)
+        off = torch.empty(rows + 1, dtype=torch.int32, device=device)
+        res = torch.empty(2, dtype=torch.int32, device=device)
+        stream = torch.cuda.current_stream(device)
+        timings = []
+        for cand in candidates(sizes, rows):
+            def launch():
+                _core.bool_eval_async(leaves, rows, table, mode, device, out=(ob, oe), result=res, offsets=off,
+                                      tuning=cand)
+            launch()
+            torch.cuda.synchronize(device)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(repeats):
+                launch()
+            e1.record(stream)
+            torch.cuda.synchronize(device)
+            timings.append((e0.elapsed_time(e1) / repeats, cand))
+        ms, best = min(timings, key=lambda t: t[0])
+        best = dict(best, ms=ms, key=key)
+        _CACHE[key] = best
+        if cache_path:
+            data = {}
+            if os.path.exists(cache_path):
+                with open(cache_path) as f:
+                    data = json.load(f)
+            data[key] = best
+            with open(cache_path, "w") as f:
+                json.dump(data, f, indent=1, sort_keys=True)
+    if install:
+        _core.TUNING.clear()
+        _core.TUNING.update({k: v for k, v in best.items() if k in ("kernel", "blocks_per_sm", "staging_cap")})
+    return best
+
+
+def load_cache(path: str) -> None:
+    """Merge a saved cache file into the in-memory cache."""
+    with open(path) as f:
+        _CACHE.update(json.load(f))
+
+
+__all__ = ["tune_bool_eval", "candidates", "workload_key", "load_cache"]

@@ -463,6 +463,38 @@ int sx_upwind_f64(const int32_t* rows, const int32_t* row_offsets, int32_t row_c
                      width, height, a, b, dt, dx, dy, direct, stream);
 }
 
+size_t sx_upwind_adjoint_scratch_bytes(int64_t cells)
+{
+    return (size_t)sx_upwind_adjoint_parts(cells) * 2 * sizeof(double);
+}
+
+int sx_upwind_adjoint(int dtype, const int32_t* rows, const int32_t* row_offsets, int32_t row_count,
+                      const int32_t* begin, const int32_t* end, const int32_t* cell_offsets, int64_t n, int64_t cells,
+                      const int32_t* lookup, const void* grad_out, const void* values, void* grad_in, int32_t width,
+                      int32_t height, double a, double b, double dt, double dx, double dy, int direct,
+                      double* grad_velocity, void* scratch, size_t scratch_bytes, void* stream)
+{
+    if (dtype != SX_F32 && dtype != SX_F64) return fail(SX_ERR_INVALID, "sx_upwind_adjoint: dtype %d", dtype);
+    if (width <= 0 || height <= 0) return fail(SX_ERR_INVALID, "sx_upwind_adjoint: width and height must be positive");
+    if (row_count < 0 || n < 0 || n > INT32_MAX || cells < 0 || cells > INT32_MAX)
+        return fail(SX_ERR_INVALID, "sx_upwind_adjoint: bad size");
+    if (!grad_velocity) return fail(SX_ERR_INVALID, "sx_upwind_adjoint: null grad_velocity");
+    if (n == 0 || cells == 0) {
+        cudaError_t err = cudaMemsetAsync(grad_velocity, 0, 2 * sizeof(double), (cudaStream_t)stream);
+        return err == cudaSuccess ? SX_OK : cuda_fail(err, "sx_upwind_adjoint");
+    }
+    if (!rows || !row_offsets || !begin || !end || !cell_offsets || !lookup || !grad_out || !values || !grad_in)
+        return fail(SX_ERR_INVALID, "sx_upwind_adjoint: null argument");
+    if (!scratch || scratch_bytes < sx_upwind_adjoint_scratch_bytes(cells))
+        return fail(SX_ERR_WORKSPACE, "sx_upwind_adjoint: scratch needs %zu bytes", sx_upwind_adjoint_scratch_bytes(cells));
+    cudaError_t err = sx_upwind_adjoint_launch(rows, row_offsets, row_count, begin, end, cell_offsets, (int)n, cells,
+                                               lookup, grad_out, values, grad_in, width, height, a, b, dt, dx, dy,
+                                               direct ? 1 : 0, dtype == SX_F64, (double*)scratch, grad_velocity,
+                                               (cudaStream_t)stream);
+    if (err != cudaSuccess) return cuda_fail(err, "sx_upwind_adjoint");
+    return SX_OK;
+}
+
 int sx_threshold_rle(const float* values, int32_t width, int32_t height, float threshold, int gradient, int32_t* counts,
                      const int32_t* offsets, int32_t* out_begin, int32_t* out_end, void* stream)
 {

@@ -421,6 +421,145 @@ __global__ void __launch_bounds__(256) sx_upwind_kernel(const int* __restrict__ 
     }
 }
 
+// ---------------------------------------------------------------------------
+// Adjoint of the upwind step (no reference counterpart).  For fixed
+// velocity the step is linear, u' = u - dt (a Dx u + b Dy u), where Dx, Dy
+// are the one-sided differences chosen by the signs of a and b, with zero
+// exterior.  Given w = dL/du', this kernel writes dL/du = w - dt (a Dx^T w
+// + b Dy^T w) and per-block float64 partial sums of dL/da = sum w (-dt Dx u)
+// and dL/db = sum w (-dt Dy u), dt held fixed.
+//
+// The transpose mirrors the forward validity rules exactly: cell i reads
+// its left neighbour j only when j is in the set and inside the domain, so
+// j receives w_i from the cell to its right whenever that cell is in the set
+// (whatever its own position) and j is inside the domain.
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T sx_in_set(int row, int x, int height, const int* __restrict__ lookup,
+                                       const int* __restrict__ off, const int* __restrict__ b,
+                                       const int* __restrict__ e, const int* __restrict__ coff,
+                                       const T* __restrict__ v)
+{
+    if (row < 0 || row >= height) return (T)0;
+    const int ord = lookup[row];
+    if (ord < 0) return (T)0;
+    int lo = off[ord], hi = off[ord + 1] - 1;
+    while (lo <= hi) {
+        const int mid = (lo + hi) >> 1;
+        if (x < b[mid]) hi = mid - 1;
+        else if (x >= e[mid]) lo = mid + 1;
+        else return v[coff[mid] + (x - b[mid])];
+    }
+    return (T)0;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) sx_upwind_adjoint_kernel(const int* __restrict__ rows,
+                                                                const int* __restrict__ off, int row_count,
+                                                                const int* __restrict__ b, const int* __restrict__ e,
+                                                                const int* __restrict__ coff, int n,
+                                                                const int* __restrict__ lookup,
+                                                                const T* __restrict__ w, const T* __restrict__ u,
+                                                                T* __restrict__ ubar, int width, int height, T a, T bb,
+                                                                T dt, T dx, T dy, int direct, long long value_count,
+                                                                double* __restrict__ partial)
+{
+    __shared__ int s_i, s_p;
+    __shared__ double s_ga[256 / 32], s_gb[256 / 32];
+    const long long cells = coff[n] < value_count ? (long long)coff[n] : value_count;
+    double ga = 0.0, gb = 0.0;
+    for (long long c0 = (long long)blockIdx.x * blockDim.x; c0 < cells; c0 += (long long)gridDim.x * blockDim.x) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int lo = 0, hi = n - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (coff[mid] <= c0) lo = mid; else hi = mid - 1;
+            }
+            s_i = lo;
+            s_p = sx_row_of(off, row_count, lo);
+        }
+        __syncthreads();
+        const long long c = c0 + threadIdx.x;
+        if (c >= cells) continue;
+        int i = s_i, p = s_p;
+        while (coff[i + 1] <= c) ++i;
+        while (off[p + 1] <= i) ++p;
+        const int row = rows[p];
+        const int ib = b[i], ie = e[i];
+        const int x = ib + (int)(c - coff[i]);
+        const bool jdom = x >= 0 && x < width && row >= 0 && row < height;
+        const T wc = w[c];
+        // transpose of the x difference
+        T tx;
+        if (a >= (T)0) {
+            T wr = (T)0;
+            if (jdom) wr = (direct && x + 1 < ie) ? w[c + 1] : sx_in_set<T>(row, x + 1, height, lookup, off, b, e, coff, w);
+            tx = sx_div(sx_sub(wc, wr), dx);
+        } else {
+            T wl = (T)0;
+            if (jdom) wl = (direct && x - 1 >= ib) ? w[c - 1] : sx_in_set<T>(row, x - 1, height, lookup, off, b, e, coff, w);
+            tx = sx_div(sx_sub(wl, wc), dx);
+        }
+        // transpose of the y difference
+        T ty;
+        if (bb >= (T)0) {
+            const T wu = jdom ? sx_in_set<T>(row + 1, x, height, lookup, off, b, e, coff, w) : (T)0;
+            ty = sx_div(sx_sub(wc, wu), dy);
+        } else {
+            const T wd = jdom ? sx_in_set<T>(row - 1, x, height, lookup, off, b, e, coff, w) : (T)0;
+            ty = sx_div(sx_sub(wd, wc), dy);
+        }
+        ubar[c] = sx_sub(wc, sx_mul(dt, sx_add(sx_mul(a, tx), sx_mul(bb, ty))));
+        // forward differences of u for the velocity gradient (forward validity rules)
+        const T uc = u[c];
+        T ul, ur;
+        if (direct && x - 1 >= ib) ul = (x - 1 >= 0 && x - 1 < width) ? u[c - 1] : (T)0;
+        else ul = sx_sample<T>(row, x - 1, height, width, lookup, off, b, e, coff, u);
+        if (direct && x + 1 < ie) ur = (x + 1 >= 0 && x + 1 < width) ? u[c + 1] : (T)0;
+        else ur = sx_sample<T>(row, x + 1, height, width, lookup, off, b, e, coff, u);
+        const T ud = sx_sample<T>(row - 1, x, height, width, lookup, off, b, e, coff, u);
+        const T uu = sx_sample<T>(row + 1, x, height, width, lookup, off, b, e, coff, u);
+        const T dux = a >= (T)0 ? sx_div(sx_sub(uc, ul), dx) : sx_div(sx_sub(ur, uc), dx);
+        const T duy = bb >= (T)0 ? sx_div(sx_sub(uc, ud), dy) : sx_div(sx_sub(uu, uc), dy);
+        ga -= (double)dt * (double)wc * (double)dux;
+        gb -= (double)dt * (double)wc * (double)duy;
+    }
+    // block reduction of the velocity gradients, fixed order
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        ga += __shfl_down_sync(0xFFFFFFFFu, ga, o);
+        gb += __shfl_down_sync(0xFFFFFFFFu, gb, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        s_ga[threadIdx.x >> 5] = ga;
+        s_gb[threadIdx.x >> 5] = gb;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double ta = 0.0, tb = 0.0;
+        for (int q = 0; q < 256 / 32; ++q) {
+            ta += s_ga[q];
+            tb += s_gb[q];
+        }
+        partial[2 * blockIdx.x] = ta;
+        partial[2 * blockIdx.x + 1] = tb;
+    }
+}
+
+__global__ void sx_sum_pairs_kernel(const double* __restrict__ partial, int parts, double* __restrict__ out)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        double sa = 0.0, sb = 0.0;
+        for (int q = 0; q < parts; ++q) {
+            sa += partial[2 * q];
+            sb += partial[2 * q + 1];
+        }
+        out[0] = sa;
+        out[1] = sb;
+    }
+}
+
 __global__ void sx_row_lookup_kernel(const int* __restrict__ rows, int row_count, int height, int* __restrict__ lookup,
                                      int* __restrict__ flags)
 {
@@ -893,5 +1032,34 @@ cudaError_t sx_mass_launch(const void* v, long long n, int dbl, double scale, do
     if (dbl) sx_mass_partial_kernel<double><<<parts, SX_BLOCK, 0, stream>>>((const double*)v, n, part);
     else sx_mass_partial_kernel<float><<<parts, SX_BLOCK, 0, stream>>>((const float*)v, n, part);
     sx_mass_final_kernel<<<1, 32, 0, stream>>>(part, parts, scale, out);
+    return cudaGetLastError();
+}
+
+int sx_upwind_adjoint_parts(long long cells)
+{
+    long long g = (cells + 255) / 256;
+    if (g < 1) g = 1;
+    if (g > 148 * 16) g = 148 * 16;
+    return (int)g;
+}
+
+cudaError_t sx_upwind_adjoint_launch(const int* rows, const int* off, int row_count, const int* b, const int* e,
+                                     const int* coff, int n, long long cells, const int* lookup, const void* w,
+                                     const void* u, void* ubar, int width, int height, double a, double bb, double dt,
+                                     double dx, double dy, int direct, int dbl, double* partial, double* grads,
+                                     cudaStream_t stream)
+{
+    const int grid = sx_upwind_adjoint_parts(cells);
+    if (dbl)
+        sx_upwind_adjoint_kernel<double><<<grid, 256, 0, stream>>>(rows, off, row_count, b, e, coff, n, lookup,
+                                                                   (const double*)w, (const double*)u, (double*)ubar,
+                                                                   width, height, a, bb, dt, dx, dy, direct, cells,
+                                                                   partial);
+    else
+        sx_upwind_adjoint_kernel<float><<<grid, 256, 0, stream>>>(rows, off, row_count, b, e, coff, n, lookup,
+                                                                  (const float*)w, (const float*)u, (float*)ubar, width,
+                                                                  height, (float)a, (float)bb, (float)dt, (float)dx,
+                                                                  (float)dy, direct, cells, partial);
+    sx_sum_pairs_kernel<<<1, 32, 0, stream>>>(partial, grid, grads);
     return cudaGetLastError();
 }

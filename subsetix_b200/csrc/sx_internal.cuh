@@ -125,3 +125,9 @@ cudaError_t sx_amr_regrid_full_launch(int dbl, const void* coarse, unsigned char
 cudaError_t sx_amr_step_full_launch(int dbl, const void* cin, const void* fin, void* cout, void* fout,
                                     const signed char* actions, int W, int H, int batch, double a, double b, double dt,
                                     double dxc, double dyc, double dxf, double dyf, cudaStream_t stream);
+int sx_upwind_adjoint_parts(long long cells);
+cudaError_t sx_upwind_adjoint_launch(const int* rows, const int* off, int row_count, const int* b, const int* e,
+                                     const int* coff, int n, long long cells, const int* lookup, const void* w,
+                                     const void* u, void* ubar, int width, int height, double a, double bb, double dt,
+                                     double dx, double dy, int direct, int dbl, double* partial, double* grads,
+                                     cudaStream_t stream);

@@ -234,3 +234,22 @@ def concat_sets(sets: Sequence[HostSet], row_strides: Sequence[int]) -> HostSet:
             np.concatenate(ends).astype(np.int32) if ends else np.zeros(0, np.int32),
             off.astype(np.int32),
             np.concatenate(rows_list).astype(np.int32) if rows_list else np.zeros(0, np.int32))
+
+
+def disk_rows(size: int, radius: float, cx: float | None = None, cy: float | None = None) -> HostSet:
+    """Disk of cells whose centres lie within ``radius`` of ``(cx, cy)`` (cell units), built row by row.
+
+    Rows that the disk misses are left out; each kept row holds one interval.
+    """
+    cx = size / 2.0 if cx is None else cx
+    cy = size / 2.0 if cy is None else cy
+    ys = np.arange(size, dtype=np.float64)
+    dy = ys + 0.5 - cy
+    inside = dy * dy <= radius * radius
+    hw = np.sqrt(np.maximum(radius * radius - dy * dy, 0.0))
+    x0 = np.maximum(np.ceil(cx - hw - 0.5), 0).astype(np.int64)
+    x1 = np.minimum(np.floor(cx + hw - 0.5), size - 1).astype(np.int64) + 1
+    keep = inside & (x1 > x0)
+    rows = np.nonzero(keep)[0]
+    off = np.arange(rows.size + 1, dtype=np.int64)
+    return x0[keep].astype(np.int32), x1[keep].astype(np.int32), off.astype(np.int32), rows.astype(np.int32)
