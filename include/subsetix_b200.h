@@ -315,6 +315,26 @@ int sx_upwind(int dtype, const int32_t* rows, const int32_t* row_ids, const int3
               const int32_t* begin, const int32_t* end, const int32_t* cell_offsets, int64_t n, int64_t cells, const int32_t* lookup,
               const void* values, void* out, int32_t width, int32_t height, double a, double b, double dt, double dx,
               double dy, int direct, void* stream);
+/* Chunked form of sx_upwind for fixed geometry whose rows are sorted and
+ * disjoint (sx_check_rows reports no UNSORTED_BEGIN, OVERLAP or EMPTY); same
+ * results.  A plan is built once per geometry:
+ *   sx_upwind_plan       chunk_offsets[n + 1] = exclusive scan of
+ *                        ceil(len / 128) per interval; result = {chunks,
+ *                        flags}; workspace: sx_scan_workspace_bytes(n);
+ *   sx_upwind_plan_fill  chunk_info[8 * chunks] (16-byte aligned): per
+ *                        128-cell chunk its interval, its index in the
+ *                        interval, its row, and where the rows above and
+ *                        below start to overlap it (lookup as for sx_upwind).
+ * Each step is then sx_upwind_chunked (values != out). */
+int sx_upwind_plan(const int32_t* begin, const int32_t* end, int64_t n, int32_t* chunk_offsets, int32_t* result,
+                   void* workspace, size_t workspace_bytes, void* stream);
+int sx_upwind_plan_fill(const int32_t* rows, const int32_t* row_offsets, int32_t row_count, const int32_t* begin,
+                        const int32_t* end, int64_t n, const int32_t* chunk_offsets, int64_t chunks,
+                        const int32_t* lookup, int32_t height, int32_t* chunk_info, void* stream);
+int sx_upwind_chunked(int dtype, const int32_t* row_offsets, const int32_t* begin, const int32_t* end,
+                      const int32_t* cell_offsets, const int32_t* chunk_info, int64_t chunks, const int32_t* lookup,
+                      const void* values, void* out, int32_t width, int32_t height, double a, double b, double dt,
+                      double dx, double dy, void* stream);
 int sx_upwind_f32(const int32_t* rows, const int32_t* row_offsets, int32_t row_count, const int32_t* begin,
                   const int32_t* end, const int32_t* cell_offsets, int64_t n, int64_t cells, const int32_t* lookup,
                   const float* values, float* out, int32_t width, int32_t height, float a, float b, float dt, float dx,
@@ -337,6 +357,16 @@ int sx_upwind_adjoint(int dtype, const int32_t* rows, const int32_t* row_offsets
                       const int32_t* lookup, const void* grad_out, const void* values, void* grad_in, int32_t width,
                       int32_t height, double a, double b, double dt, double dx, double dy, int direct,
                       double* grad_velocity, void* scratch, size_t scratch_bytes, void* stream);
+
+/* sx_upwind_adjoint on a chunk plan (sx_upwind_plan / sx_upwind_plan_fill;
+ * rows sorted and disjoint); same values.  scratch:
+ * sx_upwind_adjoint_chunked_scratch_bytes(chunks) bytes. */
+size_t sx_upwind_adjoint_chunked_scratch_bytes(int64_t chunks);
+int sx_upwind_adjoint_chunked(int dtype, const int32_t* row_offsets, const int32_t* begin, const int32_t* end,
+                              const int32_t* cell_offsets, const int32_t* chunk_info, int64_t chunks,
+                              const int32_t* lookup, const void* grad_out, const void* values, void* grad_in,
+                              int32_t width, int32_t height, double a, double b, double dt, double dx, double dy,
+                              double* grad_velocity, void* scratch, size_t scratch_bytes, void* stream);
 
 /* Threshold run-length encoding of a full width x height float32 grid
  * (subsetix_amr2/regrid.py:20-124 K11/K12, and regrid.py:172-223 K14 when

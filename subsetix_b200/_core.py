@@ -333,6 +333,35 @@ def upwind(rows, offsets, begin, end, cell_offs, cells: int, lookup, values, out
                              1 if direct else 0, stream_handle(device)), "sx_upwind")
 
 
+def upwind_plan(rows, offsets, begin, end, lookup, height: int, device):
+    """Plan of sx_upwind_chunked for a fixed geometry: ``(chunk_info, chunks)`` (one synchronisation)."""
+    lib = _lib.load()
+    n = int(begin.numel())
+    chunk_off = empty_i32(n + 1, device)
+    result = empty_i32(2, device)
+    wsp, wsn = workspace(device, lib.sx_scan_workspace_bytes(n))
+    s = stream_handle(device)
+    _lib.check(lib.sx_upwind_plan(ptr(begin), ptr(end), n, ptr(chunk_off), ptr(result), wsp, wsn, s),
+               "sx_upwind_plan")
+    chunks, flags = read_pair(result)
+    if flags & _lib.FLAG_TIMEOUT:
+        raise _lib.SubsetixError("sx_upwind_plan: look-back wait timed out")
+    info = empty_i32(8 * max(chunks, 1), device)
+    _lib.check(lib.sx_upwind_plan_fill(ptr(rows), ptr(offsets), int(rows.numel()), ptr(begin), ptr(end), n,
+                                       ptr(chunk_off), chunks, ptr(lookup), int(height), ptr(info), s),
+               "sx_upwind_plan_fill")
+    return info, chunks
+
+
+def upwind_chunked(offsets, begin, end, cell_offs, chunk_info, chunks: int, lookup, values, out, width: int,
+                   height: int, a, b, dt, dx, dy, device):
+    lib = _lib.load()
+    _lib.check(lib.sx_upwind_chunked(_dtype_code(values), ptr(offsets), ptr(begin), ptr(end), ptr(cell_offs),
+                                     ptr(chunk_info), int(chunks), ptr(lookup), ptr(values), ptr(out), int(width),
+                                     int(height), float(a), float(b), float(dt), float(dx), float(dy),
+                                     stream_handle(device)), "sx_upwind_chunked")
+
+
 def threshold_rle(values, width: int, height: int, threshold: float, gradient: bool, device):
     """Runs of value >= threshold per row of a full grid.  Returns ``(begin, end, offsets)`` (synchronising)."""
     lib = _lib.load()

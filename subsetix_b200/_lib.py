@@ -96,6 +96,12 @@ _SIGNATURES = {
                                  ctypes.c_int64, c_vp, c_vp, c_vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
                                  ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                  c_vp]),
+    "sx_upwind_plan": (ctypes.c_int, [c_vp, c_vp, ctypes.c_int64, c_vp, c_vp, c_vp, ctypes.c_size_t, c_vp]),
+    "sx_upwind_plan_fill": (ctypes.c_int, [c_vp, c_vp, ctypes.c_int32, c_vp, c_vp, ctypes.c_int64, c_vp,
+                                           ctypes.c_int64, c_vp, ctypes.c_int32, c_vp, c_vp]),
+    "sx_upwind_chunked": (ctypes.c_int, [ctypes.c_int, c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.c_int64, c_vp, c_vp, c_vp,
+                                         ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
+                                         ctypes.c_double, ctypes.c_double, ctypes.c_double, c_vp]),
     "sx_upwind_f32": (ctypes.c_int, [c_vp, c_vp, ctypes.c_int32, c_vp, c_vp, c_vp, ctypes.c_int64, ctypes.c_int64,
                                      c_vp, c_vp, c_vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_float, ctypes.c_float,
                                      ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_int, c_vp]),
@@ -108,6 +114,11 @@ _SIGNATURES = {
                                          ctypes.c_int64, c_vp, c_vp, c_vp, c_vp, ctypes.c_int32, ctypes.c_int32,
                                          ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                          ctypes.c_double, ctypes.c_int, c_vp, c_vp, ctypes.c_size_t, c_vp]),
+    "sx_upwind_adjoint_chunked_scratch_bytes": (ctypes.c_size_t, [ctypes.c_int64]),
+    "sx_upwind_adjoint_chunked": (ctypes.c_int, [ctypes.c_int, c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.c_int64, c_vp,
+                                                 c_vp, c_vp, c_vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
+                                                 ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                                 c_vp, c_vp, ctypes.c_size_t, c_vp]),
     "sx_threshold_rle": (ctypes.c_int, [c_vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_float, ctypes.c_int, c_vp,
                                         c_vp, c_vp, c_vp, c_vp]),
     "sx_gradient_magnitude": (ctypes.c_int, [c_vp, ctypes.c_int32, ctypes.c_int32, c_vp, c_vp]),

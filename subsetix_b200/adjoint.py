@@ -49,14 +49,21 @@ class Level:
         if bad:
             raise ValueError("interval_set rows exceed provided height")
         self.direct = not (_core.check_rows(self.begin, self.end, self.off, device) & _ROWS_UNSAFE)
+        self.chunk_off, self.chunks = (_core.upwind_plan(self.rows, self.off, self.begin, self.end, self.lookup,
+                                                         self.height, device) if self.direct else (None, 0))
         self.device = device
         lib = _lib.load()
-        self.scratch = torch.empty(int(lib.sx_upwind_adjoint_scratch_bytes(self.cells)), dtype=torch.uint8,
-                                   device=device)
+        nbytes = max(int(lib.sx_upwind_adjoint_scratch_bytes(self.cells)),
+                     int(lib.sx_upwind_adjoint_chunked_scratch_bytes(self.chunks)))
+        self.scratch = torch.empty(nbytes, dtype=torch.uint8, device=device)
 
     def step(self, u: torch.Tensor, out: torch.Tensor, a: float, b: float, dt: float) -> torch.Tensor:
-        _core.upwind(self.rows, self.off, self.begin, self.end, self.cell_off, self.cells, self.lookup, u, out,
-                     self.width, self.height, a, b, dt, self.dx, self.dy, self.direct, self.device)
+        if self.chunk_off is not None:
+            _core.upwind_chunked(self.off, self.begin, self.end, self.cell_off, self.chunk_off, self.chunks,
+                                 self.lookup, u, out, self.width, self.height, a, b, dt, self.dx, self.dy, self.device)
+        else:
+            _core.upwind(self.rows, self.off, self.begin, self.end, self.cell_off, self.cells, self.lookup, u, out,
+                         self.width, self.height, a, b, dt, self.dx, self.dy, self.direct, self.device)
         return out
 
     def adjoint(self, w: torch.Tensor, u: torch.Tensor, a: float, b: float, dt: float, grad_ab: torch.Tensor
@@ -66,6 +73,15 @@ class Level:
         ubar = torch.empty_like(w)
         g = torch.empty(2, dtype=torch.float64, device=self.device)
         code = _lib.SX_F64 if w.dtype == torch.float64 else _lib.SX_F32
+        if self.chunk_off is not None:
+            _lib.check(lib.sx_upwind_adjoint_chunked(code, ptr(self.off), ptr(self.begin), ptr(self.end),
+                                                     ptr(self.cell_off), ptr(self.chunk_off), self.chunks,
+                                                     ptr(self.lookup), ptr(w), ptr(u), ptr(ubar), self.width,
+                                                     self.height, a, b, dt, self.dx, self.dy, ptr(g),
+                                                     ptr(self.scratch), int(self.scratch.numel()),
+                                                     stream_handle(self.device)), "sx_upwind_adjoint_chunked")
+            grad_ab += g
+            return ubar
         _lib.check(lib.sx_upwind_adjoint(code, ptr(self.rows), ptr(self.off), int(self.rows.numel()), ptr(self.begin),
                                          ptr(self.end), ptr(self.cell_off), int(self.begin.numel()), self.cells,
                                          ptr(self.lookup), ptr(w), ptr(u), ptr(ubar), self.width, self.height, a, b,

@@ -445,6 +445,55 @@ int sx_upwind(int dtype, const int32_t* rows, const int32_t* row_ids, const int3
     return SX_OK;
 }
 
+int sx_upwind_plan(const int32_t* begin, const int32_t* end, int64_t n, int32_t* chunk_offsets, int32_t* result,
+                   void* workspace, size_t workspace_bytes, void* stream)
+{
+    if (n < 0 || n > INT32_MAX) return fail(SX_ERR_INVALID, "sx_upwind_plan: bad size");
+    if (!chunk_offsets || !result || (n > 0 && (!begin || !end))) return fail(SX_ERR_INVALID, "sx_upwind_plan: null argument");
+    const long long tiles = sx_scan_tiles(n);
+    if (!workspace || workspace_bytes < scan_state_bytes(tiles))
+        return fail(SX_ERR_WORKSPACE, "sx_upwind_plan: workspace needs %zu bytes", scan_state_bytes(tiles));
+    cudaError_t err = sx_upwind_plan_launch(begin, end, (int)n, chunk_offsets, result, scan_state(workspace, tiles),
+                                            (cudaStream_t)stream);
+    if (err != cudaSuccess) return cuda_fail(err, "sx_upwind_plan");
+    return SX_OK;
+}
+
+int sx_upwind_plan_fill(const int32_t* rows, const int32_t* row_offsets, int32_t row_count, const int32_t* begin,
+                        const int32_t* end, int64_t n, const int32_t* chunk_offsets, int64_t chunks,
+                        const int32_t* lookup, int32_t height, int32_t* chunk_info, void* stream)
+{
+    if (row_count < 0 || n < 0 || n > INT32_MAX || chunks < 0 || height <= 0)
+        return fail(SX_ERR_INVALID, "sx_upwind_plan_fill: bad size");
+    if (n == 0 || chunks == 0) return SX_OK;
+    if (!rows || !row_offsets || !begin || !end || !chunk_offsets || !lookup || !chunk_info)
+        return fail(SX_ERR_INVALID, "sx_upwind_plan_fill: null argument");
+    if (((uintptr_t)chunk_info & 15u) != 0) return fail(SX_ERR_INVALID, "sx_upwind_plan_fill: chunk_info must be 16-byte aligned");
+    cudaError_t err = sx_upwind_plan_fill_launch(rows, row_offsets, row_count, begin, end, (int)n, chunk_offsets, chunks,
+                                                 lookup, height, chunk_info, (cudaStream_t)stream);
+    if (err != cudaSuccess) return cuda_fail(err, "sx_upwind_plan_fill");
+    return SX_OK;
+}
+
+int sx_upwind_chunked(int dtype, const int32_t* row_offsets, const int32_t* begin, const int32_t* end,
+                      const int32_t* cell_offsets, const int32_t* chunk_info, int64_t chunks, const int32_t* lookup,
+                      const void* values, void* out, int32_t width, int32_t height, double a, double b, double dt,
+                      double dx, double dy, void* stream)
+{
+    if (dtype != SX_F32 && dtype != SX_F64) return fail(SX_ERR_INVALID, "sx_upwind_chunked: dtype %d", dtype);
+    if (width <= 0 || height <= 0) return fail(SX_ERR_INVALID, "sx_upwind_chunked: width and height must be positive");
+    if (chunks < 0) return fail(SX_ERR_INVALID, "sx_upwind_chunked: bad size");
+    if (chunks == 0) return SX_OK;
+    if (!row_offsets || !begin || !end || !cell_offsets || !chunk_info || !lookup || !values || !out)
+        return fail(SX_ERR_INVALID, "sx_upwind_chunked: null argument");
+    if (((uintptr_t)chunk_info & 15u) != 0) return fail(SX_ERR_INVALID, "sx_upwind_chunked: chunk_info must be 16-byte aligned");
+    if (values == out) return fail(SX_ERR_INVALID, "sx_upwind_chunked: out must not alias values");
+    cudaError_t err = sx_upwind_chunk_launch(row_offsets, begin, end, cell_offsets, chunk_info, chunks, lookup, values,
+                                             out, width, height, a, b, dt, dx, dy, dtype == SX_F64, (cudaStream_t)stream);
+    if (err != cudaSuccess) return cuda_fail(err, "sx_upwind_chunked");
+    return SX_OK;
+}
+
 int sx_upwind_f32(const int32_t* rows, const int32_t* row_offsets, int32_t row_count, const int32_t* begin,
                   const int32_t* end, const int32_t* cell_offsets, int64_t n, int64_t cells, const int32_t* lookup,
                   const float* values, float* out, int32_t width, int32_t height, float a, float b, float dt, float dx,
@@ -492,6 +541,40 @@ int sx_upwind_adjoint(int dtype, const int32_t* rows, const int32_t* row_offsets
                                                direct ? 1 : 0, dtype == SX_F64, (double*)scratch, grad_velocity,
                                                (cudaStream_t)stream);
     if (err != cudaSuccess) return cuda_fail(err, "sx_upwind_adjoint");
+    return SX_OK;
+}
+
+size_t sx_upwind_adjoint_chunked_scratch_bytes(int64_t chunks)
+{
+    return (size_t)sx_upwind_adjoint_chunk_parts(chunks) * 2 * sizeof(double);
+}
+
+int sx_upwind_adjoint_chunked(int dtype, const int32_t* row_offsets, const int32_t* begin, const int32_t* end,
+                              const int32_t* cell_offsets, const int32_t* chunk_info, int64_t chunks,
+                              const int32_t* lookup, const void* grad_out, const void* values, void* grad_in,
+                              int32_t width, int32_t height, double a, double b, double dt, double dx, double dy,
+                              double* grad_velocity, void* scratch, size_t scratch_bytes, void* stream)
+{
+    if (dtype != SX_F32 && dtype != SX_F64) return fail(SX_ERR_INVALID, "sx_upwind_adjoint_chunked: dtype %d", dtype);
+    if (width <= 0 || height <= 0) return fail(SX_ERR_INVALID, "sx_upwind_adjoint_chunked: width and height must be positive");
+    if (chunks < 0) return fail(SX_ERR_INVALID, "sx_upwind_adjoint_chunked: bad size");
+    if (!grad_velocity) return fail(SX_ERR_INVALID, "sx_upwind_adjoint_chunked: null grad_velocity");
+    if (chunks == 0) {
+        cudaError_t err = cudaMemsetAsync(grad_velocity, 0, 2 * sizeof(double), (cudaStream_t)stream);
+        return err == cudaSuccess ? SX_OK : cuda_fail(err, "sx_upwind_adjoint_chunked");
+    }
+    if (!row_offsets || !begin || !end || !cell_offsets || !chunk_info || !lookup || !grad_out || !values || !grad_in)
+        return fail(SX_ERR_INVALID, "sx_upwind_adjoint_chunked: null argument");
+    if (((uintptr_t)chunk_info & 15u) != 0)
+        return fail(SX_ERR_INVALID, "sx_upwind_adjoint_chunked: chunk_info must be 16-byte aligned");
+    if (!scratch || scratch_bytes < sx_upwind_adjoint_chunked_scratch_bytes(chunks))
+        return fail(SX_ERR_WORKSPACE, "sx_upwind_adjoint_chunked: scratch needs %zu bytes",
+                    sx_upwind_adjoint_chunked_scratch_bytes(chunks));
+    cudaError_t err = sx_upwind_adjoint_chunk_launch(row_offsets, begin, end, cell_offsets, chunk_info, chunks, lookup,
+                                                     grad_out, values, grad_in, width, height, a, b, dt, dx, dy,
+                                                     dtype == SX_F64, (double*)scratch, grad_velocity,
+                                                     (cudaStream_t)stream);
+    if (err != cudaSuccess) return cuda_fail(err, "sx_upwind_adjoint_chunked");
     return SX_OK;
 }
 

@@ -560,6 +560,296 @@ __global__ void sx_sum_pairs_kernel(const double* __restrict__ partial, int part
     }
 }
 
+// ---------------------------------------------------------------------------
+// Upwind, chunked form, for rows whose intervals are sorted and disjoint
+// (touching allowed).  Same results as sx_upwind_kernel.  Work is split
+// into chunks of SX_CHUNK = 128 consecutive cells of one interval
+// (`chunk_off[i]` is the first chunk of interval i); a warp takes a
+// contiguous range of chunks and covers a chunk in four sub-rounds of 32
+// cells, so every load is coalesced and the four sub-rounds' loads are
+// independent.  Left and right neighbours come from the neighbouring lanes
+// (or the neighbouring sub-round); for the rows above and below, the warp
+// finds the first interval ending after the chunk's first cell once per
+// chunk, then each lane steps forward through intervals ending inside the
+// chunk (fewer than 128: they are disjoint and non-empty).
+// ---------------------------------------------------------------------------
+#define SX_CHUNK 128
+#define SX_CHUNK_SUB (SX_CHUNK / 32)
+
+__global__ void sx_chunk_count_kernel(const int* __restrict__ b, const int* __restrict__ e, int n,
+                                      int* __restrict__ counts)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const long long len = (long long)e[i] - b[i];
+        counts[i] = len > 0 ? (int)((len + SX_CHUNK - 1) / SX_CHUNK) : 0;
+    }
+}
+
+// Neighbour-row reader: first interval of row `row` ending after x0 (warp-uniform search).
+struct SxRowCursor {
+    int j, je;
+};
+
+__device__ __forceinline__ SxRowCursor sx_row_cursor(int row, int x0, int height, const int* __restrict__ lookup,
+                                                     const int* __restrict__ off, const int* __restrict__ e)
+{
+    SxRowCursor cur{0, 0};
+    if (row < 0 || row >= height) return cur;
+    const int ord = lookup[row];
+    if (ord < 0) return cur;
+    int lo = off[ord], hi = off[ord + 1];
+    const int je = hi;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (e[mid] <= x0) lo = mid + 1; else hi = mid;
+    }
+    cur.j = lo;
+    cur.je = je;
+    return cur;
+}
+
+// Value at column x of a neighbour row.  The cursor keeps the current
+// interval's bounds and cell offset in registers and reloads them only when
+// it steps (x non-decreasing between calls of one lane).
+struct SxRowReader {
+    int j, je, cb, ce, cc;
+};
+
+__device__ __forceinline__ SxRowReader sx_row_reader(int j, int je, const int* __restrict__ b,
+                                                     const int* __restrict__ e, const int* __restrict__ coff)
+{
+    SxRowReader r{j, je, 0, 0, 0};
+    if (j < je) {
+        r.cb = b[j];
+        r.ce = e[j];
+        r.cc = coff[j];
+    }
+    return r;
+}
+
+template <typename T>
+__device__ __forceinline__ T sx_row_take(SxRowReader& r, int x, int width, const int* __restrict__ b,
+                                         const int* __restrict__ e, const int* __restrict__ coff,
+                                         const T* __restrict__ v, bool act)
+{
+    while (r.j < r.je && r.ce <= x) {
+        ++r.j;
+        if (r.j < r.je) {
+            r.cb = b[r.j];
+            r.ce = e[r.j];
+            r.cc = coff[r.j];
+        }
+    }
+    if (!act || r.j >= r.je || r.cb > x || x < 0 || x >= width) return (T)0;
+    return v[r.cc + (x - r.cb)];
+}
+
+// Per-chunk plan: info[8u .. 8u+7] = (interval, chunk within it, row id,
+// first interval of the row below ending after the chunk's first cell, end
+// of that row's intervals, the same two for the row above, 0).  Depends only
+// on the geometry, so it is built once per set.
+__global__ void sx_chunk_info_kernel(const int* __restrict__ rows, const int* __restrict__ off, int row_count,
+                                     const int* __restrict__ b, const int* __restrict__ e, int n,
+                                     const int* __restrict__ chunk_off, long long chunks,
+                                     const int* __restrict__ lookup, int height, int* __restrict__ info)
+{
+    for (long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x; u < chunks;
+         u += (long long)gridDim.x * blockDim.x) {
+        int lo = 0, hi = n - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (chunk_off[mid] <= u) lo = mid; else hi = mid - 1;
+        }
+        const int i = lo;
+        const int k = (int)(u - chunk_off[i]);
+        const int row = rows[sx_row_of(off, row_count, i)];
+        const int x0 = b[i] + SX_CHUNK * k;
+        const SxRowCursor dn = sx_row_cursor(row - 1, x0, height, lookup, off, e);
+        const SxRowCursor up = sx_row_cursor(row + 1, x0, height, lookup, off, e);
+        int4* o = (int4*)(info + 8 * u);
+        o[0] = make_int4(i, k, row, dn.j);
+        o[1] = make_int4(dn.je, up.j, up.je, 0);
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) sx_upwind_chunk_kernel(const int* __restrict__ off,
+                                                              const int* __restrict__ b, const int* __restrict__ e,
+                                                              const int* __restrict__ coff,
+                                                              const int* __restrict__ info, long long chunks,
+                                                              const int* __restrict__ lookup,
+                                                              const T* __restrict__ v, T* __restrict__ out, int width,
+                                                              int height, T a, T bb, T dt, T dx, T dy)
+{
+    const int lane = threadIdx.x & 31;
+    const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long u = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); u < chunks; u += warps) {
+        const int4 p0 = __ldg((const int4*)(info + 8 * u));
+        const int4 p1 = __ldg((const int4*)(info + 8 * u) + 1);
+        const int i = p0.x, k = p0.y, row = p0.z;
+        const int ib = b[i], ie = e[i];
+        const int x0 = ib + SX_CHUNK * k;
+        const long long c0 = (long long)coff[i] + (long long)SX_CHUNK * k;
+        T cen[SX_CHUNK_SUB];
+#pragma unroll
+        for (int q = 0; q < SX_CHUNK_SUB; ++q) {
+            const int x = x0 + 32 * q + lane;
+            cen[q] = x < ie ? v[c0 + 32 * q + lane] : (T)0;
+        }
+        SxRowReader dn = sx_row_reader(p0.w, p1.x, b, e, coff);
+        SxRowReader upc = sx_row_reader(p1.y, p1.z, b, e, coff);
+        T prev_last = (T)0;  // lane 31's centre of the previous sub-round
+#pragma unroll
+        for (int q = 0; q < SX_CHUNK_SUB; ++q) {
+            const int x = x0 + 32 * q + lane;
+            const bool act = x < ie;
+            const long long c = c0 + 32 * q + lane;
+            const T center = cen[q];
+            T from_left = __shfl_up_sync(0xFFFFFFFFu, center, 1);
+            if (lane == 0) from_left = prev_last;
+            T from_right = __shfl_down_sync(0xFFFFFFFFu, center, 1);
+            const T next_first = q + 1 < SX_CHUNK_SUB ? __shfl_sync(0xFFFFFFFFu, cen[q + 1 < SX_CHUNK_SUB ? q + 1 : q], 0)
+                                                      : (T)0;
+            if (lane == 31) from_right = next_first;
+            prev_last = __shfl_sync(0xFFFFFFFFu, center, 31);
+            T left, right;
+            if (x - 1 >= ib) left = (x - 1 >= 0 && x - 1 < width) ? ((lane > 0 || q > 0) ? from_left : v[c - 1]) : (T)0;
+            else left = act ? sx_sample<T>(row, x - 1, height, width, lookup, off, b, e, coff, v) : (T)0;
+            if (x + 1 < ie)
+                right = (x + 1 >= 0 && x + 1 < width) ? ((lane < 31 || q + 1 < SX_CHUNK_SUB) ? from_right : v[c + 1])
+                                                      : (T)0;
+            else right = act ? sx_sample<T>(row, x + 1, height, width, lookup, off, b, e, coff, v) : (T)0;
+            const T down = sx_row_take<T>(dn, x, width, b, e, coff, v, act);
+            const T up = sx_row_take<T>(upc, x, width, b, e, coff, v, act);
+            if (act) {
+                const T du_dx = a >= (T)0 ? sx_div(sx_sub(center, left), dx) : sx_div(sx_sub(right, center), dx);
+                const T du_dy = bb >= (T)0 ? sx_div(sx_sub(center, down), dy) : sx_div(sx_sub(up, center), dy);
+                out[c] = sx_sub(center, sx_mul(dt, sx_add(sx_mul(a, du_dx), sx_mul(bb, du_dy))));
+            }
+        }
+    }
+}
+
+// Adjoint of the upwind step on a chunk plan (rows sorted and disjoint);
+// same values as sx_upwind_adjoint_kernel.  One row reader per direction
+// serves both arrays (w and u share the geometry).  Per-block float64
+// partial sums of dL/da, dL/db go to partial[2 * block].
+template <typename T>
+__global__ void __launch_bounds__(256) sx_upwind_adjoint_chunk_kernel(const int* __restrict__ off,
+                                                                      const int* __restrict__ b,
+                                                                      const int* __restrict__ e,
+                                                                      const int* __restrict__ coff,
+                                                                      const int* __restrict__ info, long long chunks,
+                                                                      const int* __restrict__ lookup,
+                                                                      const T* __restrict__ w, const T* __restrict__ u,
+                                                                      T* __restrict__ ubar, int width, int height, T a,
+                                                                      T bb, T dt, T dx, T dy,
+                                                                      double* __restrict__ partial)
+{
+    __shared__ double s_ga[8], s_gb[8];
+    const int lane = threadIdx.x & 31;
+    const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+    double ga = 0.0, gb = 0.0;
+    for (long long q0 = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); q0 < chunks; q0 += warps) {
+        const int4 p0 = __ldg((const int4*)(info + 8 * q0));
+        const int4 p1 = __ldg((const int4*)(info + 8 * q0) + 1);
+        const int i = p0.x, k = p0.y, row = p0.z;
+        const int ib = b[i], ie = e[i];
+        const int x0 = ib + SX_CHUNK * k;
+        const long long c0 = (long long)coff[i] + (long long)SX_CHUNK * k;
+        T wc[SX_CHUNK_SUB], uc[SX_CHUNK_SUB];
+#pragma unroll
+        for (int q = 0; q < SX_CHUNK_SUB; ++q) {
+            const bool act = x0 + 32 * q + lane < ie;
+            wc[q] = act ? w[c0 + 32 * q + lane] : (T)0;
+            uc[q] = act ? u[c0 + 32 * q + lane] : (T)0;
+        }
+        SxRowReader dn = sx_row_reader(p0.w, p1.x, b, e, coff);
+        SxRowReader upr = sx_row_reader(p1.y, p1.z, b, e, coff);
+        SxRowReader dn2 = dn, up2 = upr;
+        T wprev = (T)0, uprev = (T)0;
+#pragma unroll
+        for (int q = 0; q < SX_CHUNK_SUB; ++q) {
+            const int x = x0 + 32 * q + lane;
+            const bool act = x < ie;
+            const long long c = c0 + 32 * q + lane;
+            const bool jdom = x >= 0 && x < width && row >= 0 && row < height;
+            T wl = __shfl_up_sync(0xFFFFFFFFu, wc[q], 1), ul = __shfl_up_sync(0xFFFFFFFFu, uc[q], 1);
+            if (lane == 0) {
+                wl = wprev;
+                ul = uprev;
+            }
+            T wr = __shfl_down_sync(0xFFFFFFFFu, wc[q], 1), ur = __shfl_down_sync(0xFFFFFFFFu, uc[q], 1);
+            const int qn = q + 1 < SX_CHUNK_SUB ? q + 1 : q;
+            const T wn = __shfl_sync(0xFFFFFFFFu, wc[qn], 0), un = __shfl_sync(0xFFFFFFFFu, uc[qn], 0);
+            if (lane == 31) {
+                wr = wn;
+                ur = un;
+            }
+            wprev = __shfl_sync(0xFFFFFFFFu, wc[q], 31);
+            uprev = __shfl_sync(0xFFFFFFFFu, uc[q], 31);
+            const bool first = lane == 0 && q == 0, last = lane == 31 && q + 1 == SX_CHUNK_SUB;
+            // in-set values of w left and right (the transpose checks only this cell's domain)
+            T w_left, w_right, u_left, u_right;
+            if (x - 1 >= ib) {
+                w_left = first ? w[c - 1] : wl;
+                const T uv = first ? u[c - 1] : ul;
+                u_left = (x - 1 >= 0 && x - 1 < width) ? uv : (T)0;
+            } else {
+                w_left = act ? sx_in_set<T>(row, x - 1, height, lookup, off, b, e, coff, w) : (T)0;
+                u_left = act ? sx_sample<T>(row, x - 1, height, width, lookup, off, b, e, coff, u) : (T)0;
+            }
+            if (x + 1 < ie) {
+                w_right = last ? w[c + 1] : wr;
+                const T uv = last ? u[c + 1] : ur;
+                u_right = (x + 1 >= 0 && x + 1 < width) ? uv : (T)0;
+            } else {
+                w_right = act ? sx_in_set<T>(row, x + 1, height, lookup, off, b, e, coff, w) : (T)0;
+                u_right = act ? sx_sample<T>(row, x + 1, height, width, lookup, off, b, e, coff, u) : (T)0;
+            }
+            // rows above and below: w in-set needs jdom only (x is then inside the domain, so the
+            // reader's domain test is the same), u needs the forward's domain test
+            const T w_dn = sx_row_take<T>(dn, x, width, b, e, coff, w, act && jdom);
+            const T w_up = sx_row_take<T>(upr, x, width, b, e, coff, w, act && jdom);
+            const T u_dn = sx_row_take<T>(dn2, x, width, b, e, coff, u, act);
+            const T u_up = sx_row_take<T>(up2, x, width, b, e, coff, u, act);
+            if (act) {
+                const T c_w = wc[q];
+                T tx, ty;
+                if (a >= (T)0) tx = sx_div(sx_sub(c_w, jdom ? w_right : (T)0), dx);
+                else tx = sx_div(sx_sub(jdom ? w_left : (T)0, c_w), dx);
+                if (bb >= (T)0) ty = sx_div(sx_sub(c_w, w_up), dy);
+                else ty = sx_div(sx_sub(w_dn, c_w), dy);
+                ubar[c] = sx_sub(c_w, sx_mul(dt, sx_add(sx_mul(a, tx), sx_mul(bb, ty))));
+                const T c_u = uc[q];
+                const T dux = a >= (T)0 ? sx_div(sx_sub(c_u, u_left), dx) : sx_div(sx_sub(u_right, c_u), dx);
+                const T duy = bb >= (T)0 ? sx_div(sx_sub(c_u, u_dn), dy) : sx_div(sx_sub(u_up, c_u), dy);
+                ga -= (double)dt * (double)c_w * (double)dux;
+                gb -= (double)dt * (double)c_w * (double)duy;
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        ga += __shfl_down_sync(0xFFFFFFFFu, ga, o);
+        gb += __shfl_down_sync(0xFFFFFFFFu, gb, o);
+    }
+    if (lane == 0) {
+        s_ga[threadIdx.x >> 5] = ga;
+        s_gb[threadIdx.x >> 5] = gb;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double ta = 0.0, tb = 0.0;
+        for (int q = 0; q < 8; ++q) {
+            ta += s_ga[q];
+            tb += s_gb[q];
+        }
+        partial[2 * blockIdx.x] = ta;
+        partial[2 * blockIdx.x + 1] = tb;
+    }
+}
+
 __global__ void sx_row_lookup_kernel(const int* __restrict__ rows, int row_count, int height, int* __restrict__ lookup,
                                      int* __restrict__ flags)
 {
@@ -1061,5 +1351,72 @@ cudaError_t sx_upwind_adjoint_launch(const int* rows, const int* off, int row_co
                                                                   height, (float)a, (float)bb, (float)dt, (float)dx,
                                                                   (float)dy, direct, cells, partial);
     sx_sum_pairs_kernel<<<1, 32, 0, stream>>>(partial, grid, grads);
+    return cudaGetLastError();
+}
+
+cudaError_t sx_upwind_plan_launch(const int* b, const int* e, int n, int* chunk_off, int* result, const SxScanState& st,
+                                  cudaStream_t stream)
+{
+    if (n > 0) sx_chunk_count_kernel<<<sx_grid(n, 256), 256, 0, stream>>>(b, e, n, chunk_off);
+    // in place: each scan thread reads its own items before writing them
+    return sx_scan_i32_launch(chunk_off, n, chunk_off, result, st, stream);
+}
+
+cudaError_t sx_upwind_plan_fill_launch(const int* rows, const int* off, int row_count, const int* b, const int* e,
+                                       int n, const int* chunk_off, long long chunks, const int* lookup, int height,
+                                       int* info, cudaStream_t stream)
+{
+    if (n <= 0 || chunks <= 0) return cudaSuccess;
+    sx_chunk_info_kernel<<<sx_grid(chunks, 256, 148 * 32), 256, 0, stream>>>(rows, off, row_count, b, e, n, chunk_off,
+                                                                             chunks, lookup, height, info);
+    return cudaGetLastError();
+}
+
+cudaError_t sx_upwind_chunk_launch(const int* off, const int* b, const int* e, const int* coff, const int* info,
+                                   long long chunks, const int* lookup, const void* v, void* out, int width, int height,
+                                   double a, double bb, double dt, double dx, double dy, int dbl, cudaStream_t stream)
+{
+    if (chunks <= 0) return cudaSuccess;
+    long long blocks = (chunks + 7) / 8;
+    if (blocks > 148 * 64) blocks = 148 * 64;
+    if (dbl)
+        sx_upwind_chunk_kernel<double><<<(int)blocks, 256, 0, stream>>>(off, b, e, coff, info, chunks, lookup,
+                                                                        (const double*)v, (double*)out, width, height,
+                                                                        a, bb, dt, dx, dy);
+    else
+        sx_upwind_chunk_kernel<float><<<(int)blocks, 256, 0, stream>>>(off, b, e, coff, info, chunks, lookup,
+                                                                       (const float*)v, (float*)out, width, height,
+                                                                       (float)a, (float)bb, (float)dt, (float)dx,
+                                                                       (float)dy);
+    return cudaGetLastError();
+}
+
+int sx_upwind_adjoint_chunk_parts(long long chunks)
+{
+    long long blocks = (chunks + 7) / 8;
+    if (blocks < 1) blocks = 1;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    return (int)blocks;
+}
+
+cudaError_t sx_upwind_adjoint_chunk_launch(const int* off, const int* b, const int* e, const int* coff, const int* info,
+                                           long long chunks, const int* lookup, const void* w, const void* u,
+                                           void* ubar, int width, int height, double a, double bb, double dt,
+                                           double dx, double dy, int dbl, double* partial, double* grads,
+                                           cudaStream_t stream)
+{
+    const int blocks = sx_upwind_adjoint_chunk_parts(chunks);
+    if (dbl)
+        sx_upwind_adjoint_chunk_kernel<double><<<blocks, 256, 0, stream>>>(off, b, e, coff, info, chunks, lookup,
+                                                                           (const double*)w, (const double*)u,
+                                                                           (double*)ubar, width, height, a, bb, dt, dx,
+                                                                           dy, partial);
+    else
+        sx_upwind_adjoint_chunk_kernel<float><<<blocks, 256, 0, stream>>>(off, b, e, coff, info, chunks, lookup,
+                                                                          (const float*)w, (const float*)u,
+                                                                          (float*)ubar, width, height, (float)a,
+                                                                          (float)bb, (float)dt, (float)dx, (float)dy,
+                                                                          partial);
+    sx_sum_pairs_kernel<<<1, 32, 0, stream>>>(partial, blocks, grads);
     return cudaGetLastError();
 }

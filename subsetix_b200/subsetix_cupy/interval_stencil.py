@@ -1,10 +1,13 @@
 """First-order upwind step on interval fields (drop-in for ``subsetix_cupy.interval_stencil``).
 
 Arguments, checks and results follow ``subsetix_cupy/interval_stencil.py``
-of the reference.  The kernel (``sx_upwind``) assigns 256 consecutive
-cells to each thread block, so work is even across intervals of any length.
-Neighbours inside a cell's own interval are read directly when the rows are
-sorted and disjoint, and are searched for otherwise.  Float32 is the
+of the reference.  On geometry whose rows are sorted and disjoint (the
+usual case, checked once per set) the chunked kernel ``sx_upwind_chunked``
+runs: warps take chunks of 128 cells of one interval in four coalesced
+sub-rounds, exchange left/right neighbours by shuffles and read the rows
+above and below with coalesced loads.  Other geometry takes ``sx_upwind``, which assigns 256 consecutive
+cells to each block and searches every neighbour.  Both give the same
+values.  Float32 is the
 reference's arithmetic.  Float64 values run the same formula in double
 precision (an addition of this package).
 """
@@ -30,12 +33,14 @@ class _Geometry:
     lookup (and its synchronising range check) once.
     """
 
-    __slots__ = ("height", "lookup", "direct")
+    __slots__ = ("height", "lookup", "direct", "chunk_off", "chunks")
 
-    def __init__(self, height: int, lookup: torch.Tensor, direct: bool):
+    def __init__(self, height: int, lookup: torch.Tensor, direct: bool, chunk_off=None, chunks: int = 0):
         self.height = height
         self.lookup = lookup
         self.direct = direct
+        self.chunk_off = chunk_off
+        self.chunks = chunks
 
 
 def _geometry(interval_set, height: int) -> _Geometry:
@@ -51,7 +56,11 @@ def _geometry(interval_set, height: int) -> _Geometry:
         raise ValueError("interval_set rows exceed provided height")
     flags = _core.check_rows(_t(interval_set.begin), _t(interval_set.end), _t(interval_set.row_offsets), device)
     direct = not (flags & (_lib.ROWS_UNSORTED_BEGIN | _lib.ROWS_OVERLAP | _lib.ROWS_EMPTY))
-    geo = _Geometry(height, lookup, direct)
+    chunk_off, chunks = (None, 0)
+    if direct:
+        chunk_off, chunks = _core.upwind_plan(rows, _t(interval_set.row_offsets), _t(interval_set.begin),
+                                              _t(interval_set.end), lookup, height, device)
+    geo = _Geometry(height, lookup, direct, chunk_off, chunks)
     try:
         object.__setattr__(interval_set, "_sx_stencil", geo)
     except Exception:  # pragma: no cover - sets that refuse attributes
@@ -104,8 +113,13 @@ def step_upwind_interval(field: IntervalField, *, width: int, height: int, a: fl
         if bool(((rid < 0) | (rid >= height)).any()) or int(geo.lookup[rid.long()].min().item()) < 0:
             raise ValueError("interval_set rows exceed provided height")
     vals = vals.contiguous()
-    _core.upwind(_t(s.rows), _t(s.row_offsets), begin, _t(s.end), cell_off, int(vals.numel()), geo.lookup, vals,
-                 out_t, width, height, a, b, dt, dx, dy, geo.direct and rid is None, device, row_ids=rid)
+    if geo.chunk_off is not None and rid is None and out_t.data_ptr() != vals.data_ptr():
+        # fixed geometry with sorted, disjoint rows: the chunked kernel (same results)
+        _core.upwind_chunked(_t(s.row_offsets), begin, _t(s.end), cell_off, geo.chunk_off, geo.chunks, geo.lookup, vals,
+                             out_t, width, height, a, b, dt, dx, dy, device)
+    else:
+        _core.upwind(_t(s.rows), _t(s.row_offsets), begin, _t(s.end), cell_off, int(vals.numel()), geo.lookup, vals,
+                     out_t, width, height, a, b, dt, dx, dy, geo.direct and rid is None, device, row_ids=rid)
     return out if out is not None else like(kind, out_t)
 
 

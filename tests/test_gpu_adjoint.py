@@ -132,3 +132,28 @@ def test_checkpoint_spacing_and_fp32(cuda_device):
     assert float(torch.linalg.vector_norm(v32 - v64) / torch.linalg.vector_norm(v64)) < 1e-4
     for a, b in zip(u32, u64):
         assert float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b)) < 1e-5
+
+
+@pytest.mark.parametrize("a,b", [(0.7, 0.4), (-0.5, -0.9)])
+def test_chunked_adjoint_equals_generic(cuda_device, a, b):
+    from subsetix_b200 import _lib
+    from subsetix_b200._runtime import ptr, stream_handle
+
+    h = rand_set(400, 12.0, seed=8, row_stride=1, max_col=350, touching=True, row0=0)
+    lvl = _level(h, 330, 400)      # some cells lie beyond the width
+    assert lvl.chunk_off is not None
+    rng = np.random.default_rng(3)
+    w = torch.as_tensor(rng.standard_normal(lvl.cells), device="cuda")
+    u = torch.as_tensor(rng.standard_normal(lvl.cells), device="cuda")
+    g_chunk = torch.zeros(2, dtype=torch.float64, device="cuda")
+    got = lvl.adjoint(w, u, a, b, 1e-3, g_chunk)
+    lib = _lib.load()
+    ref = torch.empty_like(w)
+    g_ref = torch.empty(2, dtype=torch.float64, device="cuda")
+    _lib.check(lib.sx_upwind_adjoint(_lib.SX_F64, ptr(lvl.rows), ptr(lvl.off), int(lvl.rows.numel()), ptr(lvl.begin),
+                                     ptr(lvl.end), ptr(lvl.cell_off), int(lvl.begin.numel()), lvl.cells,
+                                     ptr(lvl.lookup), ptr(w), ptr(u), ptr(ref), lvl.width, lvl.height, a, b, 1e-3,
+                                     lvl.dx, lvl.dy, 0, ptr(g_ref), ptr(lvl.scratch), int(lvl.scratch.numel()),
+                                     stream_handle(torch.device("cuda", 0))), "sx_upwind_adjoint")
+    assert torch.equal(got, ref)
+    assert torch.allclose(g_chunk, g_ref, rtol=1e-12, atol=0)

@@ -275,3 +275,32 @@ def test_upwind_rows_out_of_range(cuda_device):
         sc.step_upwind_interval(f, width=4, height=4, a=1.0, b=1.0, dt=0.1, dx=1.0, dy=1.0)
     with pytest.raises(ValueError):
         sc.step_upwind_interval(f, width=0, height=4, a=1.0, b=1.0, dt=0.1, dx=1.0, dy=1.0)
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+def test_upwind_chunked_equals_generic(cuda_device, dtype):
+    from subsetix_b200 import _core
+
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(13)
+    cases = [rand_set(700, 25.0, seed=31, row_stride=1, touching=True, row0=0),   # ragged, touching, beyond width
+             rand_set(300, 1.0, seed=32, row_stride=2, row0=1),                   # sparse rows, gaps between rows
+             (np.zeros(64, np.int32), np.full(64, 5000, np.int32), np.arange(65, dtype=np.int32),
+              np.arange(64, dtype=np.int32))]                                     # long single intervals
+    for h in cases:
+        S = dev_set(h)
+        H = int(h[3].max()) + 2
+        W = 300
+        b, e, off, rows = (torch.as_tensor(a, device=dev) for a in h)
+        coff, cells = _core.cell_offsets(b, e, dev)
+        lookup, bad = _core.row_lookup(rows, H, dev)
+        assert not bad
+        chunk_off, chunks = _core.upwind_plan(rows, off, b, e, lookup, H, dev)
+        v = torch.as_tensor(rng.standard_normal(cells), device=dev).to(dtype)
+        for a_, b_ in ((0.6, 0.3), (-0.4, -0.9)):
+            ref = torch.empty_like(v)
+            got = torch.empty_like(v)
+            _core.upwind(rows, off, b, e, coff, cells, lookup, v, ref, W, H, a_, b_, 1e-3, 1e-2, 1e-2, False, dev)
+            _core.upwind_chunked(off, b, e, coff, chunk_off, chunks, lookup, v, got, W, H, a_, b_, 1e-3, 1e-2, 1e-2,
+                                 dev)
+            assert torch.equal(got, ref)
