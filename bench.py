@@ -55,6 +55,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-amr", action="store_true", help="skip the two-level AMR step section")
     p.add_argument("--no-autotune", action="store_true", help="use the automatic launch choice")
+    p.add_argument("--section", default="all", choices=["all", "amr", "adjoint"],
+                   help="run only the AMR or the adjoint section (for profiling)")
     return p.parse_args()
 
 
@@ -395,6 +397,16 @@ def main():
 
         dist.init_process_group("nccl", init_method="env://", timeout=timedelta(seconds=120),
                                 device_id=device)
+
+    if args.section in ("amr", "adjoint"):
+        # one section alone (profiling runs); prints that section's JSON object
+        out = amr_section(device) if args.section == "amr" else adjoint_section(device)
+        if rank == 0:
+            print(json.dumps({args.section: out}), flush=True)
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
 
     from subsetix_b200 import _core, _lib
     from subsetix_b200.subsetix_cupy import expressions as E

@@ -33,6 +33,8 @@
 // bit-identical to the interval kernels (and to the reference) on the same
 // inputs, in float32 and in float64.
 
+#include <cmath>
+
 #include "sx_internal.cuh"
 
 __device__ __forceinline__ float sxa_add(float a, float b) { return __fadd_rn(a, b); }
@@ -44,10 +46,19 @@ __device__ __forceinline__ double sxa_sub(double a, double b) { return __dsub_rn
 __device__ __forceinline__ double sxa_mul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double sxa_div(double a, double b) { return __ddiv_rn(a, b); }
 
+// x / d, or x * d when the launcher passed the reciprocal of a power-of-two
+// spacing instead (pow2 != 0).  Dividing by 2^k and multiplying by 2^-k
+// have the same exact real result, so the rounded results are identical.
+template <typename T>
+__device__ __forceinline__ T sxa_over(T x, T d, int pow2)
+{
+    return pow2 ? sxa_mul(x, d) : sxa_div(x, d);
+}
+
 // One thread per cell; x fastest.  blockIdx.z is the batch entry.
 template <typename T>
 __global__ void __launch_bounds__(256) sx_upwind_full_kernel(const T* __restrict__ in, T* __restrict__ out, int W,
-                                                             int H, T a, T b, T dt, T dx, T dy)
+                                                             int H, T a, T b, T dt, T dx, T dy, int pow2)
 {
     const long long plane = (long long)W * H;
     const T* v = in + plane * blockIdx.z;
@@ -61,8 +72,8 @@ __global__ void __launch_bounds__(256) sx_upwind_full_kernel(const T* __restrict
     const T r = x + 1 < W ? v[idx + 1] : (T)0;
     const T d = y > 0 ? v[idx - W] : (T)0;
     const T u = y + 1 < H ? v[idx + W] : (T)0;
-    const T du_dx = a >= (T)0 ? sxa_div(sxa_sub(c, l), dx) : sxa_div(sxa_sub(r, c), dx);
-    const T du_dy = b >= (T)0 ? sxa_div(sxa_sub(c, d), dy) : sxa_div(sxa_sub(u, c), dy);
+    const T du_dx = a >= (T)0 ? sxa_over(sxa_sub(c, l), dx, pow2) : sxa_over(sxa_sub(r, c), dx, pow2);
+    const T du_dy = b >= (T)0 ? sxa_over(sxa_sub(c, d), dy, pow2) : sxa_over(sxa_sub(u, c), dy, pow2);
     o[idx] = sxa_sub(c, sxa_mul(dt, sxa_add(sxa_mul(a, du_dx), sxa_mul(b, du_dy))));
 }
 
@@ -101,10 +112,10 @@ __global__ void __launch_bounds__(256) sx_amr_sync_full_kernel(T* __restrict__ c
 // new values, so this equals upwind(coarse); upwind(fine); sync, value for
 // value.  in/out are distinct buffers.
 template <typename T>
-__device__ __forceinline__ T sxa_upwind_cell(T c, T l, T r, T d, T u, T a, T b, T dt, T dx, T dy)
+__device__ __forceinline__ T sxa_upwind_cell(T c, T l, T r, T d, T u, T a, T b, T dt, T dx, T dy, int pow2)
 {
-    const T du_dx = a >= (T)0 ? sxa_div(sxa_sub(c, l), dx) : sxa_div(sxa_sub(r, c), dx);
-    const T du_dy = b >= (T)0 ? sxa_div(sxa_sub(c, d), dy) : sxa_div(sxa_sub(u, c), dy);
+    const T du_dx = a >= (T)0 ? sxa_over(sxa_sub(c, l), dx, pow2) : sxa_over(sxa_sub(r, c), dx, pow2);
+    const T du_dy = b >= (T)0 ? sxa_over(sxa_sub(c, d), dy, pow2) : sxa_over(sxa_sub(u, c), dy, pow2);
     return sxa_sub(c, sxa_mul(dt, sxa_add(sxa_mul(a, du_dx), sxa_mul(b, du_dy))));
 }
 
@@ -112,7 +123,8 @@ template <typename T>
 __global__ void __launch_bounds__(256) sx_amr_step_full_kernel(const T* __restrict__ cin, const T* __restrict__ fin,
                                                                T* __restrict__ cout, T* __restrict__ fout,
                                                                const signed char* __restrict__ actions, int W, int H,
-                                                               T a, T b, T dt, T dxc, T dyc, T dxf, T dyf, T norm)
+                                                               T a, T b, T dt, T dxc, T dyc, T dxf, T dyf, T norm,
+                                                               int pow2c, int pow2f)
 {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
@@ -128,7 +140,7 @@ __global__ void __launch_bounds__(256) sx_amr_step_full_kernel(const T* __restri
     const T cr = x + 1 < W ? C[ci + 1] : (T)0;
     const T cd = y > 0 ? C[ci - W] : (T)0;
     const T cu = y + 1 < H ? C[ci + W] : (T)0;
-    const T cn = sxa_upwind_cell(c, cl, cr, cd, cu, a, b, dt, dxc, dyc);
+    const T cn = sxa_upwind_cell(c, cl, cr, cd, cu, a, b, dt, dxc, dyc, pow2c);
     // fine block: rows 2y-1 .. 2y+2, columns 2x-1 .. 2x+2
     const int fx = 2 * x, fy = 2 * y;
     T v[4][4];
@@ -148,7 +160,7 @@ __global__ void __launch_bounds__(256) sx_amr_step_full_kernel(const T* __restri
 #pragma unroll
         for (int i = 0; i < 2; ++i)
             fn[j][i] = sxa_upwind_cell(v[j + 1][i + 1], v[j + 1][i], v[j + 1][i + 2], v[j][i + 1], v[j + 2][i + 1], a, b,
-                                       dt, dxf, dyf);
+                                       dt, dxf, dyf, pow2f);
     T* CO = cout + plane * blockIdx.z;
     T* FO = fout + 4 * plane * blockIdx.z;
     if (actions[plane * blockIdx.z + ci] == 1) {
@@ -224,15 +236,36 @@ __global__ void __launch_bounds__(256) sx_amr_grade_full_kernel(const unsigned c
 
 static dim3 sxa_grid(int W, int H, int batch) { return dim3((unsigned)((W + 255) / 256), (unsigned)H, (unsigned)batch); }
 
+// Spacings that are powers of two (in the kernel's precision) are passed
+// as their exact reciprocals, turning divisions into multiplications.
+template <typename T>
+static int sxa_pow2_pair(T& dx, T& dy)
+{
+    int ex, ey;
+    const bool p = frexp((double)dx, &ex) == 0.5 && frexp((double)dy, &ey) == 0.5;
+    if (!p) return 0;
+    const T ix = (T)1 / dx, iy = (T)1 / dy;
+    if (!std::isfinite((double)ix) || !std::isfinite((double)iy)) return 0;  // reciprocal out of range
+    dx = ix;
+    dy = iy;
+    return 1;
+}
+
 cudaError_t sx_upwind_full_launch(int dbl, const void* in, void* out, int W, int H, int batch, double a, double b,
                                   double dt, double dx, double dy, cudaStream_t stream)
 {
     const dim3 g = sxa_grid(W, H, batch);
-    if (dbl)
-        sx_upwind_full_kernel<double><<<g, 256, 0, stream>>>((const double*)in, (double*)out, W, H, a, b, dt, dx, dy);
-    else
+    if (dbl) {
+        double ddx = dx, ddy = dy;
+        const int p = sxa_pow2_pair(ddx, ddy);
+        sx_upwind_full_kernel<double><<<g, 256, 0, stream>>>((const double*)in, (double*)out, W, H, a, b, dt, ddx, ddy,
+                                                             p);
+    } else {
+        float fdx = (float)dx, fdy = (float)dy;
+        const int p = sxa_pow2_pair(fdx, fdy);
         sx_upwind_full_kernel<float><<<g, 256, 0, stream>>>((const float*)in, (float*)out, W, H, (float)a, (float)b,
-                                                            (float)dt, (float)dx, (float)dy);
+                                                            (float)dt, fdx, fdy, p);
+    }
     return cudaGetLastError();
 }
 
@@ -276,14 +309,18 @@ cudaError_t sx_amr_step_full_launch(int dbl, const void* cin, const void* fin, v
                                     double dxc, double dyc, double dxf, double dyf, cudaStream_t stream)
 {
     const dim3 g = sxa_grid(W, H, batch);
-    if (dbl)
+    if (dbl) {
+        double cx = dxc, cy = dyc, fx = dxf, fy = dyf;
+        const int pc = sxa_pow2_pair(cx, cy), pf = sxa_pow2_pair(fx, fy);
         sx_amr_step_full_kernel<double><<<g, 256, 0, stream>>>((const double*)cin, (const double*)fin, (double*)cout,
-                                                               (double*)fout, actions, W, H, a, b, dt, dxc, dyc, dxf,
-                                                               dyf, 0.25);
-    else
+                                                               (double*)fout, actions, W, H, a, b, dt, cx, cy, fx, fy,
+                                                               0.25, pc, pf);
+    } else {
+        float cx = (float)dxc, cy = (float)dyc, fx = (float)dxf, fy = (float)dyf;
+        const int pc = sxa_pow2_pair(cx, cy), pf = sxa_pow2_pair(fx, fy);
         sx_amr_step_full_kernel<float><<<g, 256, 0, stream>>>((const float*)cin, (const float*)fin, (float*)cout,
                                                               (float*)fout, actions, W, H, (float)a, (float)b,
-                                                              (float)dt, (float)dxc, (float)dyc, (float)dxf,
-                                                              (float)dyf, 0.25f);
+                                                              (float)dt, cx, cy, fx, fy, 0.25f, pc, pf);
+    }
     return cudaGetLastError();
 }

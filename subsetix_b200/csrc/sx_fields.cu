@@ -11,6 +11,7 @@
 // FP32 and FP64.
 
 #include <climits>
+#include <cmath>
 
 #include "sx_internal.cuh"
 
@@ -26,6 +27,29 @@ __device__ __forceinline__ double sx_add(double a, double b) { return __dadd_rn(
 __device__ __forceinline__ double sx_sub(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ double sx_mul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double sx_div(double a, double b) { return __ddiv_rn(a, b); }
+
+// x / d, or x * d when the launcher passed the reciprocal of a power-of-two
+// spacing instead (pow2 != 0): dividing by 2^k and multiplying by 2^-k have
+// the same exact real result, so the rounded results are identical.
+template <typename T>
+__device__ __forceinline__ T sx_over(T x, T d, int pow2)
+{
+    return pow2 ? sx_mul(x, d) : sx_div(x, d);
+}
+
+// Spacings that are powers of two (in the kernel's precision) become their
+// exact reciprocals.
+template <typename T>
+static int sx_pow2_pair(T& dx, T& dy)
+{
+    int ex, ey;
+    if (!(frexp((double)dx, &ex) == 0.5 && frexp((double)dy, &ey) == 0.5)) return 0;
+    const T ix = (T)1 / dx, iy = (T)1 / dy;
+    if (!std::isfinite((double)ix) || !std::isfinite((double)iy)) return 0;  // reciprocal out of range
+    dx = ix;
+    dy = iy;
+    return 1;
+}
 
 // Row ordinal of interval i: the last p with off[p] <= i and off[p+1] > i.
 __device__ __forceinline__ int sx_row_of(const int* __restrict__ off, int rows, int i)
@@ -679,7 +703,7 @@ __global__ void __launch_bounds__(256) sx_upwind_chunk_kernel(const int* __restr
                                                               const int* __restrict__ info, long long chunks,
                                                               const int* __restrict__ lookup,
                                                               const T* __restrict__ v, T* __restrict__ out, int width,
-                                                              int height, T a, T bb, T dt, T dx, T dy)
+                                                              int height, T a, T bb, T dt, T dx, T dy, int pow2)
 {
     const int lane = threadIdx.x & 31;
     const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
@@ -722,8 +746,8 @@ __global__ void __launch_bounds__(256) sx_upwind_chunk_kernel(const int* __restr
             const T down = sx_row_take<T>(dn, x, width, b, e, coff, v, act);
             const T up = sx_row_take<T>(upc, x, width, b, e, coff, v, act);
             if (act) {
-                const T du_dx = a >= (T)0 ? sx_div(sx_sub(center, left), dx) : sx_div(sx_sub(right, center), dx);
-                const T du_dy = bb >= (T)0 ? sx_div(sx_sub(center, down), dy) : sx_div(sx_sub(up, center), dy);
+                const T du_dx = a >= (T)0 ? sx_over(sx_sub(center, left), dx, pow2) : sx_over(sx_sub(right, center), dx, pow2);
+                const T du_dy = bb >= (T)0 ? sx_over(sx_sub(center, down), dy, pow2) : sx_over(sx_sub(up, center), dy, pow2);
                 out[c] = sx_sub(center, sx_mul(dt, sx_add(sx_mul(a, du_dx), sx_mul(bb, du_dy))));
             }
         }
@@ -743,7 +767,7 @@ __global__ void __launch_bounds__(256) sx_upwind_adjoint_chunk_kernel(const int*
                                                                       const int* __restrict__ lookup,
                                                                       const T* __restrict__ w, const T* __restrict__ u,
                                                                       T* __restrict__ ubar, int width, int height, T a,
-                                                                      T bb, T dt, T dx, T dy,
+                                                                      T bb, T dt, T dx, T dy, int pow2,
                                                                       double* __restrict__ partial)
 {
     __shared__ double s_ga[8], s_gb[8];
@@ -816,14 +840,14 @@ __global__ void __launch_bounds__(256) sx_upwind_adjoint_chunk_kernel(const int*
             if (act) {
                 const T c_w = wc[q];
                 T tx, ty;
-                if (a >= (T)0) tx = sx_div(sx_sub(c_w, jdom ? w_right : (T)0), dx);
-                else tx = sx_div(sx_sub(jdom ? w_left : (T)0, c_w), dx);
-                if (bb >= (T)0) ty = sx_div(sx_sub(c_w, w_up), dy);
-                else ty = sx_div(sx_sub(w_dn, c_w), dy);
+                if (a >= (T)0) tx = sx_over(sx_sub(c_w, jdom ? w_right : (T)0), dx, pow2);
+                else tx = sx_over(sx_sub(jdom ? w_left : (T)0, c_w), dx, pow2);
+                if (bb >= (T)0) ty = sx_over(sx_sub(c_w, w_up), dy, pow2);
+                else ty = sx_over(sx_sub(w_dn, c_w), dy, pow2);
                 ubar[c] = sx_sub(c_w, sx_mul(dt, sx_add(sx_mul(a, tx), sx_mul(bb, ty))));
                 const T c_u = uc[q];
-                const T dux = a >= (T)0 ? sx_div(sx_sub(c_u, u_left), dx) : sx_div(sx_sub(u_right, c_u), dx);
-                const T duy = bb >= (T)0 ? sx_div(sx_sub(c_u, u_dn), dy) : sx_div(sx_sub(u_up, c_u), dy);
+                const T dux = a >= (T)0 ? sx_over(sx_sub(c_u, u_left), dx, pow2) : sx_over(sx_sub(u_right, c_u), dx, pow2);
+                const T duy = bb >= (T)0 ? sx_over(sx_sub(c_u, u_dn), dy, pow2) : sx_over(sx_sub(u_up, c_u), dy, pow2);
                 ga -= (double)dt * (double)c_w * (double)dux;
                 gb -= (double)dt * (double)c_w * (double)duy;
             }
@@ -1379,15 +1403,19 @@ cudaError_t sx_upwind_chunk_launch(const int* off, const int* b, const int* e, c
     if (chunks <= 0) return cudaSuccess;
     long long blocks = (chunks + 7) / 8;
     if (blocks > 148 * 64) blocks = 148 * 64;
-    if (dbl)
+    if (dbl) {
+        double ddx = dx, ddy = dy;
+        const int p = sx_pow2_pair(ddx, ddy);
         sx_upwind_chunk_kernel<double><<<(int)blocks, 256, 0, stream>>>(off, b, e, coff, info, chunks, lookup,
                                                                         (const double*)v, (double*)out, width, height,
-                                                                        a, bb, dt, dx, dy);
-    else
+                                                                        a, bb, dt, ddx, ddy, p);
+    } else {
+        float fdx = (float)dx, fdy = (float)dy;
+        const int p = sx_pow2_pair(fdx, fdy);
         sx_upwind_chunk_kernel<float><<<(int)blocks, 256, 0, stream>>>(off, b, e, coff, info, chunks, lookup,
                                                                        (const float*)v, (float*)out, width, height,
-                                                                       (float)a, (float)bb, (float)dt, (float)dx,
-                                                                       (float)dy);
+                                                                       (float)a, (float)bb, (float)dt, fdx, fdy, p);
+    }
     return cudaGetLastError();
 }
 
@@ -1406,17 +1434,21 @@ cudaError_t sx_upwind_adjoint_chunk_launch(const int* off, const int* b, const i
                                            cudaStream_t stream)
 {
     const int blocks = sx_upwind_adjoint_chunk_parts(chunks);
-    if (dbl)
+    if (dbl) {
+        double ddx = dx, ddy = dy;
+        const int p = sx_pow2_pair(ddx, ddy);
         sx_upwind_adjoint_chunk_kernel<double><<<blocks, 256, 0, stream>>>(off, b, e, coff, info, chunks, lookup,
                                                                            (const double*)w, (const double*)u,
-                                                                           (double*)ubar, width, height, a, bb, dt, dx,
-                                                                           dy, partial);
-    else
+                                                                           (double*)ubar, width, height, a, bb, dt,
+                                                                           ddx, ddy, p, partial);
+    } else {
+        float fdx = (float)dx, fdy = (float)dy;
+        const int p = sx_pow2_pair(fdx, fdy);
         sx_upwind_adjoint_chunk_kernel<float><<<blocks, 256, 0, stream>>>(off, b, e, coff, info, chunks, lookup,
                                                                           (const float*)w, (const float*)u,
                                                                           (float*)ubar, width, height, (float)a,
-                                                                          (float)bb, (float)dt, (float)dx, (float)dy,
-                                                                          partial);
+                                                                          (float)bb, (float)dt, fdx, fdy, p, partial);
+    }
     sx_sum_pairs_kernel<<<1, 32, 0, stream>>>(partial, blocks, grads);
     return cudaGetLastError();
 }

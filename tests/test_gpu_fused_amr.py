@@ -144,3 +144,16 @@ def test_batched_uneven_sets_against_oracle(cuda_device):
         exp = O.upwind(f, width=side, height=side, a=1.0, b=-0.5, dt=1e-4, dx=1e-3, dy=1e-3)
         np.testing.assert_array_equal(got[pos:pos + exp.size], exp)
         pos += exp.size
+
+
+@pytest.mark.parametrize("res", [32, 40])
+def test_power_of_two_spacing_matches_division(cuda_device, res):
+    # res 32 has power-of-two spacings (multiplication by the exact reciprocal),
+    # res 40 does not (division); both must equal the FP64 oracle and AMR2Simulation
+    u0 = _gauss(res, 0.08)
+    ref = O.AMR2(res, (0.9, -0.4), cfl=0.5, threshold=0.05, grading_pad=1, dtype=np.float64)
+    ref.init(u0)
+    ref.run(6, 3)
+    eng = FusedTwoLevelAMR(torch.as_tensor(u0, device="cuda"), velocity=(0.9, -0.4), cfl=0.5, dtype=torch.float64)
+    eng.run(6, regrid_every=3)
+    np.testing.assert_array_equal(_vals(eng.fine_values).reshape(-1), ref.fine.values)
