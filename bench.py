@@ -60,11 +60,12 @@ def parse():
     return p.parse_args()
 
 
-def workload(copies: int):
+def workload(copies: int, first: int = 0):
+    """The five shape operands, ``copies`` shifted copies stacked on row bands (copy ids from ``first``)."""
     from subsetix_b200 import synth
 
     shapes = synth.shape_operands(4096)
-    return [synth.stack_rows(s, copies, 4096) for s in shapes]
+    return [synth.stack_rows(s, copies, 4096, first=first) for s in shapes]
 
 
 def algorithmic_bytes(leaves, n_out: int, r_out: int) -> int:
@@ -411,7 +412,11 @@ def main():
     from subsetix_b200 import _core, _lib
     from subsetix_b200.subsetix_cupy import expressions as E
 
-    leaves_host = workload(args.copies)
+    from subsetix_b200.distributed import max_over_ranks, shard
+
+    # weak scaling: the global batch holds world * copies distinct copies, one shard per rank
+    first, _ = shard(world * args.copies, rank, world)
+    leaves_host = workload(args.copies, first)
     n_in = sum(int(h[0].size) for h in leaves_host)
     R = int(leaves_host[0][3].size)
     dev = [tuple(torch.as_tensor(a, device=device) for a in h) for h in leaves_host]
@@ -459,11 +464,7 @@ def main():
             ev[i + 1].record(stream)
         torch.cuda.synchronize()
     per_step = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
-    elapsed_ms = ev[0].elapsed_time(ev[-1])
-    if world > 1:
-        t = torch.tensor([elapsed_ms], device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
+    elapsed_ms = max_over_ranks(ev[0].elapsed_time(ev[-1]), device)
     value = world * n_in * args.steps / (elapsed_ms / 1e3) / 1e9
 
     # end to end through the public API with pinned host buffers
@@ -491,11 +492,7 @@ def main():
         d2h = sum(int(o.numel()) * 4 for o in outs)
         if i > 0:
             e2e_times.append(s0.elapsed_time(s1))
-    e2e_ms = statistics.median(e2e_times)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(statistics.median(e2e_times), device)
     e2e_value = world * n_in / (e2e_ms / 1e3) / 1e9
 
     kernel_ms = statistics.mean(per_step)

@@ -170,17 +170,19 @@ def shape_operands(size: int = 4096) -> List[HostSet]:
     ]
 
 
-def stack_rows(host_set: HostSet, copies: int, row_stride: int, shift_step: int = 37, shift_mod: int = 128) -> HostSet:
+def stack_rows(host_set: HostSet, copies: int, row_stride: int, shift_step: int = 37, shift_mod: int = 128,
+               first: int = 0) -> HostSet:
     """Stack ``copies`` x-shifted copies of a set on disjoint row bands.
 
-    Copy ``k`` moves its rows by ``k * row_stride`` and its columns by
-    ``(k * shift_step) % shift_mod - shift_mod // 2``.
+    Copy ``k`` (counted from ``first``, so batches split across ranks stay
+    distinct) moves its rows by ``(k - first) * row_stride`` and its columns
+    by ``(k * shift_step) % shift_mod - shift_mod // 2``.
     """
 
     begin, end, offsets, rows = host_set
     n = int(offsets[-1])
     r = int(rows.size)
-    shifts = (np.arange(copies, dtype=np.int64) * shift_step) % shift_mod - shift_mod // 2
+    shifts = ((np.arange(copies, dtype=np.int64) + first) * shift_step) % shift_mod - shift_mod // 2
     b = (begin[None, :].astype(np.int64) + shifts[:, None]).reshape(-1)
     e = (end[None, :].astype(np.int64) + shifts[:, None]).reshape(-1)
     counts = np.diff(offsets.astype(np.int64))
