@@ -571,16 +571,31 @@ __global__ void __launch_bounds__(256) sx_upwind_adjoint_kernel(const int* __res
     }
 }
 
-__global__ void sx_sum_pairs_kernel(const double* __restrict__ partial, int parts, double* __restrict__ out)
+// Sum of (a, b) pairs, one block of 256 threads: thread t adds pairs t,
+// t + 256, ... in order, then a fixed tree combines the threads, so the
+// result does not depend on timing.
+__global__ void __launch_bounds__(256) sx_sum_pairs_kernel(const double* __restrict__ partial, int parts,
+                                                           double* __restrict__ out)
 {
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        double sa = 0.0, sb = 0.0;
-        for (int q = 0; q < parts; ++q) {
-            sa += partial[2 * q];
-            sb += partial[2 * q + 1];
+    __shared__ double sa[256], sb[256];
+    double a = 0.0, b = 0.0;
+    for (int q = threadIdx.x; q < parts; q += 256) {
+        a += partial[2 * q];
+        b += partial[2 * q + 1];
+    }
+    sa[threadIdx.x] = a;
+    sb[threadIdx.x] = b;
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if (threadIdx.x < h) {
+            sa[threadIdx.x] += sa[threadIdx.x + h];
+            sb[threadIdx.x] += sb[threadIdx.x + h];
         }
-        out[0] = sa;
-        out[1] = sb;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[0] = sa[0];
+        out[1] = sb[0];
     }
 }
 
@@ -982,16 +997,32 @@ __global__ void sx_mass_partial_kernel(const T* __restrict__ v, long long n, dou
     }
 }
 
-__global__ void sx_mass_final_kernel(const double* __restrict__ part, int parts, double scale, double* __restrict__ out)
+// Final combination of the per-block (sum, compensation) pairs, one block of
+// 256 threads: each thread folds parts t, t + 256, ... with Neumaier steps,
+// then a fixed tree merges the threads' pairs (Neumaier on the sums, the
+// compensations added).  Deterministic.
+__global__ void __launch_bounds__(256) sx_mass_final_kernel(const double* __restrict__ part, int parts, double scale,
+                                                            double* __restrict__ out)
 {
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        double S = 0.0, C = 0.0;
-        for (int t = 0; t < parts; ++t) {
-            sx_neumaier(S, C, part[2 * t]);
-            C = __dadd_rn(C, part[2 * t + 1]);
-        }
-        out[0] = __dmul_rn(__dadd_rn(S, C), scale);
+    __shared__ double ss[256], sc[256];
+    double S = 0.0, C = 0.0;
+    for (int t = threadIdx.x; t < parts; t += 256) {
+        sx_neumaier(S, C, part[2 * t]);
+        C = __dadd_rn(C, part[2 * t + 1]);
     }
+    ss[threadIdx.x] = S;
+    sc[threadIdx.x] = C;
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if (threadIdx.x < h) {
+            double s1 = ss[threadIdx.x], c1 = sc[threadIdx.x];
+            sx_neumaier(s1, c1, ss[threadIdx.x + h]);
+            ss[threadIdx.x] = s1;
+            sc[threadIdx.x] = __dadd_rn(c1, sc[threadIdx.x + h]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[0] = __dmul_rn(__dadd_rn(ss[0], sc[0]), scale);
 }
 
 // ---------------------------------------------------------------------------
@@ -1345,7 +1376,7 @@ cudaError_t sx_mass_launch(const void* v, long long n, int dbl, double scale, do
 {
     if (dbl) sx_mass_partial_kernel<double><<<parts, SX_BLOCK, 0, stream>>>((const double*)v, n, part);
     else sx_mass_partial_kernel<float><<<parts, SX_BLOCK, 0, stream>>>((const float*)v, n, part);
-    sx_mass_final_kernel<<<1, 32, 0, stream>>>(part, parts, scale, out);
+    sx_mass_final_kernel<<<1, 256, 0, stream>>>(part, parts, scale, out);
     return cudaGetLastError();
 }
 
@@ -1374,7 +1405,7 @@ cudaError_t sx_upwind_adjoint_launch(const int* rows, const int* off, int row_co
                                                                   (const float*)w, (const float*)u, (float*)ubar, width,
                                                                   height, (float)a, (float)bb, (float)dt, (float)dx,
                                                                   (float)dy, direct, cells, partial);
-    sx_sum_pairs_kernel<<<1, 32, 0, stream>>>(partial, grid, grads);
+    sx_sum_pairs_kernel<<<1, 256, 0, stream>>>(partial, grid, grads);
     return cudaGetLastError();
 }
 
@@ -1449,6 +1480,6 @@ cudaError_t sx_upwind_adjoint_chunk_launch(const int* off, const int* b, const i
                                                                           (float*)ubar, width, height, (float)a,
                                                                           (float)bb, (float)dt, fdx, fdy, p, partial);
     }
-    sx_sum_pairs_kernel<<<1, 32, 0, stream>>>(partial, blocks, grads);
+    sx_sum_pairs_kernel<<<1, 256, 0, stream>>>(partial, blocks, grads);
     return cudaGetLastError();
 }
