@@ -55,7 +55,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-amr", action="store_true", help="skip the two-level AMR step section")
     p.add_argument("--no-autotune", action="store_true", help="use the automatic launch choice")
-    p.add_argument("--section", default="all", choices=["all", "amr", "adjoint"],
+    p.add_argument("--section", default="all", choices=["all", "amr", "adjoint", "batched"],
                    help="run only the AMR or the adjoint section (for profiling)")
     return p.parse_args()
 
@@ -379,6 +379,68 @@ def adjoint_section(device, base: int = 2048, steps: int = 50, every: int = 10, 
             "check": "FP32 adjoint gradient vs FP64 central differences of the same loss"}
 
 
+def batched_section(device, count: int = 256, repeats: int = 10):
+    """Batched uneven sets: `count` sets with sides log-uniform in [128, 4096] and lognormal(1.5, 1.0)
+    intervals per row.  Every set gets a union and an intersection with its partner and one FP32
+    upwind step; each of the three is one launch of the set or stencil kernel over the whole batch
+    (rows of set i on band i), through the public API (host synchronisations included)."""
+    import torch
+
+    from subsetix_b200 import synth
+    from subsetix_b200.batch import SetBatch, batched_binary, batched_upwind
+    from subsetix_b200.subsetix_cupy.expressions import IntervalSet
+
+    sides, a_sets = synth.batched_uneven_sets(count=count, seed=3)
+    _, b_sets = synth.batched_uneven_sets(count=count, seed=4)
+
+    def dev(h):
+        return IntervalSet._trusted(*(torch.as_tensor(x, device=device) for x in h))
+
+    A = SetBatch.from_sets([dev(h) for h in a_sets], sides)
+    B = SetBatch.from_sets([dev(h) for h in b_sets], sides)
+    n_in = int(A.combined.begin.numel() + B.combined.begin.numel())
+    cells = int((torch.as_tensor(A.combined.end) - torch.as_tensor(A.combined.begin)).sum())
+    gen = torch.Generator(device=device)
+    gen.manual_seed(5)
+    vals = torch.rand(cells, device=device, generator=gen)
+    out = torch.empty_like(vals)
+    width = max(sides)
+    dt, dx = 0.25 / width, 1.0 / width
+
+    def step():
+        u = batched_binary(A, B, "union")
+        i = batched_binary(A, B, "intersection")
+        batched_upwind(A, vals, width=width, a=1.0, b=0.5, dt=dt, dx=dx, dy=dx, out=out)
+        return u, i
+
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream(device)
+    marks = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    t_u = t_i = t_w = 0.0
+    for _ in range(repeats):
+        marks[0].record(stream)
+        batched_binary(A, B, "union")
+        marks[1].record(stream)
+        batched_binary(A, B, "intersection")
+        marks[2].record(stream)
+        batched_upwind(A, vals, width=width, a=1.0, b=0.5, dt=dt, dx=dx, dy=dx, out=out)
+        marks[3].record(stream)
+        torch.cuda.synchronize()
+        t_u += marks[0].elapsed_time(marks[1])
+        t_i += marks[1].elapsed_time(marks[2])
+        t_w += marks[2].elapsed_time(marks[3])
+    t_u, t_i, t_w = t_u / repeats, t_i / repeats, t_w / repeats
+    return {"workload": f"{count} sets, sides log-uniform [128, 4096], lognormal(1.5, 1.0) intervals per row; "
+                        "union + intersection + one FP32 upwind step per set, one launch each for the batch",
+            "sets": count, "rows": int(sum(sides)), "input_intervals": n_in, "cells": cells,
+            "union_ms": t_u, "intersection_ms": t_i, "upwind_ms": t_w, "batch_step_ms": t_u + t_i + t_w,
+            "setops_gintervals_per_s": 2 * n_in / ((t_u + t_i) / 1e3) / 1e9,
+            "upwind_gcell_updates_per_s": cells / (t_w / 1e3) / 1e9,
+            "timing": "device events around the public calls (host synchronisations of the API included)"}
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -399,9 +461,9 @@ def main():
         dist.init_process_group("nccl", init_method="env://", timeout=timedelta(seconds=120),
                                 device_id=device)
 
-    if args.section in ("amr", "adjoint"):
+    if args.section in ("amr", "adjoint", "batched"):
         # one section alone (profiling runs); prints that section's JSON object
-        out = amr_section(device) if args.section == "amr" else adjoint_section(device)
+        out = {"amr": amr_section, "adjoint": adjoint_section, "batched": batched_section}[args.section](device)
         if rank == 0:
             print(json.dumps({args.section: out}), flush=True)
         if world > 1:
@@ -518,6 +580,7 @@ def main():
     if not args.no_amr:
         line["amr_step"] = amr_section(device)
         line["adjoint"] = adjoint_section(device)
+        line["batched"] = batched_section(device)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         one = [synth_one for synth_one in workload(1)]
         line["cpu_baseline"] = cpu_baseline(one, args.cpu_seconds, True)

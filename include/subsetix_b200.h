@@ -321,16 +321,18 @@ int sx_upwind(int dtype, const int32_t* rows, const int32_t* row_ids, const int3
  *   sx_upwind_plan       chunk_offsets[n + 1] = exclusive scan of
  *                        ceil(len / 128) per interval; result = {chunks,
  *                        flags}; workspace: sx_scan_workspace_bytes(n);
- *   sx_upwind_plan_fill  chunk_info[8 * chunks] (16-byte aligned): per
- *                        128-cell chunk its interval, its index in the
- *                        interval, its row, and where the rows above and
- *                        below start to overlap it (lookup as for sx_upwind).
+ *   sx_upwind_plan_fill  chunk_info[16 * chunks] (16-byte aligned): per
+ *                        128-cell chunk its first column, value index and
+ *                        interval bounds, its row, whether its interval
+ *                        touches its neighbours in the row, and where the
+ *                        rows above and below start to overlap it (lookup
+ *                        as for sx_upwind).
  * Each step is then sx_upwind_chunked (values != out). */
 int sx_upwind_plan(const int32_t* begin, const int32_t* end, int64_t n, int32_t* chunk_offsets, int32_t* result,
                    void* workspace, size_t workspace_bytes, void* stream);
 int sx_upwind_plan_fill(const int32_t* rows, const int32_t* row_offsets, int32_t row_count, const int32_t* begin,
-                        const int32_t* end, int64_t n, const int32_t* chunk_offsets, int64_t chunks,
-                        const int32_t* lookup, int32_t height, int32_t* chunk_info, void* stream);
+                        const int32_t* end, const int32_t* cell_offsets, int64_t n, const int32_t* chunk_offsets,
+                        int64_t chunks, const int32_t* lookup, int32_t height, int32_t* chunk_info, void* stream);
 int sx_upwind_chunked(int dtype, const int32_t* row_offsets, const int32_t* begin, const int32_t* end,
                       const int32_t* cell_offsets, const int32_t* chunk_info, int64_t chunks, const int32_t* lookup,
                       const void* values, void* out, int32_t width, int32_t height, double a, double b, double dt,

@@ -30,6 +30,28 @@ def empty_i32(n: int, device) -> torch.Tensor:
     return torch.empty(max(int(n), 0), dtype=I32, device=device)
 
 
+def max_tile_boundaries(leaves, rows: int, device, tile_rows: int = 32) -> int:
+    """Largest number of leaf boundaries in one tile of ``tile_rows`` aligned rows (one synchronisation)."""
+    if rows <= 0:
+        return 0
+    edges = torch.arange(0, rows + tile_rows, tile_rows, device=device).clamp_(max=rows).long()
+    total = None
+    for leaf in leaves:
+        off = leaf[2]
+        ends = leaf[5] if len(leaf) > 5 and leaf[5] is not None else None
+        if ends is not None:
+            return 0  # explicit row ranges: the union sweep, no tiles
+        t = off[edges[1:]] - off[edges[:-1]]
+        total = t if total is None else total + t
+    return 2 * int(total.max().item())
+
+
+def _default_keys(leaves, rows: int) -> int:
+    tiles = max(1, (rows + 31) // 32)
+    avg = 2 * sum(int(leaf[0].numel()) for leaf in leaves) // tiles
+    return avg + avg // 4 + 256
+
+
 def bool_eval(leaves: Sequence[Tuple[torch.Tensor, torch.Tensor, torch.Tensor, int]], rows: int, table: Sequence[int],
               mode: int, device, out: Optional[Tuple[torch.Tensor, torch.Tensor]] = None):
     """Run the row sweep (sx_bool_eval) and read back its result pair.
@@ -41,7 +63,14 @@ def bool_eval(leaves: Sequence[Tuple[torch.Tensor, torch.Tensor, torch.Tensor, i
     ``(begin, end, offsets, total, flags)``; begin and end are capacity
     buffers to be sliced to ``total``.
     """
-    ob, oe, ooff, result = bool_eval_async(leaves, rows, table, mode, device, out)
+    tuning = None
+    if mode == _lib.MODE_TABLE and not TUNING and rows > 0:
+        # skewed rows: size the tile capacity for the largest tile, so no tile
+        # leaves the merge path (shared memory allows 12288 keys per tile)
+        need = max_tile_boundaries(leaves, rows, device)
+        if need > _default_keys(leaves, rows):
+            tuning = {"kernel": 3, "staging_cap": min(need, 12288)}
+    ob, oe, ooff, result = bool_eval_async(leaves, rows, table, mode, device, out, tuning=tuning)
     if result is None:
         return ob, oe, ooff, 0, 0
     total, flags = read_pair(result)
@@ -333,7 +362,7 @@ def upwind(rows, offsets, begin, end, cell_offs, cells: int, lookup, values, out
                              1 if direct else 0, stream_handle(device)), "sx_upwind")
 
 
-def upwind_plan(rows, offsets, begin, end, lookup, height: int, device):
+def upwind_plan(rows, offsets, begin, end, cell_offs, lookup, height: int, device):
     """Plan of sx_upwind_chunked for a fixed geometry: ``(chunk_info, chunks)`` (one synchronisation)."""
     lib = _lib.load()
     n = int(begin.numel())
@@ -346,10 +375,10 @@ def upwind_plan(rows, offsets, begin, end, lookup, height: int, device):
     chunks, flags = read_pair(result)
     if flags & _lib.FLAG_TIMEOUT:
         raise _lib.SubsetixError("sx_upwind_plan: look-back wait timed out")
-    info = empty_i32(8 * max(chunks, 1), device)
-    _lib.check(lib.sx_upwind_plan_fill(ptr(rows), ptr(offsets), int(rows.numel()), ptr(begin), ptr(end), n,
-                                       ptr(chunk_off), chunks, ptr(lookup), int(height), ptr(info), s),
-               "sx_upwind_plan_fill")
+    info = empty_i32(16 * max(chunks, 1), device)
+    _lib.check(lib.sx_upwind_plan_fill(ptr(rows), ptr(offsets), int(rows.numel()), ptr(begin), ptr(end),
+                                       ptr(cell_offs), n, ptr(chunk_off), chunks, ptr(lookup), int(height), ptr(info),
+                                       s), "sx_upwind_plan_fill")
     return info, chunks
 
 

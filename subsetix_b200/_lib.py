@@ -97,7 +97,7 @@ _SIGNATURES = {
                                  ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                  c_vp]),
     "sx_upwind_plan": (ctypes.c_int, [c_vp, c_vp, ctypes.c_int64, c_vp, c_vp, c_vp, ctypes.c_size_t, c_vp]),
-    "sx_upwind_plan_fill": (ctypes.c_int, [c_vp, c_vp, ctypes.c_int32, c_vp, c_vp, ctypes.c_int64, c_vp,
+    "sx_upwind_plan_fill": (ctypes.c_int, [c_vp, c_vp, ctypes.c_int32, c_vp, c_vp, c_vp, ctypes.c_int64, c_vp,
                                            ctypes.c_int64, c_vp, ctypes.c_int32, c_vp, c_vp]),
     "sx_upwind_chunked": (ctypes.c_int, [ctypes.c_int, c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.c_int64, c_vp, c_vp, c_vp,
                                          ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double,

@@ -49,8 +49,8 @@ class Level:
         if bad:
             raise ValueError("interval_set rows exceed provided height")
         self.direct = not (_core.check_rows(self.begin, self.end, self.off, device) & _ROWS_UNSAFE)
-        self.chunk_off, self.chunks = (_core.upwind_plan(self.rows, self.off, self.begin, self.end, self.lookup,
-                                                         self.height, device) if self.direct else (None, 0))
+        self.chunk_off, self.chunks = (_core.upwind_plan(self.rows, self.off, self.begin, self.end, self.cell_off,
+                                                         self.lookup, self.height, device) if self.direct else (None, 0))
         self.device = device
         lib = _lib.load()
         nbytes = max(int(lib.sx_upwind_adjoint_scratch_bytes(self.cells)),

@@ -460,17 +460,18 @@ int sx_upwind_plan(const int32_t* begin, const int32_t* end, int64_t n, int32_t*
 }
 
 int sx_upwind_plan_fill(const int32_t* rows, const int32_t* row_offsets, int32_t row_count, const int32_t* begin,
-                        const int32_t* end, int64_t n, const int32_t* chunk_offsets, int64_t chunks,
-                        const int32_t* lookup, int32_t height, int32_t* chunk_info, void* stream)
+                        const int32_t* end, const int32_t* cell_offsets, int64_t n, const int32_t* chunk_offsets,
+                        int64_t chunks, const int32_t* lookup, int32_t height, int32_t* chunk_info, void* stream)
 {
     if (row_count < 0 || n < 0 || n > INT32_MAX || chunks < 0 || height <= 0)
         return fail(SX_ERR_INVALID, "sx_upwind_plan_fill: bad size");
     if (n == 0 || chunks == 0) return SX_OK;
-    if (!rows || !row_offsets || !begin || !end || !chunk_offsets || !lookup || !chunk_info)
+    if (!rows || !row_offsets || !begin || !end || !cell_offsets || !chunk_offsets || !lookup || !chunk_info)
         return fail(SX_ERR_INVALID, "sx_upwind_plan_fill: null argument");
     if (((uintptr_t)chunk_info & 15u) != 0) return fail(SX_ERR_INVALID, "sx_upwind_plan_fill: chunk_info must be 16-byte aligned");
-    cudaError_t err = sx_upwind_plan_fill_launch(rows, row_offsets, row_count, begin, end, (int)n, chunk_offsets, chunks,
-                                                 lookup, height, chunk_info, (cudaStream_t)stream);
+    cudaError_t err = sx_upwind_plan_fill_launch(rows, row_offsets, row_count, begin, end, cell_offsets, (int)n,
+                                                 chunk_offsets, chunks, lookup, height, chunk_info,
+                                                 (cudaStream_t)stream);
     if (err != cudaSuccess) return cuda_fail(err, "sx_upwind_plan_fill");
     return SX_OK;
 }

@@ -683,14 +683,25 @@ __device__ __forceinline__ T sx_row_take(SxRowReader& r, int x, int width, const
     return v[r.cc + (x - r.cb)];
 }
 
-// Per-chunk plan: info[8u .. 8u+7] = (interval, chunk within it, row id,
-// first interval of the row below ending after the chunk's first cell, end
-// of that row's intervals, the same two for the row above, 0).  Depends only
-// on the geometry, so it is built once per set.
+// Per-chunk plan, SX_PLAN_INTS ints per 128-cell chunk, everything a warp
+// needs before its data loads:
+//   [0..3]   first column x0, interval end, value index of x0, touching bits
+//   [4..7]   row below: first interval ending after x0, end of the row's
+//            intervals, that interval's begin and end
+//   [8..11]  row below: its value offset; row above: first interval, end,
+//            begin
+//   [12..15] row above: end and value offset; row id; interval begin
+// Touching bits: on sorted disjoint rows the cell just left of an interval
+// is in the set exactly when the previous interval ends there (bit 0; value
+// index c - 1), likewise on the right (bit 1; c + 1).  The plan depends only
+// on the geometry and is built once per set.
+#define SX_PLAN_INTS 16
+
 __global__ void sx_chunk_info_kernel(const int* __restrict__ rows, const int* __restrict__ off, int row_count,
-                                     const int* __restrict__ b, const int* __restrict__ e, int n,
-                                     const int* __restrict__ chunk_off, long long chunks,
-                                     const int* __restrict__ lookup, int height, int* __restrict__ info)
+                                     const int* __restrict__ b, const int* __restrict__ e,
+                                     const int* __restrict__ coff, int n, const int* __restrict__ chunk_off,
+                                     long long chunks, const int* __restrict__ lookup, int height,
+                                     int* __restrict__ info)
 {
     for (long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x; u < chunks;
          u += (long long)gridDim.x * blockDim.x) {
@@ -701,13 +712,19 @@ __global__ void sx_chunk_info_kernel(const int* __restrict__ rows, const int* __
         }
         const int i = lo;
         const int k = (int)(u - chunk_off[i]);
-        const int row = rows[sx_row_of(off, row_count, i)];
+        const int p = sx_row_of(off, row_count, i);
+        const int row = rows[p];
         const int x0 = b[i] + SX_CHUNK * k;
+        const int c0 = coff[i] + SX_CHUNK * k;
         const SxRowCursor dn = sx_row_cursor(row - 1, x0, height, lookup, off, e);
         const SxRowCursor up = sx_row_cursor(row + 1, x0, height, lookup, off, e);
-        int4* o = (int4*)(info + 8 * u);
-        o[0] = make_int4(i, k, row, dn.j);
-        o[1] = make_int4(dn.je, up.j, up.je, 0);
+        const int touch = ((i > off[p] && e[i - 1] == b[i]) ? 1 : 0) | ((i + 1 < off[p + 1] && b[i + 1] == e[i]) ? 2 : 0);
+        const bool hd = dn.j < dn.je, hu = up.j < up.je;
+        int4* o = (int4*)(info + (long long)SX_PLAN_INTS * u);
+        o[0] = make_int4(x0, e[i], c0, touch);
+        o[1] = make_int4(dn.j, dn.je, hd ? b[dn.j] : 0, hd ? e[dn.j] : 0);
+        o[2] = make_int4(hd ? coff[dn.j] : 0, up.j, up.je, hu ? b[up.j] : 0);
+        o[3] = make_int4(hu ? e[up.j] : 0, hu ? coff[up.j] : 0, row, b[i]);
     }
 }
 
@@ -723,20 +740,18 @@ __global__ void __launch_bounds__(256) sx_upwind_chunk_kernel(const int* __restr
     const int lane = threadIdx.x & 31;
     const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
     for (long long u = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); u < chunks; u += warps) {
-        const int4 p0 = __ldg((const int4*)(info + 8 * u));
-        const int4 p1 = __ldg((const int4*)(info + 8 * u) + 1);
-        const int i = p0.x, k = p0.y, row = p0.z;
-        const int ib = b[i], ie = e[i];
-        const int x0 = ib + SX_CHUNK * k;
-        const long long c0 = (long long)coff[i] + (long long)SX_CHUNK * k;
+        const int4* pl = (const int4*)(info + (long long)SX_PLAN_INTS * u);
+        const int4 p0 = __ldg(pl), p1 = __ldg(pl + 1), p2 = __ldg(pl + 2), p3 = __ldg(pl + 3);
+        const int x0 = p0.x, ie = p0.y, touch = p0.w, ib = p3.w;
+        const long long c0 = p0.z;
         T cen[SX_CHUNK_SUB];
 #pragma unroll
         for (int q = 0; q < SX_CHUNK_SUB; ++q) {
             const int x = x0 + 32 * q + lane;
             cen[q] = x < ie ? v[c0 + 32 * q + lane] : (T)0;
         }
-        SxRowReader dn = sx_row_reader(p0.w, p1.x, b, e, coff);
-        SxRowReader upc = sx_row_reader(p1.y, p1.z, b, e, coff);
+        SxRowReader dn{p1.x, p1.y, p1.z, p1.w, p2.x};
+        SxRowReader upc{p2.y, p2.z, p2.w, p3.x, p3.y};
         T prev_last = (T)0;  // lane 31's centre of the previous sub-round
 #pragma unroll
         for (int q = 0; q < SX_CHUNK_SUB; ++q) {
@@ -752,12 +767,11 @@ __global__ void __launch_bounds__(256) sx_upwind_chunk_kernel(const int* __restr
             if (lane == 31) from_right = next_first;
             prev_last = __shfl_sync(0xFFFFFFFFu, center, 31);
             T left, right;
-            if (x - 1 >= ib) left = (x - 1 >= 0 && x - 1 < width) ? ((lane > 0 || q > 0) ? from_left : v[c - 1]) : (T)0;
-            else left = act ? sx_sample<T>(row, x - 1, height, width, lookup, off, b, e, coff, v) : (T)0;
-            if (x + 1 < ie)
-                right = (x + 1 >= 0 && x + 1 < width) ? ((lane < 31 || q + 1 < SX_CHUNK_SUB) ? from_right : v[c + 1])
-                                                      : (T)0;
-            else right = act ? sx_sample<T>(row, x + 1, height, width, lookup, off, b, e, coff, v) : (T)0;
+            const bool lin = x - 1 >= 0 && x - 1 < width, rin = x + 1 >= 0 && x + 1 < width;
+            if (x - 1 >= ib) left = lin ? ((lane > 0 || q > 0) ? from_left : v[c - 1]) : (T)0;
+            else left = (act && (touch & 1) && lin) ? v[c - 1] : (T)0;
+            if (x + 1 < ie) right = rin ? ((lane < 31 || q + 1 < SX_CHUNK_SUB) ? from_right : v[c + 1]) : (T)0;
+            else right = (act && (touch & 2) && rin) ? v[c + 1] : (T)0;
             const T down = sx_row_take<T>(dn, x, width, b, e, coff, v, act);
             const T up = sx_row_take<T>(upc, x, width, b, e, coff, v, act);
             if (act) {
@@ -790,12 +804,10 @@ __global__ void __launch_bounds__(256) sx_upwind_adjoint_chunk_kernel(const int*
     const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
     double ga = 0.0, gb = 0.0;
     for (long long q0 = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); q0 < chunks; q0 += warps) {
-        const int4 p0 = __ldg((const int4*)(info + 8 * q0));
-        const int4 p1 = __ldg((const int4*)(info + 8 * q0) + 1);
-        const int i = p0.x, k = p0.y, row = p0.z;
-        const int ib = b[i], ie = e[i];
-        const int x0 = ib + SX_CHUNK * k;
-        const long long c0 = (long long)coff[i] + (long long)SX_CHUNK * k;
+        const int4* pl = (const int4*)(info + (long long)SX_PLAN_INTS * q0);
+        const int4 p0 = __ldg(pl), p1 = __ldg(pl + 1), p2 = __ldg(pl + 2), p3 = __ldg(pl + 3);
+        const int x0 = p0.x, ie = p0.y, touch = p0.w, row = p3.z, ib = p3.w;
+        const long long c0 = p0.z;
         T wc[SX_CHUNK_SUB], uc[SX_CHUNK_SUB];
 #pragma unroll
         for (int q = 0; q < SX_CHUNK_SUB; ++q) {
@@ -803,8 +815,8 @@ __global__ void __launch_bounds__(256) sx_upwind_adjoint_chunk_kernel(const int*
             wc[q] = act ? w[c0 + 32 * q + lane] : (T)0;
             uc[q] = act ? u[c0 + 32 * q + lane] : (T)0;
         }
-        SxRowReader dn = sx_row_reader(p0.w, p1.x, b, e, coff);
-        SxRowReader upr = sx_row_reader(p1.y, p1.z, b, e, coff);
+        SxRowReader dn{p1.x, p1.y, p1.z, p1.w, p2.x};
+        SxRowReader upr{p2.y, p2.z, p2.w, p3.x, p3.y};
         SxRowReader dn2 = dn, up2 = upr;
         T wprev = (T)0, uprev = (T)0;
 #pragma unroll
@@ -835,16 +847,18 @@ __global__ void __launch_bounds__(256) sx_upwind_adjoint_chunk_kernel(const int*
                 const T uv = first ? u[c - 1] : ul;
                 u_left = (x - 1 >= 0 && x - 1 < width) ? uv : (T)0;
             } else {
-                w_left = act ? sx_in_set<T>(row, x - 1, height, lookup, off, b, e, coff, w) : (T)0;
-                u_left = act ? sx_sample<T>(row, x - 1, height, width, lookup, off, b, e, coff, u) : (T)0;
+                const bool t = act && (touch & 1);
+                w_left = t ? w[c - 1] : (T)0;
+                u_left = (t && x - 1 >= 0 && x - 1 < width) ? u[c - 1] : (T)0;
             }
             if (x + 1 < ie) {
                 w_right = last ? w[c + 1] : wr;
                 const T uv = last ? u[c + 1] : ur;
                 u_right = (x + 1 >= 0 && x + 1 < width) ? uv : (T)0;
             } else {
-                w_right = act ? sx_in_set<T>(row, x + 1, height, lookup, off, b, e, coff, w) : (T)0;
-                u_right = act ? sx_sample<T>(row, x + 1, height, width, lookup, off, b, e, coff, u) : (T)0;
+                const bool t = act && (touch & 2);
+                w_right = t ? w[c + 1] : (T)0;
+                u_right = (t && x + 1 >= 0 && x + 1 < width) ? u[c + 1] : (T)0;
             }
             // rows above and below: w in-set needs jdom only (x is then inside the domain, so the
             // reader's domain test is the same), u needs the forward's domain test
@@ -1418,12 +1432,12 @@ cudaError_t sx_upwind_plan_launch(const int* b, const int* e, int n, int* chunk_
 }
 
 cudaError_t sx_upwind_plan_fill_launch(const int* rows, const int* off, int row_count, const int* b, const int* e,
-                                       int n, const int* chunk_off, long long chunks, const int* lookup, int height,
-                                       int* info, cudaStream_t stream)
+                                       const int* coff, int n, const int* chunk_off, long long chunks,
+                                       const int* lookup, int height, int* info, cudaStream_t stream)
 {
     if (n <= 0 || chunks <= 0) return cudaSuccess;
-    sx_chunk_info_kernel<<<sx_grid(chunks, 256, 148 * 32), 256, 0, stream>>>(rows, off, row_count, b, e, n, chunk_off,
-                                                                             chunks, lookup, height, info);
+    sx_chunk_info_kernel<<<sx_grid(chunks, 256, 148 * 32), 256, 0, stream>>>(rows, off, row_count, b, e, coff, n,
+                                                                             chunk_off, chunks, lookup, height, info);
     return cudaGetLastError();
 }
 

@@ -134,8 +134,8 @@ cudaError_t sx_upwind_adjoint_launch(const int* rows, const int* off, int row_co
 cudaError_t sx_upwind_plan_launch(const int* b, const int* e, int n, int* chunk_off, int* result, const SxScanState& st,
                                   cudaStream_t stream);
 cudaError_t sx_upwind_plan_fill_launch(const int* rows, const int* off, int row_count, const int* b, const int* e,
-                                       int n, const int* chunk_off, long long chunks, const int* lookup, int height,
-                                       int* info, cudaStream_t stream);
+                                       const int* coff, int n, const int* chunk_off, long long chunks,
+                                       const int* lookup, int height, int* info, cudaStream_t stream);
 cudaError_t sx_upwind_chunk_launch(const int* off, const int* b, const int* e, const int* coff, const int* info,
                                    long long chunks, const int* lookup, const void* v, void* out, int width, int height,
                                    double a, double bb, double dt, double dx, double dy, int dbl, cudaStream_t stream);

@@ -14,6 +14,7 @@ precision (an addition of this package).
 
 from __future__ import annotations
 
+import weakref
 from typing import Any, Optional
 
 import torch
@@ -33,14 +34,34 @@ class _Geometry:
     lookup (and its synchronising range check) once.
     """
 
-    __slots__ = ("height", "lookup", "direct", "chunk_off", "chunks")
+    __slots__ = ("height", "lookup", "direct", "chunk_off", "chunks", "cell_off", "_seen")
 
-    def __init__(self, height: int, lookup: torch.Tensor, direct: bool, chunk_off=None, chunks: int = 0):
+    def __init__(self, height: int, lookup: torch.Tensor, direct: bool, chunk_off=None, chunks: int = 0,
+                 cell_off=None):
         self.height = height
         self.lookup = lookup
         self.direct = direct
         self.chunk_off = chunk_off
         self.chunks = chunks
+        self.cell_off = cell_off
+        self._seen = None
+
+    def canonical(self, cell_off: torch.Tensor) -> bool:
+        """Whether ``cell_off`` is the prefix sum of the interval lengths.
+
+        The chunk plan holds value indices taken from that prefix sum, so the
+        chunked kernel serves only fields laid out that way.  The answer for
+        one offsets tensor is kept until the tensor is modified in place.
+        """
+        seen = self._seen
+        if seen is not None and seen[0]() is cell_off and seen[1] == cell_off._version:
+            return seen[2]
+        ok = cell_off.data_ptr() == self.cell_off.data_ptr() or bool(torch.equal(cell_off, self.cell_off))
+        try:
+            self._seen = (weakref.ref(cell_off), cell_off._version, ok)
+        except TypeError:  # pragma: no cover - tensors that refuse weak references
+            self._seen = None
+        return ok
 
 
 def _geometry(interval_set, height: int) -> _Geometry:
@@ -56,11 +77,12 @@ def _geometry(interval_set, height: int) -> _Geometry:
         raise ValueError("interval_set rows exceed provided height")
     flags = _core.check_rows(_t(interval_set.begin), _t(interval_set.end), _t(interval_set.row_offsets), device)
     direct = not (flags & (_lib.ROWS_UNSORTED_BEGIN | _lib.ROWS_OVERLAP | _lib.ROWS_EMPTY))
-    chunk_off, chunks = (None, 0)
+    chunk_off, chunks, coff = (None, 0, None)
     if direct:
-        chunk_off, chunks = _core.upwind_plan(rows, _t(interval_set.row_offsets), _t(interval_set.begin),
-                                              _t(interval_set.end), lookup, height, device)
-    geo = _Geometry(height, lookup, direct, chunk_off, chunks)
+        b, e = _t(interval_set.begin), _t(interval_set.end)
+        coff, _ = _core.cell_offsets(b, e, device)
+        chunk_off, chunks = _core.upwind_plan(rows, _t(interval_set.row_offsets), b, e, coff, lookup, height, device)
+    geo = _Geometry(height, lookup, direct, chunk_off, chunks, coff)
     try:
         object.__setattr__(interval_set, "_sx_stencil", geo)
     except Exception:  # pragma: no cover - sets that refuse attributes
@@ -113,8 +135,9 @@ def step_upwind_interval(field: IntervalField, *, width: int, height: int, a: fl
         if bool(((rid < 0) | (rid >= height)).any()) or int(geo.lookup[rid.long()].min().item()) < 0:
             raise ValueError("interval_set rows exceed provided height")
     vals = vals.contiguous()
-    if geo.chunk_off is not None and rid is None and out_t.data_ptr() != vals.data_ptr():
-        # fixed geometry with sorted, disjoint rows: the chunked kernel (same results)
+    if (geo.chunk_off is not None and rid is None and out_t.data_ptr() != vals.data_ptr()
+            and geo.canonical(cell_off)):
+        # fixed geometry with sorted, disjoint rows and packed values: the chunked kernel (same results)
         _core.upwind_chunked(_t(s.row_offsets), begin, _t(s.end), cell_off, geo.chunk_off, geo.chunks, geo.lookup, vals,
                              out_t, width, height, a, b, dt, dx, dy, device)
     else:

@@ -295,7 +295,7 @@ def test_upwind_chunked_equals_generic(cuda_device, dtype):
         coff, cells = _core.cell_offsets(b, e, dev)
         lookup, bad = _core.row_lookup(rows, H, dev)
         assert not bad
-        chunk_off, chunks = _core.upwind_plan(rows, off, b, e, lookup, H, dev)
+        chunk_off, chunks = _core.upwind_plan(rows, off, b, e, coff, lookup, H, dev)
         v = torch.as_tensor(rng.standard_normal(cells), device=dev).to(dtype)
         for a_, b_ in ((0.6, 0.3), (-0.4, -0.9)):
             ref = torch.empty_like(v)
@@ -304,3 +304,28 @@ def test_upwind_chunked_equals_generic(cuda_device, dtype):
             _core.upwind_chunked(off, b, e, coff, chunk_off, chunks, lookup, v, got, W, H, a_, b_, 1e-3, 1e-2, 1e-2,
                                  dev)
             assert torch.equal(got, ref)
+
+
+def test_upwind_padded_cell_offsets(cuda_device):
+    """Values laid out with gaps between intervals take the generic kernel and agree."""
+    dev = torch.device("cuda", 0)
+    h = rand_set(200, 9.0, seed=41, row_stride=1, touching=True, row0=0)
+    S = dev_set(h)
+    b, e = h[0].astype(np.int64), h[1].astype(np.int64)
+    lens = e - b
+    packed = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    padded = np.concatenate([[0], np.cumsum(lens + 3)]).astype(np.int32)
+    rng = np.random.default_rng(5)
+    v = rng.standard_normal(int(packed[-1])).astype(np.float32)
+    vp = np.zeros(int(padded[-1]), np.float32)
+    for i in range(lens.size):
+        vp[padded[i]:padded[i] + lens[i]] = v[packed[i]:packed[i + 1]]
+    kw = dict(width=180, height=202, a=0.5, b=-0.7, dt=1e-3, dx=1e-2, dy=1e-2)
+    f = sc.IntervalField(interval_set=S, values=torch.as_tensor(v, device=dev),
+                         interval_cell_offsets=torch.as_tensor(packed, device=dev))
+    fp = sc.IntervalField(interval_set=S, values=torch.as_tensor(vp, device=dev),
+                          interval_cell_offsets=torch.as_tensor(padded, device=dev))
+    ref = sc.step_upwind_interval(f, **kw).cpu().numpy()
+    got = sc.step_upwind_interval(fp, **kw).cpu().numpy()
+    for i in range(lens.size):
+        assert np.array_equal(got[padded[i]:padded[i] + lens[i]], ref[packed[i]:packed[i + 1]])
