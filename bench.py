@@ -149,9 +149,14 @@ def peak_hbm():
         return 6650.0, "fallback"
 
 
-def traffic_per_launch(copies: int):
-    """DRAM bytes of one fused launch, from the committed ncu summary (scaled by copies)."""
-    path = os.path.join(REPO, "profiles", "sx_merge_kernel_shapes4096.md")
+# sx_tuning kernel kinds (0 = automatic, the warp-tile segmented sweep)
+KERNELS = {1: "sx_sweep_kernel<5,0>", 2: "sx_sweep_smem_kernel<5>", 3: "sx_merge_kernel<5>", 4: "sx_seg_kernel<5>",
+           5: "sx_wseg_kernel<5>"}
+
+
+def traffic_per_launch(copies: int, kernel: str = "sx_wseg_kernel<5>"):
+    """DRAM bytes of one fused launch, from the committed ncu summary of that kernel (scaled by copies)."""
+    path = os.path.join(REPO, "profiles", kernel.split("<")[0] + "_shapes4096.md")
     try:
         for line in open(path):
             if line.startswith("traffic_bytes_per_copy:"):
@@ -558,6 +563,7 @@ def main():
     e2e_value = world * n_in / (e2e_ms / 1e3) / 1e9
 
     kernel_ms = statistics.mean(per_step)
+    kname = KERNELS[int(tuning.get("kernel", 0)) or 5]
     peak, peak_kind = peak_hbm()
     achieved = algo / (kernel_ms / 1e3) / 1e9
     line = {
@@ -572,8 +578,8 @@ def main():
                 "ms_per_step": e2e_ms},
         "gpu_launches": args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic_per_launch(args.copies),
-                     "peak_source": peak_kind, "algorithmic_bytes": algo, "kernel": "sx_merge_kernel<5>",
+                     "frac": achieved / peak, "traffic": traffic_per_launch(args.copies, kname),
+                     "peak_source": peak_kind, "algorithmic_bytes": algo, "kernel": kname,
                      "kernel_ms": kernel_ms},
         "clocks": clocks.summary(),
     }

@@ -92,21 +92,35 @@ typedef struct sx_leaf {
 
 /* Launch tuning for sx_bool_eval; NULL or zero fields select automatic values.
  * kernel: 1 = global-memory sweep, 2 = shared-memory staged sweep, 3 =
- * merge-path tile kernel (table mode; the default); blocks_per_sm: residency
- * cap of the global sweep; staging_cap: elements per warp of the staged
- * sweep, or keys per tile of the merge-path kernel.  Results never depend on
- * the tuning. */
+ * merge-path tile kernel, 4 = segmented sweep (table mode; the default);
+ * blocks_per_sm: residency cap of the global sweep; staging_cap: elements per
+ * warp of the staged sweep, or boundaries per tile of kernels 3 and 4;
+ * warps: warps per tile of kernel 4; tile_rows: rows per tile of kernel 4
+ * (16 or 32).  Results never depend on the tuning. */
 typedef struct sx_tuning {
     int32_t kernel;
     int32_t blocks_per_sm;
     int32_t staging_cap;
+    int32_t warps;
+    int32_t tile_rows;
 } sx_tuning;
 
+/* Workspace for sx_bool_eval: the size returned here lets every kernel use
+ * its preferred tiles; sx_bool_eval accepts down to 8 bytes per 32 rows plus
+ * a few KiB (the look-back state of 32-row tiles) and then uses 32-row tiles. */
 size_t sx_bool_workspace_bytes(int32_t rows);
 int sx_bool_eval(const sx_leaf* leaves /* host array of k */, int k, int32_t rows, const uint32_t* table /* host, 8 */,
                  int mode, int32_t* out_begin, int32_t* out_end, int32_t* out_offsets, int64_t capacity,
                  int32_t* result, void* workspace, size_t workspace_bytes, const sx_tuning* tuning /* host */,
                  void* stream);
+
+/* Largest number of leaf boundaries (2 x intervals, summed over the leaves)
+ * in one tile of tile_rows_a aligned rows (out[0]) and of tile_rows_b aligned
+ * rows (out[1]), asynchronously on `stream`.  The leaves' row_offsets are
+ * aligned (rows + 1 entries each); the other sx_leaf fields are ignored.
+ * Callers size sx_tuning.staging_cap with it.  No reference counterpart. */
+int sx_tile_boundaries_max(const sx_leaf* leaves /* host array of k */, int k, int32_t rows, int32_t tile_rows_a,
+                           int32_t tile_rows_b, int32_t* out /* device, 2 */, void* stream);
 
 /* ---------------------------------------------------------------------------
  * sx_bool_eval without a caller workspace.  This entry point has no

@@ -30,26 +30,31 @@ def empty_i32(n: int, device) -> torch.Tensor:
     return torch.empty(max(int(n), 0), dtype=I32, device=device)
 
 
-def max_tile_boundaries(leaves, rows: int, device, tile_rows: int = 32) -> int:
-    """Largest number of leaf boundaries in one tile of ``tile_rows`` aligned rows (one synchronisation)."""
-    if rows <= 0:
-        return 0
-    edges = torch.arange(0, rows + tile_rows, tile_rows, device=device).clamp_(max=rows).long()
-    total = None
-    for leaf in leaves:
-        off = leaf[2]
-        ends = leaf[5] if len(leaf) > 5 and leaf[5] is not None else None
-        if ends is not None:
-            return 0  # explicit row ranges: the union sweep, no tiles
-        t = off[edges[1:]] - off[edges[:-1]]
-        total = t if total is None else total + t
-    return 2 * int(total.max().item())
+def max_tile_boundaries(leaves, rows: int, device, tile_rows=32):
+    """Largest number of leaf boundaries in one tile of ``tile_rows`` aligned rows (one synchronisation).
+
+    ``tile_rows`` may be a pair of tile heights; the result is then a list
+    with one maximum per height, from the same launch and read-back.
+    """
+    many = isinstance(tile_rows, (tuple, list))
+    heights = list(tile_rows) if many else [tile_rows, tile_rows]
+    if rows <= 0 or any(len(leaf) > 5 and leaf[5] is not None for leaf in leaves):
+        return [0, 0] if many else 0  # no rows, or explicit row ranges (the union sweep has no tiles)
+    lib = _lib.load()
+    arr = (_lib.SxLeaf * len(leaves))()
+    for i, leaf in enumerate(leaves):
+        arr[i].row_offsets = ptr(leaf[2])
+    out = empty_i32(2, device)
+    _lib.check(lib.sx_tile_boundaries_max(arr, len(leaves), int(rows), int(heights[0]), int(heights[1]), ptr(out),
+                                          stream_handle(device)), "sx_tile_boundaries_max")
+    a, b = (int(x) for x in out.tolist())
+    return [a, b] if many else a
 
 
-def _default_keys(leaves, rows: int) -> int:
-    tiles = max(1, (rows + 31) // 32)
+def _default_keys(leaves, rows: int, tile_rows: int = 32) -> int:
+    tiles = max(1, (rows + tile_rows - 1) // tile_rows)
     avg = 2 * sum(int(leaf[0].numel()) for leaf in leaves) // tiles
-    return avg + avg // 4 + 256
+    return avg + avg // 4 + 64
 
 
 def bool_eval(leaves: Sequence[Tuple[torch.Tensor, torch.Tensor, torch.Tensor, int]], rows: int, table: Sequence[int],
@@ -65,11 +70,16 @@ def bool_eval(leaves: Sequence[Tuple[torch.Tensor, torch.Tensor, torch.Tensor, i
     """
     tuning = None
     if mode == _lib.MODE_TABLE and not TUNING and rows > 0:
-        # skewed rows: size the tile capacity for the largest tile, so no tile
-        # leaves the merge path (shared memory allows 12288 keys per tile)
-        need = max_tile_boundaries(leaves, rows, device)
-        if need > _default_keys(leaves, rows):
-            tuning = {"kernel": 3, "staging_cap": min(need, 12288)}
+        # Even rows: 8-row warp tiles with buffers sized for the largest tile
+        # (no tile leaves the staged sweep, no buffer larger than needed).
+        # Skewed rows (the largest 8-row tile far above the mean): 32-row
+        # block tiles sized for their largest tile, which evens out the load.
+        need8, need32 = max_tile_boundaries(leaves, rows, device, tile_rows=(8, 32))
+        mean8 = 2 * sum(int(leaf[0].numel()) for leaf in leaves) / max(1, (rows + 7) // 8)
+        if need8 <= 3 * mean8 + 256:
+            tuning = {"kernel": 5, "staging_cap": min(need8, 25000), "tile_rows": 8}
+        else:
+            tuning = {"kernel": 4, "staging_cap": min(need32, 25000), "tile_rows": 32, "warps": 4}
     ob, oe, ooff, result = bool_eval_async(leaves, rows, table, mode, device, out, tuning=tuning)
     if result is None:
         return ob, oe, ooff, 0, 0
@@ -117,7 +127,8 @@ def bool_eval_async(leaves: Sequence[Tuple[torch.Tensor, torch.Tensor, torch.Ten
     tab = (ctypes.c_uint32 * 8)(*[int(x) & 0xFFFFFFFF for x in (list(table) + [0] * 8)[:8]])
     wsp, wsn = workspace(device, lib.sx_bool_workspace_bytes(int(rows)))
     t = TUNING if tuning is None else tuning
-    tun = _lib.SxTuning(int(t.get("kernel", 0)), int(t.get("blocks_per_sm", 0)), int(t.get("staging_cap", 0)))
+    tun = _lib.SxTuning(int(t.get("kernel", 0)), int(t.get("blocks_per_sm", 0)), int(t.get("staging_cap", 0)),
+                        int(t.get("warps", 0)), int(t.get("tile_rows", 0)))
     rc = lib.sx_bool_eval(arr, k, int(rows), tab, int(mode), ptr(ob), ptr(oe), ptr(ooff), cap, ptr(result), wsp, wsn,
                           ctypes.byref(tun), stream_handle(device))
     _lib.check(rc, "sx_bool_eval")

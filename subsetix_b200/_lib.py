@@ -39,7 +39,8 @@ class SxLeaf(ctypes.Structure):
 
 
 class SxTuning(ctypes.Structure):
-    _fields_ = [("kernel", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32), ("staging_cap", ctypes.c_int32)]
+    _fields_ = [("kernel", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32), ("staging_cap", ctypes.c_int32),
+                ("warps", ctypes.c_int32), ("tile_rows", ctypes.c_int32)]
 
 
 class SxRowList(ctypes.Structure):
@@ -67,6 +68,8 @@ _SIGNATURES = {
     "sx_align_rows": (ctypes.c_int, [ctypes.POINTER(SxRowList), ctypes.c_int, ctypes.c_int32, ctypes.c_int32, c_vp,
                                      ctypes.c_int32, ctypes.POINTER(c_vp), ctypes.POINTER(c_vp), c_vp, c_vp,
                                      ctypes.c_size_t, c_vp]),
+    "sx_tile_boundaries_max": (ctypes.c_int, [ctypes.POINTER(SxLeaf), ctypes.c_int, ctypes.c_int32, ctypes.c_int32,
+                                              ctypes.c_int32, c_vp, c_vp]),
     "sx_check_rows": (ctypes.c_int, [c_vp, c_vp, c_vp, ctypes.c_int32, ctypes.c_int64, c_vp, c_vp]),
     "sx_cell_offsets": (ctypes.c_int, [c_vp, c_vp, ctypes.c_int64, c_vp, c_vp, c_vp, ctypes.c_size_t, c_vp]),
     "sx_prolong_set_workspace_bytes": (ctypes.c_size_t, [ctypes.c_int32]),

@@ -1,9 +1,10 @@
 """Launch autotuner for the row-sweep set algebra (sx_bool_eval).
 
-The candidates are the kernel kinds of ``sx_tuning``: the merge-path tile
-kernel with several key capacities per tile (how many boundaries a block
-stages, i.e. the work per warp), and the one-lane-per-row sweep with
-several residency caps.  Each candidate is timed with CUDA events on the
+The candidates are the kernel kinds of ``sx_tuning``: the warp-tile
+segmented sweep (8-row tiles) with several warps per block, the block-tile
+segmented sweep (32-row tiles) with two block sizes, the merge-path tile
+kernel with two key capacities per tile, and the one-lane-per-row sweep
+with several residency caps.  Each candidate is timed with CUDA events on the
 caller's workload; the fastest is cached under a key of the workload's
 shape (leaf count, row count, mean boundaries per 32-row tile, bucketed by
 powers of two) and installed in ``_core.TUNING`` so later evaluations use
@@ -31,11 +32,17 @@ def workload_key(sizes: Sequence[int], rows: int) -> str:
     return f"k{k}-r{int(math.log2(max(rows, 1)))}-t{int(math.log2(max(per_tile, 1.0)))}"
 
 
-def candidates(sizes: Sequence[int], rows: int) -> List[dict]:
+def candidates(sizes: Sequence[int], rows: int, largest_tile: int = 0, largest_eighth_tile: int = 0) -> List[dict]:
     tiles = max(1, (int(rows) + 31) // 32)
     avg = 2 * sum(int(s) for s in sizes) / tiles
     out = []
-    for f in (1.1, 1.25, 1.5, 2.0):
+    cap8 = min(max(int(avg / 4 * 1.25 + 64), int(largest_eighth_tile)), 25000)
+    for w in (2, 4, 8):
+        out.append({"kernel": 5, "staging_cap": cap8, "warps": w, "tile_rows": 8})
+    cap = min(max(int(avg * 1.25 + 256), int(largest_tile)), 25000)
+    for w in (4, 8):
+        out.append({"kernel": 4, "staging_cap": cap, "warps": w, "tile_rows": 32})
+    for f in (1.25, 2.0):
         out.append({"kernel": 3, "staging_cap": int(avg * f + 256)})
     for b in (3, 5, 8):
         out.append({"kernel": 1, "blocks_per_sm": b})
@@ -57,7 +64,10 @@ def tune_bool_eval(leaves, rows: int, table: Sequence[int], device, *, mode: int
         res = torch.empty(2, dtype=torch.int32, device=device)
         stream = torch.cuda.current_stream(device)
         timings = []
-        for cand in candidates(sizes, rows):
+        table_mode = mode == _lib.MODE_TABLE
+        largest = _core.max_tile_boundaries(leaves, rows, device) if table_mode else 0
+        eighth = _core.max_tile_boundaries(leaves, rows, device, tile_rows=8) if table_mode else 0
+        for cand in candidates(sizes, rows, largest, eighth):
             def launch():
                 _core.bool_eval_async(leaves, rows, table, mode, device, out=(ob, oe), result=res, offsets=off,
                                       tuning=cand)
@@ -83,7 +93,7 @@ def tune_bool_eval(leaves, rows: int, table: Sequence[int], device, *, mode: int
                 json.dump(data, f, indent=1, sort_keys=True)
     if install:
         _core.TUNING.clear()
-        _core.TUNING.update({k: v for k, v in best.items() if k in ("kernel", "blocks_per_sm", "staging_cap")})
+        _core.TUNING.update({k: v for k, v in best.items() if k in ("kernel", "blocks_per_sm", "staging_cap", "warps", "tile_rows")})
     return best
 
 

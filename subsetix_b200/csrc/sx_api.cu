@@ -50,7 +50,11 @@ int sx_abi_version(void) { return SX_ABI_VERSION; }
 
 const char* sx_last_error(void) { return g_err; }
 
-size_t sx_bool_workspace_bytes(int32_t rows) { return sx_sweep_state_bytes(sx_sweep_tiles(rows < 1 ? 1 : rows)); }
+size_t sx_bool_workspace_bytes(int32_t rows)
+{
+    const long long r = rows < 1 ? 1 : rows;
+    return sx_sweep_state_bytes((r + 3) / 4);  // down to 4-row tiles of the segmented sweeps
+}
 
 int sx_bool_eval(const sx_leaf* leaves, int k, int32_t rows, const uint32_t* table, int mode, int32_t* out_begin,
                  int32_t* out_end, int32_t* out_offsets, int64_t capacity, int32_t* result, void* workspace,
@@ -68,9 +72,9 @@ int sx_bool_eval(const sx_leaf* leaves, int k, int32_t rows, const uint32_t* tab
     }
     if (capacity < 0) return fail(SX_ERR_INVALID, "sx_bool_eval: negative capacity");
     if (rows == 0) return SX_OK;
-    if (!workspace || workspace_bytes < sx_bool_workspace_bytes(rows))
-        return fail(SX_ERR_WORKSPACE, "sx_bool_eval: workspace needs %zu bytes, got %zu",
-                    sx_bool_workspace_bytes(rows), workspace_bytes);
+    const size_t ws_min = sx_sweep_state_bytes(sx_sweep_tiles(rows));
+    if (!workspace || workspace_bytes < ws_min)
+        return fail(SX_ERR_WORKSPACE, "sx_bool_eval: workspace needs %zu bytes, got %zu", ws_min, workspace_bytes);
     SxBoolArgs A;
     memset(&A, 0, sizeof(A));
     for (int l = 0; l < k; ++l) {
@@ -93,14 +97,40 @@ int sx_bool_eval(const sx_leaf* leaves, int k, int32_t rows, const uint32_t* tab
     A.capacity = capacity;
     A.result = result;
     if (tuning) {
-        if (tuning->kernel < 0 || tuning->kernel > 3 || tuning->blocks_per_sm < 0 || tuning->staging_cap < 0)
+        if (tuning->kernel < 0 || tuning->kernel > 5 || tuning->blocks_per_sm < 0 || tuning->staging_cap < 0 ||
+            tuning->warps < 0 || tuning->warps > 8 ||
+            tuning->tile_rows < 0 || tuning->tile_rows > 32)
             return fail(SX_ERR_INVALID, "sx_bool_eval: bad tuning");
         A.tune_kernel = tuning->kernel;
         A.tune_blocks_per_sm = tuning->blocks_per_sm;
         A.tune_staging_cap = tuning->staging_cap;
+        A.tune_warps = tuning->warps;
+        A.tune_tile_rows = tuning->tile_rows;
     }
-    cudaError_t err = sx_sweep_launch(A, mode == SX_MODE_UNION, workspace, (cudaStream_t)stream);
+    cudaError_t err = sx_sweep_launch(A, mode == SX_MODE_UNION, workspace, workspace_bytes, (cudaStream_t)stream);
     if (err != cudaSuccess) return cuda_fail(err, "sx_bool_eval");
+    return SX_OK;
+}
+
+int sx_tile_boundaries_max(const sx_leaf* leaves, int k, int32_t rows, int32_t tile_rows_a, int32_t tile_rows_b,
+                           int32_t* out, void* stream)
+{
+    if (k < 1 || k > SX_MAX_LEAVES) return fail(SX_ERR_INVALID, "sx_tile_boundaries_max: k=%d outside [1, %d]", k,
+                                                SX_MAX_LEAVES);
+    if (!leaves || !out) return fail(SX_ERR_INVALID, "sx_tile_boundaries_max: null argument");
+    if (rows < 0 || tile_rows_a < 1 || tile_rows_b < 1)
+        return fail(SX_ERR_INVALID, "sx_tile_boundaries_max: bad rows or tile heights");
+    const int* offs[SX_MAX_LEAVES];
+    for (int l = 0; l < k; ++l) {
+        if (!leaves[l].row_offsets) return fail(SX_ERR_INVALID, "sx_tile_boundaries_max: leaf %d has no offsets", l);
+        offs[l] = leaves[l].row_offsets;
+    }
+    if (rows == 0) {
+        cudaError_t err = cudaMemsetAsync(out, 0, 2 * sizeof(int32_t), (cudaStream_t)stream);
+        return err == cudaSuccess ? SX_OK : cuda_fail(err, "sx_tile_boundaries_max");
+    }
+    cudaError_t err = sx_tile_max_launch(offs, k, rows, tile_rows_a, tile_rows_b, out, (cudaStream_t)stream);
+    if (err != cudaSuccess) return cuda_fail(err, "sx_tile_boundaries_max");
     return SX_OK;
 }
 

@@ -30,11 +30,15 @@ struct SxBoolArgs {
     int* result;  // written by the last block: [0] total intervals, [1] SXF_* flags
     SxScanState scan;
     // launch tuning (0 = automatic): kernel 1 = global-memory sweep, 2 = staged
-    // sweep; blocks_per_sm caps residency (via shared-memory padding);
-    // staging_cap is the staged kernel's per-warp element capacity
+    // sweep, 3 = merge-path tiles, 4 = segmented sweep (the default for
+    // tables); blocks_per_sm caps residency (via shared-memory padding);
+    // staging_cap is the staged kernel's per-warp element capacity, or keys
+    // per tile for kernels 3 and 4
     int tune_kernel;
     int tune_blocks_per_sm;
     int tune_staging_cap;
+    int tune_warps;      // segmented sweep: warps per tile block
+    int tune_tile_rows;  // segmented sweep: rows per tile (16 or 32)
 };
 
 struct SxRowList {
@@ -61,7 +65,10 @@ struct SxAlignArgs {
     int* result;       // [0] rows_out count, [1] flags
 };
 
-cudaError_t sx_sweep_launch(const SxBoolArgs& A, bool union_mode, void* workspace, cudaStream_t stream);
+cudaError_t sx_sweep_launch(const SxBoolArgs& A, bool union_mode, void* workspace, size_t workspace_bytes,
+                            cudaStream_t stream);
+cudaError_t sx_tile_max_launch(const int* const* offsets, int k, int rows, int tra, int trb, int* out,
+                               cudaStream_t stream);
 size_t sx_sweep_state_bytes(long long tiles);
 long long sx_sweep_tiles(int rows);
 cudaError_t sx_scan_i32_launch(const int* in, long long n, int* out, int* result, const SxScanState& st,

@@ -115,3 +115,54 @@ cudaError_t sx_align_launch(SxAlignArgs& A, int out_capacity, const SxScanState&
     sx_align_offsets_kernel<<<dim3(gy, A.k), block, 0, stream>>>(A);
     return cudaGetLastError();
 }
+
+// Largest number of leaf boundaries (2 x intervals, all leaves together) in
+// a tile of `tr[0]` aligned rows and in a tile of `tr[1]` aligned rows;
+// out[0], out[1] must start at zero.
+struct SxOffList {
+    const int* off[SX_MAX_LEAVES];
+};
+
+__global__ void sx_tile_max_kernel(SxOffList L, int k, int rows, int tra, int trb, int* out)
+{
+    const int tiles_a = (rows + tra - 1) / tra, tiles_b = (rows + trb - 1) / trb;
+    int ma = 0, mb = 0;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < tiles_a || t < tiles_b; t += gridDim.x * blockDim.x) {
+        if (t < tiles_a) {
+            const int r0 = t * tra, r1 = min(rows, r0 + tra);
+            int c = 0;
+            for (int l = 0; l < k; ++l) c += L.off[l][r1] - L.off[l][r0];
+            ma = max(ma, c);
+        }
+        if (t < tiles_b) {
+            const int r0 = t * trb, r1 = min(rows, r0 + trb);
+            int c = 0;
+            for (int l = 0; l < k; ++l) c += L.off[l][r1] - L.off[l][r0];
+            mb = max(mb, c);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        ma = max(ma, __shfl_xor_sync(0xFFFFFFFFu, ma, o));
+        mb = max(mb, __shfl_xor_sync(0xFFFFFFFFu, mb, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (ma > 0) atomicMax(&out[0], 2 * ma);
+        if (mb > 0) atomicMax(&out[1], 2 * mb);
+    }
+}
+
+cudaError_t sx_tile_max_launch(const int* const* offsets, int k, int rows, int tra, int trb, int* out,
+                               cudaStream_t stream)
+{
+    SxOffList L;
+    for (int l = 0; l < SX_MAX_LEAVES; ++l) L.off[l] = l < k ? offsets[l] : nullptr;
+    cudaError_t err = cudaMemsetAsync(out, 0, 2 * sizeof(int), stream);
+    if (err != cudaSuccess) return err;
+    const int tiles = (rows + min(tra, trb) - 1) / min(tra, trb);
+    int grid = (tiles + 255) / 256;
+    if (grid > 1184) grid = 1184;
+    if (grid < 1) grid = 1;
+    sx_tile_max_kernel<<<grid, 256, 0, stream>>>(L, k, rows, tra, trb, out);
+    return cudaGetLastError();
+}

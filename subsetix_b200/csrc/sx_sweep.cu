@@ -1060,6 +1060,865 @@ __global__ void __launch_bounds__(SXM_THREADS) sx_merge_kernel(SxBoolArgs A, SxS
     }
 }
 
+// ---------------------------------------------------------------------------
+// Segmented sweep: the default path for set algebra.
+//
+// A block owns one tile of 32 aligned rows, as in the merge-path kernel.
+// Thread 0 copies every leaf's begin and end ranges of the tile into shared
+// memory with bulk asynchronous copies (one round trip for the whole tile,
+// completion counted on an mbarrier); meanwhile the warps build, per leaf,
+// a bitmap of row starts.  Every boundary then becomes a 32-bit key
+// (row << 26 | (x - xmin)) in its leaf's list; the row of an interval is
+// the rank of its row start (a prefix popcount) mapped through the list of
+// the leaf's non-empty rows.  Each list is sorted (rows are consecutive
+// and, on canonical leaves, boundaries rise strictly inside a row) and ends
+// with the sentinel 0xFFFFFFFF.
+//
+// Each thread then sweeps one piece of the tile by itself: the keys in
+// [p_t, p_t+1), where the pivots p_t are the keys of the longest list at
+// positions t/L of it (L threads).  The piece starts in every list at the
+// first key not below p_t (binary searches, interleaved over the lists);
+// the membership state there is the parity of that position, because every
+// interval contributes a begin and an end.  The sweep takes the smallest
+// head, toggles the state bit of every leaf holding it and compares f(state)
+// with f before; a change is an output boundary.  A piece never splits a
+// (row, x) group, so f is evaluated exactly where the truth-table semantics
+// require it.  Output boundaries alternate begin/end and never cross rows
+// (every row ends with all leaves outside, and f(0) = 0).  A thread's output
+// boundaries are at most its keys, so each thread writes them to its own
+// slice of an output area (the space of the copies, dead by then); a block
+// scan of the counts packs them into the key area while the look-back gives
+// the tile's global base, and the tile is written with coalesced stores.
+//
+// Inputs are read once, outputs written once.  Per boundary the sweep
+// costs a few instructions per leaf plus the min and the table lookup.
+//
+// Contract: each leaf's boundaries must rise strictly inside a row
+// (non-empty, non-touching, sorted intervals); otherwise SXF_CONTRACT and
+// the tile writes no intervals.  A tile whose lists exceed the shared-memory
+// capacity or whose coordinates span 2^26 or more is swept by its first
+// warp with the one-lane-per-row sweep (same results, slower).  Every wait
+// is bounded.
+// ---------------------------------------------------------------------------
+#define SXS_XBITS 26
+#define SXS_XMASK ((1u << SXS_XBITS) - 1u)
+#define SXS_MAX_THREADS 256
+#define SXS_SENTINEL 0xFFFFFFFFu
+#define SXS_WAIT_LIMIT (1u << 22)
+
+struct SxsTile {
+    int off[SX_TABLE_MAX_LEAVES][SXM_TR + 1];
+    int rowtab[SX_TABLE_MAX_LEAVES][SXM_TR];  // rank among the leaf's non-empty rows -> row
+    int rawb[SX_TABLE_MAX_LEAVES];            // word index of the tile's first begin in the copy area
+    int rawe[SX_TABLE_MAX_LEAVES];            // same for the ends
+    unsigned tab[8];
+    int warp[SXS_MAX_THREADS / 32 + 1];
+    int xmin, xmax;
+    int tile, base;
+    unsigned flags;
+    unsigned long long bar;
+};
+
+__device__ __forceinline__ unsigned sxs_saddr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void sxs_bar_init(unsigned long long* bar)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(sxs_saddr(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// The single arrival of the barrier's phase 0, announcing `bytes` of copies.
+__device__ __forceinline__ void sxs_bar_expect(unsigned long long* bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sxs_saddr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// Bulk copy of `bytes` (a multiple of 16) between 16-byte aligned addresses,
+// global to this block's shared memory, counted on `bar`.
+__device__ __forceinline__ void sxs_bulk_copy(void* dst, const void* src, unsigned bytes, unsigned long long* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     sxs_saddr(dst)),
+                 "l"(src), "r"(bytes), "r"(sxs_saddr(bar))
+                 : "memory");
+}
+
+// Bounded wait for phase 0 of `bar`; false if it did not complete.
+__device__ __forceinline__ bool sxs_bar_wait(unsigned long long* bar)
+{
+    const unsigned a = sxs_saddr(bar);
+    for (unsigned i = 0; i < SXS_WAIT_LIMIT; ++i) {
+        unsigned done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(a)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// Single-level decoupled look-back for the segmented sweeps (whole warp).
+// Status word of a tile: bits 0-31 the value, bits 32-33 the kind (1 tile
+// aggregate, 2 inclusive prefix), bits 34-37 the OR of the SXF_* flags of
+// the tiles the value covers.  The tile publishes its aggregate, then reads
+// its 32 nearest predecessors at once (each wait bounded) and adds values up
+// to the nearest inclusive prefix, 32 tiles per step.  Returns the exclusive
+// prefix; `flags` comes back as the OR over this tile and all before it.
+__device__ __forceinline__ int sxs_lookback(const SxSweepState& st, int tile, int aggregate, unsigned& flags)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned long long own = ((unsigned long long)(flags & 15u) << 34) | (unsigned long long)(unsigned)aggregate;
+    if (tile == 0) {
+        if (lane == 0) atomicExch(&st.tile_status[0], own | (SX_KIND_PREFIX << 32));
+        return 0;
+    }
+    if (lane == 0) atomicExch(&st.tile_status[tile], own | (SX_KIND_AGG << 32));
+    int exclusive = 0;
+    unsigned fl = flags;
+    bool timed_out = false;
+    for (int pos = tile - 1;; pos -= 32) {
+        const int t = pos - lane;
+        unsigned long long w = SX_KIND_PREFIX << 32;  // before tile 0: an empty prefix
+        if (t >= 0) w = sx_wait_status(&st.tile_status[t], timed_out);
+        const unsigned pm = __ballot_sync(0xFFFFFFFFu, ((w >> 32) & 3ull) == SX_KIND_PREFIX);
+        const int stop = pm ? __ffs(pm) - 1 : 32;
+        int v = lane <= stop ? (int)(unsigned)(w & 0xFFFFFFFFull) : 0;
+        unsigned f = lane <= stop ? (unsigned)(w >> 34) & 15u : 0u;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+            f |= __shfl_xor_sync(0xFFFFFFFFu, f, o);
+        }
+        exclusive += v;
+        fl |= f;
+        if (pm) break;
+    }
+    if (__any_sync(0xFFFFFFFFu, timed_out)) fl |= SXF_TIMEOUT;
+    if (lane == 0)
+        atomicExch(&st.tile_status[tile], ((unsigned long long)(fl & 15u) << 34) | (SX_KIND_PREFIX << 32) |
+                                              (unsigned long long)(unsigned)(exclusive + aggregate));
+    flags = fl;
+    return exclusive;
+}
+
+// The last tile in ticket order reports the grand total and the flags of
+// every tile; an output beyond the capacity shows as a total above it.
+__device__ __forceinline__ void sxs_report(const SxBoolArgs& A, int tile, int tiles, int base, int aggregate,
+                                           unsigned flags)
+{
+    if (tile == tiles - 1 && (threadIdx.x & 31) == 0) {
+        const long long total = (long long)base + aggregate;
+        A.result[0] = (int)total;
+        A.result[1] = (int)(flags | (total > A.capacity ? SXF_CAPACITY : 0u));
+    }
+}
+
+// Block-wide exclusive sum for any block of whole warps (up to 256 threads).
+__device__ __forceinline__ int sxs_block_excl_sum(int v, int* s_warp, int* total)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    int incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_warp[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        const int w = lane < nw ? s_warp[lane] : 0;
+        int wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xFFFFFFFFu, wi, o);
+            if (lane >= o) wi += y;
+        }
+        if (lane < nw) s_warp[lane] = wi - w;
+        if (lane == nw - 1) s_warp[SXS_MAX_THREADS / 32] = wi;
+    }
+    __syncthreads();
+    const int r = s_warp[wid] + incl - v;
+    *total = s_warp[SXS_MAX_THREADS / 32];
+    __syncthreads();
+    return r;
+}
+
+// First position in the sorted list k[0, n) whose key is not below v.
+__device__ __forceinline__ int sxs_lower_bound(const unsigned* k, int n, unsigned v)
+{
+    int pos = 0;
+    while (n > 0) {
+        const int half = n >> 1;
+        if (k[pos + half] < v) {
+            pos += half + 1;
+            n -= half + 1;
+        } else {
+            n = half;
+        }
+    }
+    return pos;
+}
+
+// One leaf of a sweep step: if the head h equals the step's key c, toggle
+// the leaf's state bit and load the next key from shared-memory byte
+// address pa + 4.  Predicated, so lanes that take different leaves do not
+// diverge.
+__device__ __forceinline__ void sxs_advance(unsigned& h, unsigned& pa, unsigned& state, unsigned c, unsigned bit)
+{
+    asm volatile(
+        "{\n .reg .pred q;\n setp.eq.u32 q, %0, %3;\n @q add.u32 %1, %1, 4;\n @q xor.b32 %2, %2, %4;\n"
+        " @q ld.shared.u32 %0, [%1];\n}\n"
+        : "+r"(h), "+r"(pa), "+r"(state)
+        : "r"(c), "r"(bit));
+}
+
+// Store c at shared-memory byte address oa and advance oa when f != fprev.
+__device__ __forceinline__ void sxs_emit(unsigned& oa, unsigned f, unsigned fprev, unsigned c)
+{
+    asm volatile("{\n .reg .pred q;\n setp.ne.u32 q, %1, %2;\n @q st.shared.u32 [%0], %3;\n @q add.u32 %0, %0, 4;\n}\n"
+                 : "+r"(oa)
+                 : "r"(f), "r"(fprev), "r"(c)
+                 : "memory");
+}
+
+template <int K>
+__device__ __forceinline__ unsigned sxs_f(const SxsTile& S, unsigned tab0, unsigned state)
+{
+    if (K <= 5) return (tab0 >> state) & 1u;
+    return (S.tab[state >> 5] >> (state & 31u)) & 1u;
+}
+
+template <int K>
+__global__ void __launch_bounds__(SXS_MAX_THREADS) sx_seg_kernel(SxBoolArgs A, SxSweepState st, int tiles,
+                                                                  int cap_keys, int tr)
+{
+    extern __shared__ __align__(16) unsigned sxs_smem[];
+    __shared__ SxsTile S;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int L = blockDim.x, NW = L >> 5;
+    if (tid == 0) {
+        S.tile = (int)atomicAdd(&st.counters[0], 1u);
+        S.flags = 0u;
+        S.xmin = INT_MAX;
+        S.xmax = INT_MIN;
+        sxs_bar_init(&S.bar);
+    }
+    if (tid < 8) S.tab[tid] = A.table[tid];
+    __syncthreads();
+    const int tile = S.tile;
+    const int r0 = tile * tr;  // tr <= 32 rows per tile
+    const int nrows = min(tr, A.rows - r0);
+    for (int r = tid; r <= nrows; r += L) {
+#pragma unroll
+        for (int l = 0; l < K; ++l) S.off[l][r] = A.leaf[l].off[r0 + r];
+    }
+    __syncthreads();
+    // Shared memory, in 32-bit words: key lists [0, KS) (leaf l at ks[l],
+    // 2 n_l keys and two sentinels); copies of the begins and ends, later the
+    // output boundaries, [RO, RO + RN); row-start bitmaps and their prefix
+    // popcounts [BO, BO + BN).
+    int n[K], ks[K];
+    long long KSl = 0, El = 0, RNl = 0, BNl = 0;
+    int big = 0, nbig = -1, ksbig = 0;
+    bool ok = true;
+#pragma unroll
+    for (int l = 0; l < K; ++l) {
+        n[l] = S.off[l][nrows] - S.off[l][0];
+        ok = ok && n[l] >= 0;
+        ks[l] = (int)KSl;
+        if (n[l] > nbig) {
+            big = l;
+            nbig = n[l];
+            ksbig = (int)KSl;
+        }
+        KSl += 2ll * n[l] + 2;
+        El += 2ll * n[l];
+        RNl += 2ll * ((n[l] + 11) & ~3);  // two copies of at most n + 6 words, 16-byte aligned
+        BNl += 2ll * ((n[l] + 31) >> 5);
+    }
+    KSl = (KSl + 3) & ~3ll;
+    if (RNl < El + 1) RNl = El + 1;  // output boundaries, plus one slot a finished sweep may store into
+    const bool fits = ok && KSl + RNl + BNl <= (long long)cap_keys;
+    const int E = fits ? (int)El : 0, RO = (int)KSl, BO = (int)(KSl + RNl);
+    unsigned* keys = sxs_smem;
+    unsigned* raw = sxs_smem + RO;  // copies, then output boundaries
+    // 1. bulk copies of every leaf's begins and ends (thread 0)
+    if (fits && wid == 0) {
+        // lane q < 2K copies leaf q/2's begins (q even) or ends (q odd)
+        const int q = lane < 2 * K ? lane : 0;
+        const int l = q >> 1;
+        int nl = 0, g0 = 0;
+        const int* arr = nullptr;
+#pragma unroll
+        for (int m = 0; m < K; ++m)
+            if (m == l) {
+                nl = n[m];
+                g0 = S.off[m][0];
+                arr = (q & 1) ? A.leaf[m].end : A.leaf[m].begin;
+            }
+        const int* g = arr + g0;
+        const uintptr_t a0 = (uintptr_t)g & ~(uintptr_t)15;
+        const unsigned len =
+            (lane < 2 * K && nl > 0) ? (unsigned)((((uintptr_t)(g + nl) + 15) & ~(uintptr_t)15) - a0) : 0u;
+        int incl = (int)(len >> 2);
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int words = __shfl_sync(0xFFFFFFFFu, incl, 31);
+        const int pos = incl - (int)(len >> 2);
+        if (lane < 2 * K) {
+            const int first = pos + (int)(((uintptr_t)g & 15) >> 2);
+            if (q & 1) S.rawe[l] = first; else S.rawb[l] = first;
+        }
+        __syncwarp();  // orders the lanes' writes before lane 0's release on the barrier
+        if (lane == 0) sxs_bar_expect(&S.bar, 4u * (unsigned)words);
+        __syncwarp();
+        if (len > 0u) sxs_bulk_copy(raw + pos, (const void*)a0, len, &S.bar);
+    }
+    // 2. per leaf (one warp each): row-start bitmap and rank -> row table
+    //    (offsets only, so it overlaps the copies)
+    if (fits) {
+        int bs = BO;
+#pragma unroll
+        for (int l = 0; l < K; ++l) {
+            const int W = (n[l] + 31) >> 5;
+            if (l % NW == wid && n[l] > 0) {
+                unsigned* bm = sxs_smem + bs;
+                int* wp = (int*)(sxs_smem + bs + W);
+                const int g0 = S.off[l][0];
+                for (int w = lane; w < W; w += 32) bm[w] = 0u;
+                __syncwarp();
+                const bool act = lane < nrows;
+                const int a = act ? S.off[l][lane] - g0 : 0;
+                const int b = act ? S.off[l][lane + 1] - g0 : 0;
+                const bool ne = act && a >= 0 && a < b && b <= n[l];
+                const unsigned bal = __ballot_sync(0xFFFFFFFFu, ne);
+                if (ne) {
+                    S.rowtab[l][__popc(bal & ((1u << lane) - 1u))] = lane;
+                    atomicOr(&bm[a >> 5], 1u << (a & 31));
+                }
+                __syncwarp();
+                int carry = 0;
+                for (int w0 = 0; w0 < W; w0 += 32) {
+                    const int w = w0 + lane;
+                    const int c = w < W ? __popc(bm[w]) : 0;
+                    int incl = c;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+                        if (lane >= o) incl += y;
+                    }
+                    if (w < W) wp[w] = carry + incl - c;
+                    carry += __shfl_sync(0xFFFFFFFFu, incl, 31);
+                }
+            }
+            bs += 2 * W;
+        }
+    }
+    // 3. wait for the copies, then the coordinate span (first begin, last end of every row)
+    bool copied = true;
+    if (fits) copied = sxs_bar_wait(&S.bar);
+    if (fits && copied) {
+#pragma unroll
+        for (int l = 0; l < K; ++l) {
+            if (l % NW == wid && n[l] > 0) {
+                const int g0 = S.off[l][0];
+                const bool act = lane < nrows;
+                const int a = act ? S.off[l][lane] - g0 : 0;
+                const int b = act ? S.off[l][lane + 1] - g0 : 0;
+                int lo = INT_MAX, hi = INT_MIN;
+                if (act && a >= 0 && a < b && b <= n[l]) {
+                    lo = (int)raw[S.rawb[l] + a];
+                    hi = (int)raw[S.rawe[l] + b - 1];
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    lo = min(lo, __shfl_xor_sync(0xFFFFFFFFu, lo, o));
+                    hi = max(hi, __shfl_xor_sync(0xFFFFFFFFu, hi, o));
+                }
+                if (lane == 0) {
+                    atomicMin(&S.xmin, lo);
+                    atomicMax(&S.xmax, hi);
+                }
+            }
+        }
+    }
+    if (__syncthreads_or(!copied)) {
+        copied = false;
+        if (tid == 0) S.flags |= SXF_TIMEOUT;
+    }
+    const int xmin = S.xmin;
+    const bool staged =
+        fits && copied && (E == 0 || (long long)S.xmax - (long long)xmin < (1ll << SXS_XBITS));
+    unsigned bad = 0u;
+    // 4. keys, and the contract checked on the raw coordinates
+    if (staged) {
+        const unsigned le_mask = 0xFFFFFFFFu >> (31 - lane);  // lanes 0..lane
+        int bs = BO;
+#pragma unroll
+        for (int l = 0; l < K; ++l) {
+            const int W = (n[l] + 31) >> 5;
+            const unsigned* bm = sxs_smem + bs;
+            const int* wp = (const int*)(sxs_smem + bs + W);
+            const unsigned* rb = raw + S.rawb[l];
+            const unsigned* re = raw + S.rawe[l];
+            unsigned* kk = keys + ks[l];
+            for (int j = tid; j < n[l]; j += L) {  // j & 31 == lane
+                const int b = (int)rb[j], e = (int)re[j];
+                const unsigned word = bm[j >> 5];
+                const int rank = wp[j >> 5] + __popc(word & le_mask) - 1;  // < 0 only for disordered offsets
+                const unsigned rk = (unsigned)S.rowtab[l][max(rank, 0)] << SXS_XBITS;
+                const bool first = (word >> lane) & 1u;
+                if (!(b < e) || (!first && !((int)re[j - 1] < b)) || rank < 0) bad = 1u;
+                *(uint2*)(kk + 2 * j) =
+                    make_uint2(rk | ((unsigned)(b - xmin) & SXS_XMASK), rk | ((unsigned)(e - xmin) & SXS_XMASK));
+            }
+            if (tid == 0) {
+                kk[2 * n[l]] = SXS_SENTINEL;
+                kk[2 * n[l] + 1] = SXS_SENTINEL;
+            }
+            bs += 2 * W;
+        }
+    }
+    if (__syncthreads_or(bad)) {
+        if (tid == 0) S.flags |= SXF_CONTRACT;
+        bad = 1u;
+    }
+    const bool sweep = staged && !bad && E > 0;
+    unsigned* outk = raw;
+    int count = 0, total = 0, excl = 0, prov = 0;
+    if (sweep) {
+        // 5. this thread's piece [klo, khi) and where it starts in every list
+        const int nb2 = 2 * nbig;
+        unsigned klo = 0u, khi = SXS_SENTINEL;
+        if (tid > 0) klo = keys[ksbig + (int)(((long long)tid * nb2) / L)];
+        if (tid + 1 < L) khi = keys[ksbig + (int)(((long long)(tid + 1) * nb2) / L)];
+        // lists below the pivot's row lie wholly before it, rows above wholly after
+        int pos[K];
+        const int rp = (int)(klo >> SXS_XBITS);
+#pragma unroll
+        for (int l = 0; l < K; ++l) {
+            if (tid == 0) {
+                pos[l] = 0;
+            } else if (l == big) {
+                pos[l] = (int)(((long long)tid * nb2) / L);
+            } else {
+                const int lo = 2 * (S.off[l][rp] - S.off[l][0]);
+                const int hi = 2 * (S.off[l][rp + 1] - S.off[l][0]);
+                pos[l] = lo + sxs_lower_bound(keys + ks[l] + lo, hi - lo, klo);
+            }
+        }
+        unsigned pa[K];
+        unsigned h[K];
+        unsigned state = 0u;
+#pragma unroll
+        for (int l = 0; l < K; ++l) {
+            pa[l] = sxs_saddr(keys + ks[l] + pos[l]);
+            h[l] = keys[ks[l] + pos[l]];
+            state |= (unsigned)(pos[l] & 1) << l;
+            prov += pos[l];
+        }
+        // 6. the sweep: smallest head, toggle every leaf holding it, compare f
+        const unsigned tab0 = S.tab[0];
+        unsigned fprev = sxs_f<K>(S, tab0, state);
+        const unsigned o0 = sxs_saddr(outk + prov), oend = sxs_saddr(outk + E);
+        unsigned oa = o0;
+        while (true) {
+            unsigned c = h[0];
+#pragma unroll
+            for (int l = 1; l < K; ++l) c = min(c, h[l]);
+            if (c >= khi) break;
+#pragma unroll
+            for (int l = 0; l < K; ++l) sxs_advance(h[l], pa[l], state, c, 1u << l);
+            const unsigned f = sxs_f<K>(S, tab0, state);
+            sxs_emit(oa, f, fprev, c);
+            oa = min(oa, oend);
+            fprev = f;
+        }
+        const int o = prov + (int)((oa - o0) >> 2);
+        count = max(0, min(o, E) - prov);
+        excl = sxs_block_excl_sum(count, S.warp, &total);  // `sweep` is uniform over the block
+        total = min(total, E);
+    }
+    // fallback tile: one lane per row over global memory
+    int lane_count = 0;
+    int s_row[K], lim_row[K];
+    if (!staged && wid == 0) {
+        const bool act = lane < nrows;
+#pragma unroll
+        for (int l = 0; l < K; ++l) {
+            const int a = act ? S.off[l][lane] : 0;
+            const int b = act ? S.off[l][lane + 1] : 0;
+            s_row[l] = a;
+            lim_row[l] = 2 * (b - a);
+        }
+        bool fb_bad = false, fb_over = false;
+        if (act) lane_count = sx_sweep_table<K, false>(A, s_row, lim_row, nullptr, nullptr, 0, fb_bad, fb_over);
+        if (__any_sync(0xFFFFFFFFu, fb_bad) && lane == 0) S.flags |= SXF_CONTRACT;
+        int tot = lane_count;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xFFFFFFFFu, tot, o);
+        total = 2 * tot;
+    }
+    // 7. look-back for the tile's base (warp 0); meanwhile every thread packs
+    //    its output boundaries from the output area into the key area
+    if (wid == 0) {
+        unsigned f = S.flags;
+        const int base = sxs_lookback(st, tile, total >> 1, f);
+        if (lane == 0) {
+            S.base = base;
+            S.flags = f;
+        }
+    }
+    if (sweep) {
+        const int m = min(count, E - excl);
+        for (int i = 0; i < m; ++i) keys[excl + i] = outk[prov + i];
+    }
+    __syncthreads();
+    const int base = S.base;
+    bool over = false;
+    if (staged) {
+        // 8. coalesced output and the tile's row offsets
+        const int nint = total >> 1;
+        for (int i = tid; i < nint; i += L) {
+            const uint2 kv = *(const uint2*)(keys + 2 * i);
+            const long long o = (long long)base + i;
+            if (o < A.capacity) {
+                A.out_begin[o] = xmin + (int)(kv.x & SXS_XMASK);
+                A.out_end[o] = xmin + (int)(kv.y & SXS_XMASK);
+            } else {
+                over = true;
+            }
+        }
+        for (int r = tid; r < nrows; r += L) {
+            const int pos = sxs_lower_bound(keys, total, (unsigned)(r + 1) << SXS_XBITS);
+            A.out_off[r0 + r + 1] = base + (pos >> 1);
+        }
+        if (tile == 0 && tid == 0) A.out_off[0] = 0;
+    } else if (wid == 0) {
+        int incl = lane_count;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane < nrows) {
+            bool fb_bad = false;
+            if (lane_count > 0)
+                sx_sweep_table<K, true>(A, s_row, lim_row, A.out_begin, A.out_end, (long long)base + incl - lane_count,
+                                        fb_bad, over);
+            A.out_off[r0 + lane + 1] = base + incl;
+        }
+        if (tile == 0 && lane == 0) A.out_off[0] = 0;
+    }
+    (void)over;  // an output beyond the capacity shows in the reported total
+    if (wid == 0) sxs_report(A, tile, tiles, base, total >> 1, S.flags);
+}
+
+// ---------------------------------------------------------------------------
+// Warp-tile segmented sweep.
+//
+// The same algorithm as the block kernel above, with one warp per tile of
+// `tr` rows (at most 32) and no block-wide barrier: each warp takes its own
+// tile ticket, has its own slice of shared memory and its own mbarrier, and
+// runs its own look-back.  A block holds several independent warps.  Small
+// tiles and independent warps keep many tiles in flight per SM, so one
+// warp's waits (copies, look-back) are covered by the others' sweeps.
+//
+// The row of each staged interval is found by walking the tile's row ends
+// (a lane starts from the row of the previous chunk's last interval), which
+// needs no bitmap.
+// ---------------------------------------------------------------------------
+
+// Per-warp header at the start of the warp's slice, in 32-bit words:
+// [0, 2) mbarrier, then the tile's row offsets (tr + 1 per leaf), then the
+// begin and end copy positions (K each).
+__host__ __device__ inline int sxw_hdr_words(int k, int tr) { return (2 + (tr + 1) * k + 2 * k + 3) & ~3; }
+__host__ __device__ inline size_t sxw_slice_bytes(int k, int tr, int cap_words)
+{
+    return 4u * (size_t)(sxw_hdr_words(k, tr) + ((cap_words + 3) & ~3));
+}
+
+template <int K>
+__global__ void __launch_bounds__(256) sx_wseg_kernel(SxBoolArgs A, SxSweepState st, int tiles, int cap_words, int tr)
+{
+    extern __shared__ __align__(16) unsigned char sxw_smem[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, NW = blockDim.x >> 5;
+    if (blockIdx.x * NW + wid >= tiles) return;  // exactly `tiles` warps take tickets
+    unsigned* base_w = (unsigned*)(sxw_smem + (size_t)wid * sxw_slice_bytes(K, tr, cap_words));
+    unsigned long long* bar = (unsigned long long*)base_w;
+    const int os = tr + 1;                // row offsets of leaf l: off[l * os + r], r in [0, nrows]
+    int* off = (int*)base_w + 2;
+    int* rawb = off + os * K;             // [K]
+    int* rawe = rawb + K;                 // [K]
+    unsigned* Wd = base_w + sxw_hdr_words(K, tr);
+
+    int tile = 0;
+    if (lane == 0) {
+        tile = (int)atomicAdd(&st.counters[0], 1u);
+        sxs_bar_init(bar);
+    }
+    tile = __shfl_sync(0xFFFFFFFFu, tile, 0);
+    const int r0 = tile * tr;
+    const int nrows = min(tr, A.rows - r0);
+    for (int r = lane; r <= nrows; r += 32) {
+#pragma unroll
+        for (int l = 0; l < K; ++l) off[l * os + r] = A.leaf[l].off[r0 + r];
+    }
+    __syncwarp();
+    // layout (words): copies, later output boundaries, [0, RN); key lists [RN, RN + KS)
+    int n[K], ks[K];
+    long long KSl = 0, El = 0, RNl = 0;
+    int big = 0, nbig = -1, ksbig = 0;
+    bool ok = true;
+#pragma unroll
+    for (int l = 0; l < K; ++l) {
+        n[l] = off[l * os + nrows] - off[l * os];
+        ok = ok && n[l] >= 0;
+        RNl += 2ll * ((n[l] + 11) & ~3);  // two copies of at most n + 6 words, 16-byte aligned
+        El += 2ll * n[l];
+    }
+    if (RNl < El + 1) RNl = El + 1;
+    RNl = (RNl + 3) & ~3ll;
+#pragma unroll
+    for (int l = 0; l < K; ++l) {
+        ks[l] = (int)(RNl + KSl);
+        if (n[l] > nbig) {
+            big = l;
+            nbig = n[l];
+            ksbig = ks[l];
+        }
+        KSl += 2ll * n[l] + 2;
+    }
+    const bool fits = ok && RNl + KSl <= (long long)cap_words;
+    const int E = fits ? (int)El : 0;
+    unsigned* raw = Wd;  // copies, then output boundaries
+    unsigned* keys = Wd;  // key lists at absolute word positions ks[l]
+    // 1. bulk copies: lane q < 2K copies leaf q/2's begins (q even) or ends (q odd)
+    if (fits) {
+        const int q = lane < 2 * K ? lane : 0;
+        const int l = q >> 1;
+        int nl = 0, g0 = 0;
+        const int* arr = nullptr;
+#pragma unroll
+        for (int m = 0; m < K; ++m)
+            if (m == l) {
+                nl = n[m];
+                g0 = off[m * os];
+                arr = (q & 1) ? A.leaf[m].end : A.leaf[m].begin;
+            }
+        const int* g = arr + g0;
+        const uintptr_t a0 = (uintptr_t)g & ~(uintptr_t)15;
+        const unsigned len =
+            (lane < 2 * K && nl > 0) ? (unsigned)((((uintptr_t)(g + nl) + 15) & ~(uintptr_t)15) - a0) : 0u;
+        int incl = (int)(len >> 2);
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int words = __shfl_sync(0xFFFFFFFFu, incl, 31);
+        const int pos = incl - (int)(len >> 2);
+        if (lane < 2 * K) {
+            const int first = pos + (int)(((uintptr_t)g & 15) >> 2);
+            if (q & 1) rawe[l] = first; else rawb[l] = first;
+        }
+        __syncwarp();  // orders the lanes' writes before lane 0's release on the barrier
+        if (lane == 0) sxs_bar_expect(bar, 4u * (unsigned)words);
+        __syncwarp();
+        if (len > 0u) sxs_bulk_copy(raw + pos, (const void*)a0, len, bar);
+    }
+    bool copied = true;
+    if (fits) copied = __all_sync(0xFFFFFFFFu, sxs_bar_wait(bar));
+    unsigned flags = (fits && !copied) ? SXF_TIMEOUT : 0u;
+    // 2. coordinate span: first begin and last end of every leaf row
+    int xmin = INT_MAX, xmax = INT_MIN;
+    if (fits && copied) {
+        if (lane < nrows) {
+#pragma unroll
+            for (int l = 0; l < K; ++l) {
+                const int a = off[l * os + lane] - off[l * os], b = off[l * os + lane + 1] - off[l * os];
+                if (a >= 0 && a < b && b <= n[l]) {
+                    xmin = min(xmin, (int)raw[rawb[l] + a]);
+                    xmax = max(xmax, (int)raw[rawe[l] + b - 1]);
+                }
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            xmin = min(xmin, __shfl_xor_sync(0xFFFFFFFFu, xmin, o));
+            xmax = max(xmax, __shfl_xor_sync(0xFFFFFFFFu, xmax, o));
+        }
+    }
+    const bool staged = fits && copied && (E == 0 || (long long)xmax - (long long)xmin < (1ll << SXS_XBITS));
+    bool bad = false;
+    // 3. keys: the row of interval j is found by walking the row ends from
+    //    the previous chunk's row; the contract is checked on the raw values
+    if (staged) {
+#pragma unroll
+        for (int l = 0; l < K; ++l) {
+            const int* o = off + l * os;
+            const int g0 = o[0];
+            const unsigned* rb = raw + rawb[l];
+            const unsigned* re = raw + rawe[l];
+            unsigned* kk = keys + ks[l];
+            int rc = 0;
+            for (int j0 = 0; j0 < n[l]; j0 += 32) {
+                const int j = j0 + lane;
+                int r = rc;
+                if (j < n[l]) {
+                    while (r + 1 < nrows && o[r + 1] - g0 <= j) ++r;
+                    const int b = (int)rb[j], e = (int)re[j];
+                    const bool first = j == o[r] - g0;
+                    if (!(b < e) || (!first && !((int)re[j - 1] < b)) || o[r] - g0 > j) bad = true;
+                    const unsigned rk = (unsigned)r << SXS_XBITS;
+                    *(uint2*)(kk + 2 * j) =
+                        make_uint2(rk | ((unsigned)(b - xmin) & SXS_XMASK), rk | ((unsigned)(e - xmin) & SXS_XMASK));
+                }
+                rc = __shfl_sync(0xFFFFFFFFu, r, 31);
+            }
+            if (lane == 0) {
+                kk[2 * n[l]] = SXS_SENTINEL;
+                kk[2 * n[l] + 1] = SXS_SENTINEL;
+            }
+        }
+    }
+    bad = __any_sync(0xFFFFFFFFu, bad);
+    __syncwarp();
+    if (bad) flags |= SXF_CONTRACT;
+    const bool sweep = staged && !bad && E > 0;
+    unsigned* outk = raw;
+    int count = 0, total = 0, excl = 0, prov = 0;
+    if (sweep) {
+        // 4. this lane's piece [klo, khi) and where it starts in every list
+        const int nb2 = 2 * nbig;
+        unsigned klo = 0u, khi = SXS_SENTINEL;
+        if (lane > 0) klo = keys[ksbig + (lane * nb2) / 32];
+        if (lane < 31) khi = keys[ksbig + ((lane + 1) * nb2) / 32];
+        const int rp = (int)(klo >> SXS_XBITS);
+        int pos[K];
+#pragma unroll
+        for (int l = 0; l < K; ++l) {
+            if (lane == 0) {
+                pos[l] = 0;
+            } else if (l == big) {
+                pos[l] = (lane * nb2) / 32;
+            } else {
+                const int lo = 2 * (off[l * os + rp] - off[l * os]);
+                const int hi = 2 * (off[l * os + rp + 1] - off[l * os]);
+                pos[l] = lo + sxs_lower_bound(keys + ks[l] + lo, hi - lo, klo);
+            }
+        }
+        unsigned pa[K];
+        unsigned h[K];
+        unsigned state = 0u;
+#pragma unroll
+        for (int l = 0; l < K; ++l) {
+            pa[l] = sxs_saddr(keys + ks[l] + pos[l]);
+            h[l] = keys[ks[l] + pos[l]];
+            state |= (unsigned)(pos[l] & 1) << l;
+            prov += pos[l];
+        }
+        // 5. the sweep
+        const unsigned tab0 = A.table[0];
+        unsigned fprev = K <= 5 ? (tab0 >> state) & 1u : (A.table[state >> 5] >> (state & 31u)) & 1u;
+        const unsigned o0 = sxs_saddr(outk + prov), oend = sxs_saddr(outk + E);
+        unsigned oa = o0;
+        while (true) {
+            unsigned c = h[0];
+#pragma unroll
+            for (int l = 1; l < K; ++l) c = min(c, h[l]);
+            if (c >= khi) break;
+#pragma unroll
+            for (int l = 0; l < K; ++l) sxs_advance(h[l], pa[l], state, c, 1u << l);
+            const unsigned f = K <= 5 ? (tab0 >> state) & 1u : (A.table[state >> 5] >> (state & 31u)) & 1u;
+            sxs_emit(oa, f, fprev, c);
+            oa = min(oa, oend);
+            fprev = f;
+        }
+        count = (int)((oa - o0) >> 2);
+        int incl = count;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        excl = incl - count;
+        total = min(__shfl_sync(0xFFFFFFFFu, incl, 31), E);
+    }
+    // fallback tile: one lane per row over global memory
+    int lane_count = 0;
+    int s_row[K], lim_row[K];
+    if (!staged) {
+        const bool act = lane < nrows;
+#pragma unroll
+        for (int l = 0; l < K; ++l) {
+            const int a = act ? off[l * os + lane] : 0;
+            const int b = act ? off[l * os + lane + 1] : 0;
+            s_row[l] = a;
+            lim_row[l] = 2 * (b - a);
+        }
+        bool fb_bad = false, fb_over = false;
+        if (act) lane_count = sx_sweep_table<K, false>(A, s_row, lim_row, nullptr, nullptr, 0, fb_bad, fb_over);
+        if (__any_sync(0xFFFFFFFFu, fb_bad)) flags |= SXF_CONTRACT;
+        int tot = lane_count;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xFFFFFFFFu, tot, o);
+        total = 2 * tot;
+    }
+    // 6. look-back, then pack the output boundaries into the key area
+    const int base = sxs_lookback(st, tile, total >> 1, flags);
+    bool over = false;
+    if (staged) {
+        unsigned* packed = Wd + (int)RNl;  // the key lists are dead after the sweep
+        __syncwarp();
+        if (sweep) {
+            const int m = min(count, E - excl);
+            for (int i = 0; i < m; ++i) packed[excl + i] = outk[prov + i];
+        }
+        __syncwarp();
+        // 7. coalesced output and the tile's row offsets
+        const int nint = total >> 1;
+        for (int i = lane; i < nint; i += 32) {
+            const uint2 kv = *(const uint2*)(packed + 2 * i);
+            const long long o = (long long)base + i;
+            if (o < A.capacity) {
+                A.out_begin[o] = xmin + (int)(kv.x & SXS_XMASK);
+                A.out_end[o] = xmin + (int)(kv.y & SXS_XMASK);
+            } else {
+                over = true;
+            }
+        }
+        for (int r = lane; r < nrows; r += 32) {
+            const int pos = sxs_lower_bound(packed, total, (unsigned)(r + 1) << SXS_XBITS);
+            A.out_off[r0 + r + 1] = base + (pos >> 1);
+        }
+        if (tile == 0 && lane == 0) A.out_off[0] = 0;
+    } else {
+        int incl = lane_count;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane < nrows) {
+            bool fb_bad = false;
+            if (lane_count > 0)
+                sx_sweep_table<K, true>(A, s_row, lim_row, A.out_begin, A.out_end, (long long)base + incl - lane_count,
+                                        fb_bad, over);
+            A.out_off[r0 + lane + 1] = base + incl;
+        }
+        if (tile == 0 && lane == 0) A.out_off[0] = 0;
+    }
+    (void)over;  // an output beyond the capacity shows in the reported total
+    sxs_report(A, tile, tiles, base, total >> 1, flags);
+}
+
 size_t sx_sweep_state_bytes(long long tiles)
 {
     const long long groups = (tiles + SX_GROUP - 1) / SX_GROUP;
@@ -1154,6 +2013,58 @@ static cudaError_t sx_merge_launch_k(const SxBoolArgs& A, const SxSweepState& st
     return cudaGetLastError();
 }
 
+template <int K>
+static cudaError_t sx_seg_launch_k(const SxBoolArgs& A, const SxSweepState& st, int tiles, int cap_keys, int threads,
+                                   int tr, cudaStream_t stream)
+{
+    static int configured = 0;  // largest dynamic shared memory set for this instantiation
+    const int bytes = 4 * cap_keys;
+    if (bytes > configured) {
+        cudaError_t err = cudaFuncSetAttribute(sx_seg_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        if (err != cudaSuccess) return err;
+        configured = bytes;
+    }
+    sx_seg_kernel<K><<<tiles, threads, bytes, stream>>>(A, st, tiles, cap_keys, tr);
+    return cudaGetLastError();
+}
+
+template <int K>
+static cudaError_t sx_wseg_launch_k(const SxBoolArgs& A, const SxSweepState& st, int tiles, int cap_words, int warps,
+                                    int tr, cudaStream_t stream)
+{
+    static int configured = 0;  // largest dynamic shared memory set for this instantiation
+    const int bytes = warps * (int)sxw_slice_bytes(K, tr, cap_words);
+    if (bytes > configured) {
+        cudaError_t err = cudaFuncSetAttribute(sx_wseg_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        if (err != cudaSuccess) return err;
+        configured = bytes;
+    }
+    const int blocks = (tiles + warps - 1) / warps;
+    sx_wseg_kernel<K><<<blocks, 32 * warps, bytes, stream>>>(A, st, tiles, cap_words, tr);
+    return cudaGetLastError();
+}
+
+// Segmented sweep shape: `keys` boundaries per tile (0: 1.25x the average
+// plus slack), stored twice (lists and output area), at most 200 KiB per
+// block; `warps` per block (0: about 48 boundaries per thread).
+static void sx_seg_shape(long long leaf_intervals, long long tiles, int keys, int warps, int k, int* cap_keys,
+                         int* threads)
+{
+    const long long avg = tiles > 0 ? (2 * leaf_intervals + tiles - 1) / tiles : 0;
+    long long e = keys > 0 ? keys : avg + avg / 4 + 256;
+    long long c = 2 * e + e / 32 + 26 * k + 64;
+    c = (c + 255) / 256 * 256;
+    if (c > 51200) c = 51200;
+    *cap_keys = (int)c;
+    int w = warps;
+    if (w <= 0) {
+        w = (int)((avg + 1535) / 1536);
+        if (w < 1) w = 1;
+    }
+    if (w > SXS_MAX_THREADS / 32) w = SXS_MAX_THREADS / 32;
+    *threads = 32 * w;
+}
+
 // Shared memory per tile: two (or three) key buffers of 32-bit keys with
 // room for 1.25x the average tile plus slack, in steps of 2 KiB, between
 // 8 KiB and 96 KiB.  `requested` (keys) overrides the average.
@@ -1173,10 +2084,20 @@ static int sx_merge_cap(long long leaf_intervals, long long tiles, int requested
     return (int)bytes;
 }
 
-cudaError_t sx_sweep_launch(const SxBoolArgs& A, bool union_mode, void* workspace, cudaStream_t stream)
+cudaError_t sx_sweep_launch(const SxBoolArgs& A, bool union_mode, void* workspace, size_t workspace_bytes,
+                            cudaStream_t stream)
 {
-    const long long tiles = sx_sweep_tiles(A.rows);
-    if (tiles <= 0) return cudaSuccess;
+    if (A.rows <= 0) return cudaSuccess;
+    // The segmented sweep takes tiles of 16 rows when the workspace holds
+    // their look-back state (smaller tiles keep more blocks resident), else 32.
+    const bool seg = !union_mode && (A.tune_kernel == 0 || A.tune_kernel == 4 || A.tune_kernel == 5);
+    int tr = 32;
+    if (seg) {
+        tr = A.tune_tile_rows > 0 ? A.tune_tile_rows : (A.tune_kernel == 4 ? 32 : 8);
+        if (sx_sweep_state_bytes(((long long)A.rows + tr - 1) / tr) > workspace_bytes) tr = 32;
+    }
+    const long long tiles = ((long long)A.rows + tr - 1) / tr;
+    if (sx_sweep_state_bytes(tiles) > workspace_bytes) return cudaErrorInvalidValue;
     // The look-back state must start cleared; the workspace may hold other scratch.
     cudaError_t err = cudaMemsetAsync(workspace, 0, sx_sweep_state_bytes(tiles), stream);
     if (err != cudaSuccess) return err;
@@ -1200,7 +2121,48 @@ cudaError_t sx_sweep_launch(const SxBoolArgs& A, bool union_mode, void* workspac
     // resident), global sweep with a residency cap of 3 blocks per SM for
     // heavy tiles (measured best on the 4096x4096 shape expression).
     SxBoolArgs B = A;
-    if (B.tune_kernel == 0) B.tune_kernel = 3;
+    if (B.tune_kernel == 0) B.tune_kernel = 5;
+    if (B.tune_kernel == 5) {
+        // words per warp: the copies (or outputs) and the key lists of the largest tile
+        const long long avg = (2 * A.capacity + tiles - 1) / tiles;
+        long long e = A.tune_staging_cap > 0 ? A.tune_staging_cap : avg + avg / 4 + 64;
+        long long words = 2 * e + 26 * A.k + 16;
+        // four warps per block unless a slice that large allows fewer (200 KiB per block)
+        const long long room = (200 * 1024) / 4 - sxw_hdr_words(A.k, tr);
+        int warps = A.tune_warps > 0 ? A.tune_warps : (int)(room / (words + sxw_hdr_words(A.k, tr)));
+        if (warps > 4 && A.tune_warps <= 0) warps = 4;
+        if (warps < 1) warps = 1;
+        B.tune_kernel = 5;
+        const long long limit = (200 * 1024) / warps / 4 - sxw_hdr_words(A.k, tr);
+        if (words > limit) words = limit;
+        const int cw = (int)words;
+        switch (A.k) {
+            case 1: return sx_wseg_launch_k<1>(A, st, t, cw, warps, tr, stream);
+            case 2: return sx_wseg_launch_k<2>(A, st, t, cw, warps, tr, stream);
+            case 3: return sx_wseg_launch_k<3>(A, st, t, cw, warps, tr, stream);
+            case 4: return sx_wseg_launch_k<4>(A, st, t, cw, warps, tr, stream);
+            case 5: return sx_wseg_launch_k<5>(A, st, t, cw, warps, tr, stream);
+            case 6: return sx_wseg_launch_k<6>(A, st, t, cw, warps, tr, stream);
+            case 7: return sx_wseg_launch_k<7>(A, st, t, cw, warps, tr, stream);
+            case 8: return sx_wseg_launch_k<8>(A, st, t, cw, warps, tr, stream);
+            default: return cudaErrorInvalidValue;
+        }
+    }
+    if (B.tune_kernel == 4) {
+        int cap = 0, threads = 0;
+        sx_seg_shape(A.capacity, tiles, A.tune_staging_cap, A.tune_warps, A.k, &cap, &threads);
+        switch (A.k) {
+            case 1: return sx_seg_launch_k<1>(A, st, t, cap, threads, tr, stream);
+            case 2: return sx_seg_launch_k<2>(A, st, t, cap, threads, tr, stream);
+            case 3: return sx_seg_launch_k<3>(A, st, t, cap, threads, tr, stream);
+            case 4: return sx_seg_launch_k<4>(A, st, t, cap, threads, tr, stream);
+            case 5: return sx_seg_launch_k<5>(A, st, t, cap, threads, tr, stream);
+            case 6: return sx_seg_launch_k<6>(A, st, t, cap, threads, tr, stream);
+            case 7: return sx_seg_launch_k<7>(A, st, t, cap, threads, tr, stream);
+            case 8: return sx_seg_launch_k<8>(A, st, t, cap, threads, tr, stream);
+            default: return cudaErrorInvalidValue;
+        }
+    }
     if (B.tune_kernel == 3) {
         const int nbuf = (A.k == 3 || A.k == 6 || A.k == 7) ? 3 : 2;
         const int cap = sx_merge_cap(A.capacity, tiles, A.tune_staging_cap, nbuf);

@@ -243,7 +243,11 @@ def test_wide_coordinate_span_vs_oracle(cuda_device):
 
 
 @pytest.mark.parametrize("tuning", [{"kernel": 1}, {"kernel": 1, "blocks_per_sm": 6}, {"kernel": 2},
-                                    {"kernel": 3, "staging_cap": 256}, {"kernel": 3, "staging_cap": 12000}])
+                                    {"kernel": 3, "staging_cap": 256}, {"kernel": 3, "staging_cap": 12000},
+                                    {"kernel": 4, "staging_cap": 256}, {"kernel": 4, "warps": 1},
+                                    {"kernel": 4, "warps": 8}, {"kernel": 4, "staging_cap": 20000, "warps": 3},
+                                    {"kernel": 4, "tile_rows": 16}, {"kernel": 5}, {"kernel": 5, "tile_rows": 32},
+                                    {"kernel": 5, "tile_rows": 1, "warps": 1}, {"kernel": 5, "staging_cap": 64}])
 def test_tuning_never_changes_results(cuda_device, tuning):
     from subsetix_b200 import _core
 
@@ -259,3 +263,24 @@ def test_tuning_never_changes_results(cuda_device, tuning):
         _core.TUNING.clear()
         _core.TUNING.update(saved)
     assert_same(got, O.evaluate(EXPRS["e0"], leaves_h), str(tuning))
+
+
+def test_tile_boundaries_max(cuda_device):
+    from subsetix_b200 import _core
+
+    rng = np.random.default_rng(21)
+    rows = 1003
+    leaves = []
+    host = []
+    for _ in range(3):
+        off = np.concatenate([[0], np.cumsum(rng.integers(0, 40, rows))]).astype(np.int32)
+        host.append(off)
+        t = torch.as_tensor(off, device="cuda")
+        leaves.append((t, t, t, 0))
+    for a, b in ((8, 32), (1, 7), (16, 1000), (5, 2000)):
+        got = _core.max_tile_boundaries(leaves, rows, torch.device("cuda", 0), tile_rows=(a, b))
+        want = []
+        for tr in (a, b):
+            edges = np.minimum(np.arange(0, rows + tr, tr), rows)
+            want.append(2 * int(max(sum(o[edges[1:]] - o[edges[:-1]] for o in host).max(), 0)))
+        assert got == want, (a, b)
