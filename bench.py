@@ -497,15 +497,16 @@ def main():
     res_buf = torch.empty(2, dtype=torch.int32, device=device)
     off_buf = torch.empty(R + 1, dtype=torch.int32, device=device)
 
-    def step():
-        return _core.bool_eval_async(specs, R, table, _lib.MODE_TABLE, device, out=(ob, oe), result=res_buf,
-                                     offsets=off_buf)
-
     tuning = {}
     if not args.no_autotune:
         from subsetix_b200 import autotune
 
         tuning = autotune.tune_bool_eval(specs, R, table, device)
+    launch_tuning = {k: v for k, v in tuning.items() if k not in ("ms", "key")} or None
+
+    def step():
+        return _core.bool_eval_async(specs, R, table, _lib.MODE_TABLE, device, out=(ob, oe), result=res_buf,
+                                     offsets=off_buf, tuning=launch_tuning)
 
     # correctness guard + output size for the roofline bytes
     _, _, ooff, result = step()

@@ -21,9 +21,22 @@ I32 = torch.int32
 
 OP_UNION, OP_INTERSECTION, OP_DIFFERENCE = 0, 1, 2
 
-# Launch tuning for the row sweep (sx_tuning).  Empty means automatic.  The
-# autotuner (subsetix_b200/autotune.py) fills it per workload.
+# Launch tuning for the row sweep (sx_tuning).  TUNING, when not empty,
+# applies to every evaluation.  TUNED maps a workload key (workload_key) to
+# the launch shape the autotuner (subsetix_b200/autotune.py) found fastest for
+# that kind of workload; buffer sizes are still taken from each evaluation's
+# own largest tile.  Neither ever changes results.
 TUNING: dict = {}
+TUNED: dict = {}
+
+
+def workload_key(sizes: Sequence[int], rows: int) -> str:
+    """Bucket of a set-algebra workload: leaf count, log2 rows, log2 mean boundaries per 32-row tile."""
+    import math
+
+    tiles = max(1, (int(rows) + 31) // 32)
+    per_tile = 2 * sum(int(s) for s in sizes) / tiles
+    return f"k{len(sizes)}-r{int(math.log2(max(rows, 1)))}-t{int(math.log2(max(per_tile, 1.0)))}"
 
 
 def empty_i32(n: int, device) -> torch.Tensor:
@@ -69,7 +82,13 @@ def bool_eval(leaves: Sequence[Tuple[torch.Tensor, torch.Tensor, torch.Tensor, i
     buffers to be sliced to ``total``.
     """
     tuning = None
-    if mode == _lib.MODE_TABLE and not TUNING and rows > 0:
+    tuned = TUNED.get(workload_key([int(leaf[0].numel()) for leaf in leaves], rows)) if TUNED else None
+    if mode == _lib.MODE_TABLE and not TUNING and rows > 0 and tuned is not None:
+        tuning = dict(tuned)
+        if tuning.get("kernel") in (3, 4, 5):
+            tr = int(tuning.get("tile_rows", 0)) or (8 if tuning["kernel"] == 5 else 32)
+            tuning["staging_cap"] = min(max_tile_boundaries(leaves, rows, device, tile_rows=tr), 25000)
+    elif mode == _lib.MODE_TABLE and not TUNING and rows > 0:
         # Even rows: 8-row warp tiles with buffers sized for the largest tile
         # (no tile leaves the staged sweep, no buffer larger than needed).
         # Skewed rows (the largest 8-row tile far above the mean): 32-row

@@ -7,8 +7,10 @@ kernel with two key capacities per tile, and the one-lane-per-row sweep
 with several residency caps.  Each candidate is timed with CUDA events on the
 caller's workload; the fastest is cached under a key of the workload's
 shape (leaf count, row count, mean boundaries per 32-row tile, bucketed by
-powers of two) and installed in ``_core.TUNING`` so later evaluations use
-it.  Results never depend on the tuning; only speed does.
+powers of two) and installed in ``_core.TUNED`` under that key, so later
+evaluations of that kind of workload use its kernel and block shape (with
+buffers sized for their own largest tile).  Results never depend on the
+tuning; only speed does.
 """
 
 from __future__ import annotations
@@ -25,11 +27,7 @@ from . import _core, _lib
 _CACHE: Dict[str, dict] = {}
 
 
-def workload_key(sizes: Sequence[int], rows: int) -> str:
-    k = len(sizes)
-    tiles = max(1, (int(rows) + 31) // 32)
-    per_tile = 2 * sum(int(s) for s in sizes) / tiles
-    return f"k{k}-r{int(math.log2(max(rows, 1)))}-t{int(math.log2(max(per_tile, 1.0)))}"
+workload_key = _core.workload_key
 
 
 def candidates(sizes: Sequence[int], rows: int, largest_tile: int = 0, largest_eighth_tile: int = 0) -> List[dict]:
@@ -92,8 +90,7 @@ def tune_bool_eval(leaves, rows: int, table: Sequence[int], device, *, mode: int
             with open(cache_path, "w") as f:
                 json.dump(data, f, indent=1, sort_keys=True)
     if install:
-        _core.TUNING.clear()
-        _core.TUNING.update({k: v for k, v in best.items() if k in ("kernel", "blocks_per_sm", "staging_cap", "warps", "tile_rows")})
+        _core.TUNED[key] = {k: v for k, v in best.items() if k in ("kernel", "blocks_per_sm", "warps", "tile_rows")}
     return best
 
 
