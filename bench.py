@@ -151,7 +151,7 @@ def peak_hbm():
 
 # sx_tuning kernel kinds (0 = automatic, the warp-tile segmented sweep)
 KERNELS = {1: "sx_sweep_kernel<5,0>", 2: "sx_sweep_smem_kernel<5>", 3: "sx_merge_kernel<5>", 4: "sx_seg_kernel<5>",
-           5: "sx_wseg_kernel<5>"}
+           5: "sx_wseg_kernel<5>", 6: "sx_wseg16_kernel<5>"}
 
 
 def traffic_per_launch(copies: int, kernel: str = "sx_wseg_kernel<5>"):

@@ -92,11 +92,14 @@ typedef struct sx_leaf {
 
 /* Launch tuning for sx_bool_eval; NULL or zero fields select automatic values.
  * kernel: 1 = global-memory sweep, 2 = shared-memory staged sweep, 3 =
- * merge-path tile kernel, 4 = segmented sweep (table mode; the default);
+ * merge-path tile kernel, 4 = segmented sweep in block tiles, 5 = segmented
+ * sweep in warp tiles (table mode; the default), 6 = kernel 5 with 16-bit
+ * keys (tiles of at most 8 rows; wider-spanning tiles take the row sweep);
  * blocks_per_sm: residency cap of the global sweep; staging_cap: elements per
- * warp of the staged sweep, or boundaries per tile of kernels 3 and 4;
- * warps: warps per tile of kernel 4; tile_rows: rows per tile of kernel 4
- * (16 or 32).  Results never depend on the tuning. */
+ * warp of the staged sweep, or boundaries per tile of kernels 3 to 6; warps:
+ * warps per block of kernels 4 to 6 (in 5 and 6 each warp owns a tile);
+ * tile_rows: rows per tile of kernels 4 to 6 (at most 32, at most 8 for 6).
+ * Results never depend on the tuning. */
 typedef struct sx_tuning {
     int32_t kernel;
     int32_t blocks_per_sm;
@@ -116,11 +119,15 @@ int sx_bool_eval(const sx_leaf* leaves /* host array of k */, int k, int32_t row
 
 /* Largest number of leaf boundaries (2 x intervals, summed over the leaves)
  * in one tile of tile_rows_a aligned rows (out[0]) and of tile_rows_b aligned
- * rows (out[1]), asynchronously on `stream`.  The leaves' row_offsets are
- * aligned (rows + 1 entries each); the other sx_leaf fields are ignored.
- * Callers size sx_tuning.staging_cap with it.  No reference counterpart. */
+ * rows (out[1]), and the largest coordinate span of a tile_rows_a-row tile
+ * (out[2]: last end minus first begin over its rows), asynchronously on
+ * `stream`.  The leaves' row_offsets are aligned (rows + 1 entries each);
+ * begin and end may be NULL for a leaf without intervals; widen, scale and
+ * row_ends are ignored.  Callers size sx_tuning.staging_cap
+ * with it, and take the 16-bit-key kernel (6) where the span is at most 8190.
+ * No reference counterpart. */
 int sx_tile_boundaries_max(const sx_leaf* leaves /* host array of k */, int k, int32_t rows, int32_t tile_rows_a,
-                           int32_t tile_rows_b, int32_t* out /* device, 2 */, void* stream);
+                           int32_t tile_rows_b, int32_t* out /* device, 3 */, void* stream);
 
 /* ---------------------------------------------------------------------------
  * sx_bool_eval without a caller workspace.  This entry point has no

@@ -43,25 +43,35 @@ def empty_i32(n: int, device) -> torch.Tensor:
     return torch.empty(max(int(n), 0), dtype=I32, device=device)
 
 
+def tile_stats(leaves, rows: int, device, tile_rows_a: int = 8, tile_rows_b: int = 32):
+    """``(largest a-row tile, largest b-row tile, largest a-row tile span)`` in boundaries and coordinates.
+
+    One launch of ``sx_tile_boundaries_max`` and one read-back.
+    """
+    if rows <= 0 or any(len(leaf) > 5 and leaf[5] is not None for leaf in leaves):
+        return 0, 0, 0  # no rows, or explicit row ranges (the union sweep has no tiles)
+    lib = _lib.load()
+    arr = (_lib.SxLeaf * len(leaves))()
+    for i, leaf in enumerate(leaves):
+        arr[i].begin = ptr(leaf[0])
+        arr[i].end = ptr(leaf[1])
+        arr[i].row_offsets = ptr(leaf[2])
+    out = empty_i32(3, device)
+    _lib.check(lib.sx_tile_boundaries_max(arr, len(leaves), int(rows), int(tile_rows_a), int(tile_rows_b), ptr(out),
+                                          stream_handle(device)), "sx_tile_boundaries_max")
+    a, b, span = (int(x) for x in out.tolist())
+    return a, b, span
+
+
 def max_tile_boundaries(leaves, rows: int, device, tile_rows=32):
     """Largest number of leaf boundaries in one tile of ``tile_rows`` aligned rows (one synchronisation).
 
     ``tile_rows`` may be a pair of tile heights; the result is then a list
     with one maximum per height, from the same launch and read-back.
     """
-    many = isinstance(tile_rows, (tuple, list))
-    heights = list(tile_rows) if many else [tile_rows, tile_rows]
-    if rows <= 0 or any(len(leaf) > 5 and leaf[5] is not None for leaf in leaves):
-        return [0, 0] if many else 0  # no rows, or explicit row ranges (the union sweep has no tiles)
-    lib = _lib.load()
-    arr = (_lib.SxLeaf * len(leaves))()
-    for i, leaf in enumerate(leaves):
-        arr[i].row_offsets = ptr(leaf[2])
-    out = empty_i32(2, device)
-    _lib.check(lib.sx_tile_boundaries_max(arr, len(leaves), int(rows), int(heights[0]), int(heights[1]), ptr(out),
-                                          stream_handle(device)), "sx_tile_boundaries_max")
-    a, b = (int(x) for x in out.tolist())
-    return [a, b] if many else a
+    heights = list(tile_rows) if isinstance(tile_rows, (tuple, list)) else [tile_rows, tile_rows]
+    a, b, _ = tile_stats(leaves, rows, device, heights[0], heights[1])
+    return [a, b] if isinstance(tile_rows, (tuple, list)) else a
 
 
 def _default_keys(leaves, rows: int, tile_rows: int = 32) -> int:
@@ -85,18 +95,20 @@ def bool_eval(leaves: Sequence[Tuple[torch.Tensor, torch.Tensor, torch.Tensor, i
     tuned = TUNED.get(workload_key([int(leaf[0].numel()) for leaf in leaves], rows)) if TUNED else None
     if mode == _lib.MODE_TABLE and not TUNING and rows > 0 and tuned is not None:
         tuning = dict(tuned)
-        if tuning.get("kernel") in (3, 4, 5):
-            tr = int(tuning.get("tile_rows", 0)) or (8 if tuning["kernel"] == 5 else 32)
+        if tuning.get("kernel") in (3, 4, 5, 6):
+            tr = int(tuning.get("tile_rows", 0)) or (8 if tuning["kernel"] >= 5 else 32)
             tuning["staging_cap"] = min(max_tile_boundaries(leaves, rows, device, tile_rows=tr), 25000)
     elif mode == _lib.MODE_TABLE and not TUNING and rows > 0:
         # Even rows: 8-row warp tiles with buffers sized for the largest tile
         # (no tile leaves the staged sweep, no buffer larger than needed).
         # Skewed rows (the largest 8-row tile far above the mean): 32-row
         # block tiles sized for their largest tile, which evens out the load.
-        need8, need32 = max_tile_boundaries(leaves, rows, device, tile_rows=(8, 32))
+        # Tiles spanning at most 8190 columns take 16-bit keys (half the
+        # shared memory per tile, twice the tiles in flight).
+        need8, need32, span8 = tile_stats(leaves, rows, device, 8, 32)
         mean8 = 2 * sum(int(leaf[0].numel()) for leaf in leaves) / max(1, (rows + 7) // 8)
         if need8 <= 3 * mean8 + 256:
-            tuning = {"kernel": 5, "staging_cap": min(need8, 25000), "tile_rows": 8}
+            tuning = {"kernel": 6 if span8 <= 8190 else 5, "staging_cap": min(need8, 25000), "tile_rows": 8}
         else:
             tuning = {"kernel": 4, "staging_cap": min(need32, 25000), "tile_rows": 32, "warps": 4}
     ob, oe, ooff, result = bool_eval_async(leaves, rows, table, mode, device, out, tuning=tuning)

@@ -1,7 +1,8 @@
 """Launch autotuner for the row-sweep set algebra (sx_bool_eval).
 
 The candidates are the kernel kinds of ``sx_tuning``: the warp-tile
-segmented sweep (8-row tiles) with several warps per block, the block-tile
+segmented sweep (8-row tiles, 32-bit and 16-bit keys) with several warps
+per block, the block-tile
 segmented sweep (32-row tiles) with two block sizes, the merge-path tile
 kernel with two key capacities per tile, and the one-lane-per-row sweep
 with several residency caps.  Each candidate is timed with CUDA events on the
@@ -37,6 +38,8 @@ def candidates(sizes: Sequence[int], rows: int, largest_tile: int = 0, largest_e
     cap8 = min(max(int(avg / 4 * 1.25 + 64), int(largest_eighth_tile)), 25000)
     for w in (2, 4, 8):
         out.append({"kernel": 5, "staging_cap": cap8, "warps": w, "tile_rows": 8})
+    for w in (2, 4, 8):
+        out.append({"kernel": 6, "staging_cap": cap8, "warps": w, "tile_rows": 8})
     cap = min(max(int(avg * 1.25 + 256), int(largest_tile)), 25000)
     for w in (4, 8):
         out.append({"kernel": 4, "staging_cap": cap, "warps": w, "tile_rows": 32})

@@ -97,7 +97,7 @@ int sx_bool_eval(const sx_leaf* leaves, int k, int32_t rows, const uint32_t* tab
     A.capacity = capacity;
     A.result = result;
     if (tuning) {
-        if (tuning->kernel < 0 || tuning->kernel > 5 || tuning->blocks_per_sm < 0 || tuning->staging_cap < 0 ||
+        if (tuning->kernel < 0 || tuning->kernel > 6 || tuning->blocks_per_sm < 0 || tuning->staging_cap < 0 ||
             tuning->warps < 0 || tuning->warps > 8 ||
             tuning->tile_rows < 0 || tuning->tile_rows > 32)
             return fail(SX_ERR_INVALID, "sx_bool_eval: bad tuning");
@@ -120,16 +120,19 @@ int sx_tile_boundaries_max(const sx_leaf* leaves, int k, int32_t rows, int32_t t
     if (!leaves || !out) return fail(SX_ERR_INVALID, "sx_tile_boundaries_max: null argument");
     if (rows < 0 || tile_rows_a < 1 || tile_rows_b < 1)
         return fail(SX_ERR_INVALID, "sx_tile_boundaries_max: bad rows or tile heights");
-    const int* offs[SX_MAX_LEAVES];
+    const int *offs[SX_MAX_LEAVES], *begs[SX_MAX_LEAVES], *ends[SX_MAX_LEAVES];
     for (int l = 0; l < k; ++l) {
         if (!leaves[l].row_offsets) return fail(SX_ERR_INVALID, "sx_tile_boundaries_max: leaf %d has no offsets", l);
         offs[l] = leaves[l].row_offsets;
+        begs[l] = leaves[l].begin;
+        ends[l] = leaves[l].end;
     }
     if (rows == 0) {
-        cudaError_t err = cudaMemsetAsync(out, 0, 2 * sizeof(int32_t), (cudaStream_t)stream);
+        cudaError_t err = cudaMemsetAsync(out, 0, 3 * sizeof(int32_t), (cudaStream_t)stream);
         return err == cudaSuccess ? SX_OK : cuda_fail(err, "sx_tile_boundaries_max");
     }
-    cudaError_t err = sx_tile_max_launch(offs, k, rows, tile_rows_a, tile_rows_b, out, (cudaStream_t)stream);
+    cudaError_t err =
+        sx_tile_max_launch(offs, begs, ends, k, rows, tile_rows_a, tile_rows_b, out, (cudaStream_t)stream);
     if (err != cudaSuccess) return cuda_fail(err, "sx_tile_boundaries_max");
     return SX_OK;
 }

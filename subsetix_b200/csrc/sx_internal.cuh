@@ -67,8 +67,8 @@ struct SxAlignArgs {
 
 cudaError_t sx_sweep_launch(const SxBoolArgs& A, bool union_mode, void* workspace, size_t workspace_bytes,
                             cudaStream_t stream);
-cudaError_t sx_tile_max_launch(const int* const* offsets, int k, int rows, int tra, int trb, int* out,
-                               cudaStream_t stream);
+cudaError_t sx_tile_max_launch(const int* const* offsets, const int* const* begins, const int* const* ends, int k,
+                               int rows, int tra, int trb, int* out, cudaStream_t stream);
 size_t sx_sweep_state_bytes(long long tiles);
 long long sx_sweep_tiles(int rows);
 cudaError_t sx_scan_i32_launch(const int* in, long long n, int* out, int* result, const SxScanState& st,

@@ -14,6 +14,8 @@
 // per-word popcounts, and a compaction.  row_min and row_max come from the
 // host.
 
+#include <climits>
+
 #include "sx_internal.cuh"
 
 __global__ void sx_align_clear_kernel(unsigned* bitmap, long long nwords)
@@ -117,22 +119,38 @@ cudaError_t sx_align_launch(SxAlignArgs& A, int out_capacity, const SxScanState&
 }
 
 // Largest number of leaf boundaries (2 x intervals, all leaves together) in
-// a tile of `tr[0]` aligned rows and in a tile of `tr[1]` aligned rows;
-// out[0], out[1] must start at zero.
+// a tile of `tra` aligned rows (out[0]) and of `trb` aligned rows (out[1]),
+// and the largest coordinate span of a `tra`-row tile (out[2]: the last end
+// of its rows minus their first begin; rows are assumed canonical, anything
+// else only overstates it).  out must start at zero.
 struct SxOffList {
     const int* off[SX_MAX_LEAVES];
+    const int* begin[SX_MAX_LEAVES];
+    const int* end[SX_MAX_LEAVES];
 };
 
 __global__ void sx_tile_max_kernel(SxOffList L, int k, int rows, int tra, int trb, int* out)
 {
     const int tiles_a = (rows + tra - 1) / tra, tiles_b = (rows + trb - 1) / trb;
-    int ma = 0, mb = 0;
+    int ma = 0, mb = 0, span = 0;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < tiles_a || t < tiles_b; t += gridDim.x * blockDim.x) {
         if (t < tiles_a) {
             const int r0 = t * tra, r1 = min(rows, r0 + tra);
             int c = 0;
-            for (int l = 0; l < k; ++l) c += L.off[l][r1] - L.off[l][r0];
+            long long lo = LLONG_MAX, hi = LLONG_MIN;
+            for (int l = 0; l < k; ++l) {
+                c += L.off[l][r1] - L.off[l][r0];
+                if (!L.begin[l] || !L.end[l]) continue;  // a leaf without intervals has no arrays
+                for (int r = r0; r < r1; ++r) {
+                    const int a = L.off[l][r], b = L.off[l][r + 1];
+                    if (b > a) {
+                        lo = min(lo, (long long)min(L.begin[l][a], L.end[l][a]));
+                        hi = max(hi, (long long)max(L.end[l][b - 1], L.begin[l][b - 1]));
+                    }
+                }
+            }
             ma = max(ma, c);
+            if (hi >= lo) span = (int)min((long long)INT_MAX, max((long long)span, hi - lo));
         }
         if (t < tiles_b) {
             const int r0 = t * trb, r1 = min(rows, r0 + trb);
@@ -145,19 +163,25 @@ __global__ void sx_tile_max_kernel(SxOffList L, int k, int rows, int tra, int tr
     for (int o = 16; o > 0; o >>= 1) {
         ma = max(ma, __shfl_xor_sync(0xFFFFFFFFu, ma, o));
         mb = max(mb, __shfl_xor_sync(0xFFFFFFFFu, mb, o));
+        span = max(span, __shfl_xor_sync(0xFFFFFFFFu, span, o));
     }
     if ((threadIdx.x & 31) == 0) {
         if (ma > 0) atomicMax(&out[0], 2 * ma);
         if (mb > 0) atomicMax(&out[1], 2 * mb);
+        if (span > 0) atomicMax(&out[2], span);
     }
 }
 
-cudaError_t sx_tile_max_launch(const int* const* offsets, int k, int rows, int tra, int trb, int* out,
-                               cudaStream_t stream)
+cudaError_t sx_tile_max_launch(const int* const* offsets, const int* const* begins, const int* const* ends, int k,
+                               int rows, int tra, int trb, int* out, cudaStream_t stream)
 {
     SxOffList L;
-    for (int l = 0; l < SX_MAX_LEAVES; ++l) L.off[l] = l < k ? offsets[l] : nullptr;
-    cudaError_t err = cudaMemsetAsync(out, 0, 2 * sizeof(int), stream);
+    for (int l = 0; l < SX_MAX_LEAVES; ++l) {
+        L.off[l] = l < k ? offsets[l] : nullptr;
+        L.begin[l] = l < k ? begins[l] : nullptr;
+        L.end[l] = l < k ? ends[l] : nullptr;
+    }
+    cudaError_t err = cudaMemsetAsync(out, 0, 3 * sizeof(int), stream);
     if (err != cudaSuccess) return err;
     const int tiles = (rows + min(tra, trb) - 1) / min(tra, trb);
     int grid = (tiles + 255) / 256;

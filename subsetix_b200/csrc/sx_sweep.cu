@@ -1919,6 +1919,330 @@ __global__ void __launch_bounds__(256) sx_wseg_kernel(SxBoolArgs A, SxSweepState
     sxs_report(A, tile, tiles, base, total >> 1, flags);
 }
 
+// ---------------------------------------------------------------------------
+// Warp-tile segmented sweep with 16-bit keys.
+//
+// In a tile of at most 8 rows whose coordinates span at most 8190, a key
+// (row << 13 | (x - xmin)) fits in 16 bits.  The begins of all leaves are
+// staged first and the ends after them.  Interval j's key pair is then
+// written in place over its staged begin (one 32-bit word holds both keys),
+// the staged ends, once checked, become the output area, and the dead key
+// lists take the packed output.  A tile so needs 4 bytes of shared memory
+// per boundary instead of 8, and twice as many tiles are in flight per SM.
+// Everything else is the 32-bit warp kernel above.
+// ---------------------------------------------------------------------------
+#define SXW16_XBITS 13
+#define SXW16_XMASK ((1u << SXW16_XBITS) - 1u)
+#define SXW16_SPAN 8190
+#define SXW16_SENTINEL 0xFFFFu
+
+// The 16-bit form of sxs_advance: keys are halfwords, pa a byte address.
+__device__ __forceinline__ void sxs_advance16(unsigned& h, unsigned& pa, unsigned& state, unsigned c, unsigned bit)
+{
+    asm volatile(
+        "{\n .reg .pred q;\n .reg .b16 t;\n setp.eq.u32 q, %0, %3;\n @q add.u32 %1, %1, 2;\n"
+        " @q xor.b32 %2, %2, %4;\n @q ld.shared.u16 t, [%1];\n @q cvt.u32.u16 %0, t;\n}\n"
+        : "+r"(h), "+r"(pa), "+r"(state)
+        : "r"(c), "r"(bit));
+}
+
+__device__ __forceinline__ void sxs_emit16(unsigned& oa, unsigned f, unsigned fprev, unsigned c)
+{
+    asm volatile(
+        "{\n .reg .pred q;\n .reg .b16 t;\n setp.ne.u32 q, %1, %2;\n cvt.u16.u32 t, %3;\n"
+        " @q st.shared.u16 [%0], t;\n @q add.u32 %0, %0, 2;\n}\n"
+        : "+r"(oa)
+        : "r"(f), "r"(fprev), "r"(c)
+        : "memory");
+}
+
+__device__ __forceinline__ int sxs_lower_bound16(const unsigned short* k, int n, unsigned v)
+{
+    int pos = 0;
+    while (n > 0) {
+        const int half = n >> 1;
+        if ((unsigned)k[pos + half] < v) {
+            pos += half + 1;
+            n -= half + 1;
+        } else {
+            n = half;
+        }
+    }
+    return pos;
+}
+
+template <int K>
+__global__ void __launch_bounds__(256) sx_wseg16_kernel(SxBoolArgs A, SxSweepState st, int tiles, int cap_words,
+                                                        int tr)
+{
+    extern __shared__ __align__(16) unsigned char sxw_smem[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, NW = blockDim.x >> 5;
+    if (blockIdx.x * NW + wid >= tiles) return;  // exactly `tiles` warps take tickets
+    unsigned* base_w = (unsigned*)(sxw_smem + (size_t)wid * sxw_slice_bytes(K, tr, cap_words));
+    unsigned long long* bar = (unsigned long long*)base_w;
+    const int os = tr + 1;
+    int* off = (int*)base_w + 2;
+    int* rawb = off + os * K;
+    int* rawe = rawb + K;
+    unsigned* Wd = base_w + sxw_hdr_words(K, tr);
+
+    int tile = 0;
+    if (lane == 0) {
+        tile = (int)atomicAdd(&st.counters[0], 1u);
+        sxs_bar_init(bar);
+    }
+    tile = __shfl_sync(0xFFFFFFFFu, tile, 0);
+    const int r0 = tile * tr;
+    const int nrows = min(tr, A.rows - r0);
+    for (int r = lane; r <= nrows; r += 32) {
+#pragma unroll
+        for (int l = 0; l < K; ++l) off[l * os + r] = A.leaf[l].off[r0 + r];
+    }
+    __syncwarp();
+    // layout (words): the begins of every leaf [0, RB), then the ends [RB, 2 RB)
+    int n[K];
+    long long RBl = 0, El = 0;
+    int big = 0, nbig = -1;
+    bool ok = tr <= 8;
+#pragma unroll
+    for (int l = 0; l < K; ++l) {
+        n[l] = off[l * os + nrows] - off[l * os];
+        ok = ok && n[l] >= 0;
+        RBl += (n[l] + 11) & ~3;  // a copy of at most n + 6 words, 16-byte aligned, then the list's sentinel
+        El += 2ll * n[l];
+        if (n[l] > nbig) {
+            big = l;
+            nbig = n[l];
+        }
+    }
+    const bool fits = ok && 2 * RBl <= (long long)cap_words;
+    const int E = fits ? (int)El : 0, RB = (int)RBl;
+    unsigned* raw = Wd;
+    unsigned short* const h16 = (unsigned short*)Wd;  // halfword view of the slice
+    // 1. bulk copies: lane q < K copies leaf q's begins, lane K + q its ends
+    if (fits) {
+        const int q = lane < 2 * K ? lane : 0;
+        const bool ends = q >= K;
+        const int l = ends ? q - K : q;
+        int nl = 0, g0 = 0;
+        const int* arr = nullptr;
+#pragma unroll
+        for (int m = 0; m < K; ++m)
+            if (m == l) {
+                nl = n[m];
+                g0 = off[m * os];
+                arr = ends ? A.leaf[m].end : A.leaf[m].begin;
+            }
+        const int* g = arr + g0;
+        const uintptr_t a0 = (uintptr_t)g & ~(uintptr_t)15;
+        const unsigned len =
+            (lane < 2 * K && nl > 0) ? (unsigned)((((uintptr_t)(g + nl) + 15) & ~(uintptr_t)15) - a0) : 0u;
+        // region of this copy: the begins' regions first, then the ends'
+        int region = lane < 2 * K ? ((nl + 11) & ~3) : 0;
+        int incl = region;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int pos = incl - region;
+        int bytes = (int)len;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) bytes += __shfl_xor_sync(0xFFFFFFFFu, bytes, o);
+        if (lane < 2 * K) {
+            const int first = pos + (int)(((uintptr_t)g & 15) >> 2);
+            if (ends) rawe[l] = first; else rawb[l] = first;
+        }
+        __syncwarp();  // orders the lanes' writes before lane 0's release on the barrier
+        if (lane == 0) sxs_bar_expect(bar, (unsigned)bytes);
+        __syncwarp();
+        if (len > 0u) sxs_bulk_copy(raw + pos, (const void*)a0, len, bar);
+    }
+    bool copied = true;
+    if (fits) copied = __all_sync(0xFFFFFFFFu, sxs_bar_wait(bar));
+    unsigned flags = (fits && !copied) ? SXF_TIMEOUT : 0u;
+    // 2. coordinate span: first begin and last end of every leaf row
+    int xmin = INT_MAX, xmax = INT_MIN;
+    if (fits && copied) {
+        if (lane < nrows) {
+#pragma unroll
+            for (int l = 0; l < K; ++l) {
+                const int a = off[l * os + lane] - off[l * os], b = off[l * os + lane + 1] - off[l * os];
+                if (a >= 0 && a < b && b <= n[l]) {
+                    xmin = min(xmin, (int)raw[rawb[l] + a]);
+                    xmax = max(xmax, (int)raw[rawe[l] + b - 1]);
+                }
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            xmin = min(xmin, __shfl_xor_sync(0xFFFFFFFFu, xmin, o));
+            xmax = max(xmax, __shfl_xor_sync(0xFFFFFFFFu, xmax, o));
+        }
+    }
+    __syncwarp();  // the begins read above are overwritten below
+    const bool staged = fits && copied && (E == 0 || (long long)xmax - (long long)xmin <= SXW16_SPAN);
+    bool bad = false;
+    // 3. keys in place: begin word j becomes interval j's key pair
+    if (staged) {
+#pragma unroll
+        for (int l = 0; l < K; ++l) {
+            const int* o = off + l * os;
+            const int g0 = o[0];
+            unsigned* rb = raw + rawb[l];
+            const unsigned* re = raw + rawe[l];
+            int rc = 0;
+            for (int j0 = 0; j0 < n[l]; j0 += 32) {
+                const int j = j0 + lane;
+                int r = rc;
+                if (j < n[l]) {
+                    while (r + 1 < nrows && o[r + 1] - g0 <= j) ++r;
+                    const int b = (int)rb[j], e = (int)re[j];
+                    const bool first = j == o[r] - g0;
+                    if (!(b < e) || (!first && !((int)re[j - 1] < b)) || o[r] - g0 > j) bad = true;
+                    const unsigned rk = (unsigned)r << SXW16_XBITS;
+                    rb[j] = (rk | ((unsigned)(b - xmin) & SXW16_XMASK)) |
+                            ((rk | ((unsigned)(e - xmin) & SXW16_XMASK)) << 16);
+                }
+                rc = __shfl_sync(0xFFFFFFFFu, r, 31);
+            }
+            if (lane == 0) rb[n[l]] = 0xFFFFFFFFu;  // the list's sentinel
+        }
+    }
+    bad = __any_sync(0xFFFFFFFFu, bad);
+    __syncwarp();
+    if (bad) flags |= SXF_CONTRACT;
+    const bool sweep = staged && !bad && E > 0;
+    unsigned short* out16 = h16 + 2 * RB;  // the staged ends, dead after the check
+    int count = 0, total = 0, excl = 0, prov = 0;
+    if (sweep) {
+        // 4. this lane's piece [klo, khi) and where it starts in every list
+        const int nb2 = 2 * nbig;
+        int bigw = 0;
+#pragma unroll
+        for (int l = 0; l < K; ++l)
+            if (l == big) bigw = rawb[l];
+        const unsigned short* Lb = h16 + 2 * bigw;
+        const unsigned klo = lane > 0 ? (unsigned)Lb[(lane * nb2) / 32] : 0u;
+        const unsigned khi = lane < 31 ? (unsigned)Lb[((lane + 1) * nb2) / 32] : SXW16_SENTINEL;
+        const int rp = (int)(klo >> SXW16_XBITS);
+        unsigned pa[K];
+        unsigned h[K];
+        unsigned state = 0u;
+#pragma unroll
+        for (int l = 0; l < K; ++l) {
+            const unsigned short* Ll = h16 + 2 * rawb[l];
+            int pos;
+            if (lane == 0) {
+                pos = 0;
+            } else if (l == big) {
+                pos = (lane * nb2) / 32;
+            } else {
+                const int lo = 2 * (off[l * os + rp] - off[l * os]);
+                const int hi = 2 * (off[l * os + rp + 1] - off[l * os]);
+                pos = lo + sxs_lower_bound16(Ll + lo, hi - lo, klo);
+            }
+            pa[l] = sxs_saddr(Ll + pos);
+            h[l] = Ll[pos];
+            state |= (unsigned)(pos & 1) << l;
+            prov += pos;
+        }
+        // 5. the sweep
+        const unsigned tab0 = A.table[0];
+        unsigned fprev = K <= 5 ? (tab0 >> state) & 1u : (A.table[state >> 5] >> (state & 31u)) & 1u;
+        const unsigned o0 = sxs_saddr(out16 + prov), oend = sxs_saddr(out16 + E);
+        unsigned oa = o0;
+        while (true) {
+            unsigned c = h[0];
+#pragma unroll
+            for (int l = 1; l < K; ++l) c = min(c, h[l]);
+            if (c >= khi) break;
+#pragma unroll
+            for (int l = 0; l < K; ++l) sxs_advance16(h[l], pa[l], state, c, 1u << l);
+            const unsigned f = K <= 5 ? (tab0 >> state) & 1u : (A.table[state >> 5] >> (state & 31u)) & 1u;
+            sxs_emit16(oa, f, fprev, c);
+            oa = min(oa, oend);
+            fprev = f;
+        }
+        count = (int)((oa - o0) >> 1);
+        int incl = count;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        excl = incl - count;
+        total = min(__shfl_sync(0xFFFFFFFFu, incl, 31), E);
+    }
+    // fallback tile: one lane per row over global memory
+    int lane_count = 0;
+    int s_row[K], lim_row[K];
+    if (!staged) {
+        const bool act = lane < nrows;
+#pragma unroll
+        for (int l = 0; l < K; ++l) {
+            const int a = act ? off[l * os + lane] : 0;
+            const int b = act ? off[l * os + lane + 1] : 0;
+            s_row[l] = a;
+            lim_row[l] = 2 * (b - a);
+        }
+        bool fb_bad = false, fb_over = false;
+        if (act) lane_count = sx_sweep_table<K, false>(A, s_row, lim_row, nullptr, nullptr, 0, fb_bad, fb_over);
+        if (__any_sync(0xFFFFFFFFu, fb_bad)) flags |= SXF_CONTRACT;
+        int tot = lane_count;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xFFFFFFFFu, tot, o);
+        total = 2 * tot;
+    }
+    // 6. look-back, then pack the output boundaries over the dead key lists
+    const int base = sxs_lookback(st, tile, total >> 1, flags);
+    bool over = false;
+    if (staged) {
+        unsigned short* packed = h16;
+        __syncwarp();
+        if (sweep) {
+            const int m = min(count, E - excl);
+            for (int i = 0; i < m; ++i) packed[excl + i] = out16[prov + i];
+        }
+        __syncwarp();
+        // 7. coalesced output and the tile's row offsets
+        const int nint = total >> 1;
+        const unsigned* pw = (const unsigned*)packed;
+        for (int i = lane; i < nint; i += 32) {
+            const unsigned kv = pw[i];
+            const long long o = (long long)base + i;
+            if (o < A.capacity) {
+                A.out_begin[o] = xmin + (int)(kv & SXW16_XMASK);
+                A.out_end[o] = xmin + (int)((kv >> 16) & SXW16_XMASK);
+            } else {
+                over = true;
+            }
+        }
+        for (int r = lane; r < nrows; r += 32) {
+            const int pos = sxs_lower_bound16(packed, total, (unsigned)(r + 1) << SXW16_XBITS);
+            A.out_off[r0 + r + 1] = base + (pos >> 1);
+        }
+        if (tile == 0 && lane == 0) A.out_off[0] = 0;
+    } else {
+        int incl = lane_count;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane < nrows) {
+            bool fb_bad = false;
+            if (lane_count > 0)
+                sx_sweep_table<K, true>(A, s_row, lim_row, A.out_begin, A.out_end, (long long)base + incl - lane_count,
+                                        fb_bad, over);
+            A.out_off[r0 + lane + 1] = base + incl;
+        }
+        if (tile == 0 && lane == 0) A.out_off[0] = 0;
+    }
+    (void)over;  // an output beyond the capacity shows in the reported total
+    sxs_report(A, tile, tiles, base, total >> 1, flags);
+}
+
 size_t sx_sweep_state_bytes(long long tiles)
 {
     const long long groups = (tiles + SX_GROUP - 1) / SX_GROUP;
@@ -2044,6 +2368,23 @@ static cudaError_t sx_wseg_launch_k(const SxBoolArgs& A, const SxSweepState& st,
     return cudaGetLastError();
 }
 
+template <int K>
+static cudaError_t sx_wseg16_launch_k(const SxBoolArgs& A, const SxSweepState& st, int tiles, int cap_words,
+                                      int warps, int tr, cudaStream_t stream)
+{
+    static int configured = 0;  // largest dynamic shared memory set for this instantiation
+    const int bytes = warps * (int)sxw_slice_bytes(K, tr, cap_words);
+    if (bytes > configured) {
+        cudaError_t err =
+            cudaFuncSetAttribute(sx_wseg16_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        if (err != cudaSuccess) return err;
+        configured = bytes;
+    }
+    const int blocks = (tiles + warps - 1) / warps;
+    sx_wseg16_kernel<K><<<blocks, 32 * warps, bytes, stream>>>(A, st, tiles, cap_words, tr);
+    return cudaGetLastError();
+}
+
 // Segmented sweep shape: `keys` boundaries per tile (0: 1.25x the average
 // plus slack), stored twice (lists and output area), at most 200 KiB per
 // block; `warps` per block (0: about 48 boundaries per thread).
@@ -2090,10 +2431,11 @@ cudaError_t sx_sweep_launch(const SxBoolArgs& A, bool union_mode, void* workspac
     if (A.rows <= 0) return cudaSuccess;
     // The segmented sweep takes tiles of 16 rows when the workspace holds
     // their look-back state (smaller tiles keep more blocks resident), else 32.
-    const bool seg = !union_mode && (A.tune_kernel == 0 || A.tune_kernel == 4 || A.tune_kernel == 5);
+    const bool seg = !union_mode && (A.tune_kernel == 0 || A.tune_kernel >= 4);
     int tr = 32;
     if (seg) {
         tr = A.tune_tile_rows > 0 ? A.tune_tile_rows : (A.tune_kernel == 4 ? 32 : 8);
+        if (A.tune_kernel == 6 && tr > 8) tr = 8;  // 16-bit keys hold 3 row bits
         if (sx_sweep_state_bytes(((long long)A.rows + tr - 1) / tr) > workspace_bytes) tr = 32;
     }
     const long long tiles = ((long long)A.rows + tr - 1) / tr;
@@ -2122,6 +2464,31 @@ cudaError_t sx_sweep_launch(const SxBoolArgs& A, bool union_mode, void* workspac
     // heavy tiles (measured best on the 4096x4096 shape expression).
     SxBoolArgs B = A;
     if (B.tune_kernel == 0) B.tune_kernel = 5;
+    if (B.tune_kernel == 6 && tr <= 8) {
+        // words per warp: the staged begins and ends (later keys and outputs) of the largest tile
+        const long long avg = (2 * A.capacity + tiles - 1) / tiles;
+        const long long e = A.tune_staging_cap > 0 ? A.tune_staging_cap : avg + avg / 4 + 64;
+        long long words = e + 22 * A.k + 8;
+        const long long room = (200 * 1024) / 4 - sxw_hdr_words(A.k, tr);
+        int warps = A.tune_warps > 0 ? A.tune_warps : (int)(room / (words + sxw_hdr_words(A.k, tr)));
+        if (warps > 4 && A.tune_warps <= 0) warps = 4;
+        if (warps < 1) warps = 1;
+        const long long limit = (200 * 1024) / warps / 4 - sxw_hdr_words(A.k, tr);
+        if (words > limit) words = limit;
+        const int cw = (int)words;
+        switch (A.k) {
+            case 1: return sx_wseg16_launch_k<1>(A, st, t, cw, warps, tr, stream);
+            case 2: return sx_wseg16_launch_k<2>(A, st, t, cw, warps, tr, stream);
+            case 3: return sx_wseg16_launch_k<3>(A, st, t, cw, warps, tr, stream);
+            case 4: return sx_wseg16_launch_k<4>(A, st, t, cw, warps, tr, stream);
+            case 5: return sx_wseg16_launch_k<5>(A, st, t, cw, warps, tr, stream);
+            case 6: return sx_wseg16_launch_k<6>(A, st, t, cw, warps, tr, stream);
+            case 7: return sx_wseg16_launch_k<7>(A, st, t, cw, warps, tr, stream);
+            case 8: return sx_wseg16_launch_k<8>(A, st, t, cw, warps, tr, stream);
+            default: return cudaErrorInvalidValue;
+        }
+    }
+    if (B.tune_kernel == 6) B.tune_kernel = 5;  // tiles above 8 rows: 32-bit keys
     if (B.tune_kernel == 5) {
         // words per warp: the copies (or outputs) and the key lists of the largest tile
         const long long avg = (2 * A.capacity + tiles - 1) / tiles;

@@ -247,7 +247,9 @@ def test_wide_coordinate_span_vs_oracle(cuda_device):
                                     {"kernel": 4, "staging_cap": 256}, {"kernel": 4, "warps": 1},
                                     {"kernel": 4, "warps": 8}, {"kernel": 4, "staging_cap": 20000, "warps": 3},
                                     {"kernel": 4, "tile_rows": 16}, {"kernel": 5}, {"kernel": 5, "tile_rows": 32},
-                                    {"kernel": 5, "tile_rows": 1, "warps": 1}, {"kernel": 5, "staging_cap": 64}])
+                                    {"kernel": 5, "tile_rows": 1, "warps": 1}, {"kernel": 5, "staging_cap": 64},
+                                    {"kernel": 6}, {"kernel": 6, "tile_rows": 3, "warps": 1},
+                                    {"kernel": 6, "staging_cap": 64}, {"kernel": 6, "tile_rows": 32}])
 def test_tuning_never_changes_results(cuda_device, tuning):
     from subsetix_b200 import _core
 
@@ -274,13 +276,31 @@ def test_tile_boundaries_max(cuda_device):
     host = []
     for _ in range(3):
         off = np.concatenate([[0], np.cumsum(rng.integers(0, 40, rows))]).astype(np.int32)
-        host.append(off)
-        t = torch.as_tensor(off, device="cuda")
-        leaves.append((t, t, t, 0))
+        n = int(off[-1])
+        beg = rng.integers(-5000, 5000, n).astype(np.int32)
+        end = (beg + rng.integers(1, 50, n)).astype(np.int32)
+        host.append((off, beg, end))
+        leaves.append((torch.as_tensor(beg, device="cuda"), torch.as_tensor(end, device="cuda"),
+                       torch.as_tensor(off, device="cuda"), 0))
     for a, b in ((8, 32), (1, 7), (16, 1000), (5, 2000)):
         got = _core.max_tile_boundaries(leaves, rows, torch.device("cuda", 0), tile_rows=(a, b))
+        stats = _core.tile_stats(leaves, rows, torch.device("cuda", 0), a, b)
+        assert stats[:2] == tuple(got)
         want = []
         for tr in (a, b):
             edges = np.minimum(np.arange(0, rows + tr, tr), rows)
-            want.append(2 * int(max(sum(o[edges[1:]] - o[edges[:-1]] for o in host).max(), 0)))
+            want.append(2 * int(max(sum(o[edges[1:]] - o[edges[:-1]] for o, _, _ in host).max(), 0)))
         assert got == want, (a, b)
+        span = 0
+        for t0 in range(0, rows, a):
+            lo, hi = None, None
+            for off, beg, end in host:
+                for r in range(t0, min(rows, t0 + a)):
+                    if off[r + 1] > off[r]:
+                        x0 = min(beg[off[r]], end[off[r]])
+                        x1 = max(end[off[r + 1] - 1], beg[off[r + 1] - 1])
+                        lo = x0 if lo is None else min(lo, x0)
+                        hi = x1 if hi is None else max(hi, x1)
+            if lo is not None:
+                span = max(span, int(hi) - int(lo))
+        assert stats[2] == span, (a, b)
