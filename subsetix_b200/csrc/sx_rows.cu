@@ -172,6 +172,59 @@ __global__ void sx_tile_max_kernel(SxOffList L, int k, int rows, int tra, int tr
     }
 }
 
+// The same for tile heights that are powers of two up to 32: one thread per
+// row, tiles reduced over groups of lanes, one atomic per block.
+__global__ void sx_tile_max_rows_kernel(SxOffList L, int k, int rows, int tra, int trb, int* out)
+{
+    __shared__ int s_max[3];
+    if (threadIdx.x < 3) s_max[threadIdx.x] = 0;
+    __syncthreads();
+    int ma = 0, mb = 0, span = 0;
+    const int stride = gridDim.x * blockDim.x;
+    const int rows_up = (rows + 31) & ~31;  // whole warps, so the shuffles see full groups
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows_up; r += stride) {
+        int c = 0;
+        long long lo = LLONG_MAX, hi = LLONG_MIN;
+        if (r < rows) {
+            for (int l = 0; l < k; ++l) {
+                const int a = L.off[l][r], b = L.off[l][r + 1];
+                c += b - a;
+                if (b > a && L.begin[l] && L.end[l]) {
+                    lo = min(lo, (long long)min(L.begin[l][a], L.end[l][a]));
+                    hi = max(hi, (long long)max(L.end[l][b - 1], L.begin[l][b - 1]));
+                }
+            }
+        }
+        int ca = c, cb = c;
+        for (int o = 1; o < tra; o <<= 1) {
+            ca += __shfl_xor_sync(0xFFFFFFFFu, ca, o);
+            lo = min(lo, (long long)__shfl_xor_sync(0xFFFFFFFFu, lo, o));
+            hi = max(hi, (long long)__shfl_xor_sync(0xFFFFFFFFu, hi, o));
+        }
+        for (int o = 1; o < trb; o <<= 1) cb += __shfl_xor_sync(0xFFFFFFFFu, cb, o);
+        ma = max(ma, ca);
+        mb = max(mb, cb);
+        if (hi >= lo) span = (int)min((long long)INT_MAX, max((long long)span, hi - lo));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        ma = max(ma, __shfl_xor_sync(0xFFFFFFFFu, ma, o));
+        mb = max(mb, __shfl_xor_sync(0xFFFFFFFFu, mb, o));
+        span = max(span, __shfl_xor_sync(0xFFFFFFFFu, span, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(&s_max[0], ma);
+        atomicMax(&s_max[1], mb);
+        atomicMax(&s_max[2], span);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (s_max[0] > 0) atomicMax(&out[0], 2 * s_max[0]);
+        if (s_max[1] > 0) atomicMax(&out[1], 2 * s_max[1]);
+        if (s_max[2] > 0) atomicMax(&out[2], s_max[2]);
+    }
+}
+
 cudaError_t sx_tile_max_launch(const int* const* offsets, const int* const* begins, const int* const* ends, int k,
                                int rows, int tra, int trb, int* out, cudaStream_t stream)
 {
@@ -183,6 +236,14 @@ cudaError_t sx_tile_max_launch(const int* const* offsets, const int* const* begi
     }
     cudaError_t err = cudaMemsetAsync(out, 0, 3 * sizeof(int), stream);
     if (err != cudaSuccess) return err;
+    const bool pow2 = tra <= 32 && trb <= 32 && (tra & (tra - 1)) == 0 && (trb & (trb - 1)) == 0;
+    if (pow2) {
+        int grid = (rows + 255) / 256;
+        if (grid > 2368) grid = 2368;
+        if (grid < 1) grid = 1;
+        sx_tile_max_rows_kernel<<<grid, 256, 0, stream>>>(L, k, rows, tra, trb, out);
+        return cudaGetLastError();
+    }
     const int tiles = (rows + min(tra, trb) - 1) / min(tra, trb);
     int grid = (tiles + 255) / 256;
     if (grid > 1184) grid = 1184;
