@@ -1104,7 +1104,8 @@ __global__ void __launch_bounds__(SXM_THREADS) sx_merge_kernel(SxBoolArgs A, SxS
 #define SXS_XMASK ((1u << SXS_XBITS) - 1u)
 #define SXS_MAX_THREADS 256
 #define SXS_SENTINEL 0xFFFFFFFFu
-#define SXS_WAIT_LIMIT (1u << 22)
+#define SXS_WAIT_LIMIT (1u << 16)
+#define SXS_WAIT_HINT_NS 20000
 
 struct SxsTile {
     int off[SX_TABLE_MAX_LEAVES][SXM_TR + 1];
@@ -1144,20 +1145,41 @@ __device__ __forceinline__ void sxs_bulk_copy(void* dst, const void* src, unsign
                  : "memory");
 }
 
-// Bounded wait for phase 0 of `bar`; false if it did not complete.
+// Bounded wait for phase 0 of `bar`; false if it did not complete.  Each
+// try_wait may suspend the thread for up to SXS_WAIT_HINT_NS (it resumes as
+// soon as the phase completes), so waiting warps take no issue slots; the
+// whole wait is bounded by SXS_WAIT_LIMIT tries.
 __device__ __forceinline__ bool sxs_bar_wait(unsigned long long* bar)
 {
     const unsigned a = sxs_saddr(bar);
     for (unsigned i = 0; i < SXS_WAIT_LIMIT; ++i) {
         unsigned done;
         asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}\n"
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0, %2;\n selp.u32 %0, 1, 0, p;\n}\n"
             : "=r"(done)
-            : "r"(a)
+            : "r"(a), "n"(SXS_WAIT_HINT_NS)
             : "memory");
         if (done) return true;
     }
     return false;
+}
+
+// Wait until a tile status word is published, backing off from 32 ns to
+// 512 ns between polls so that waiting warps leave the issue slots to the
+// warps that sweep; bounded by SX_LOOKBACK_SPIN_LIMIT polls.
+__device__ __forceinline__ unsigned long long sxs_wait_status(const unsigned long long* p, bool& timed_out)
+{
+    unsigned sleep = 32;
+    for (unsigned spins = 0;; ++spins) {
+        const unsigned long long w = sx_ld_status(p);
+        if ((w >> 32) & 3ull) return w;
+        if (spins > SX_LOOKBACK_SPIN_LIMIT) {
+            timed_out = true;
+            return (SX_KIND_PREFIX << 32);  // treat as a zero prefix so the kernel finishes
+        }
+        __nanosleep(sleep);
+        if (sleep < 512) sleep <<= 1;
+    }
 }
 
 // Single-level decoupled look-back for the segmented sweeps (whole warp).
@@ -1182,7 +1204,7 @@ __device__ __forceinline__ int sxs_lookback(const SxSweepState& st, int tile, in
     for (int pos = tile - 1;; pos -= 32) {
         const int t = pos - lane;
         unsigned long long w = SX_KIND_PREFIX << 32;  // before tile 0: an empty prefix
-        if (t >= 0) w = sx_wait_status(&st.tile_status[t], timed_out);
+        if (t >= 0) w = sxs_wait_status(&st.tile_status[t], timed_out);
         const unsigned pm = __ballot_sync(0xFFFFFFFFu, ((w >> 32) & 3ull) == SX_KIND_PREFIX);
         const int stop = pm ? __ffs(pm) - 1 : 32;
         int v = lane <= stop ? (int)(unsigned)(w & 0xFFFFFFFFull) : 0;
@@ -1940,8 +1962,8 @@ __global__ void __launch_bounds__(256) sx_wseg_kernel(SxBoolArgs A, SxSweepState
 __device__ __forceinline__ void sxs_advance16(unsigned& h, unsigned& pa, unsigned& state, unsigned c, unsigned bit)
 {
     asm volatile(
-        "{\n .reg .pred q;\n .reg .b16 t;\n setp.eq.u32 q, %0, %3;\n @q add.u32 %1, %1, 2;\n"
-        " @q xor.b32 %2, %2, %4;\n @q ld.shared.u16 t, [%1];\n @q cvt.u32.u16 %0, t;\n}\n"
+        "{\n .reg .pred q;\n setp.eq.u32 q, %0, %3;\n @q add.u32 %1, %1, 2;\n"
+        " @q xor.b32 %2, %2, %4;\n @q ld.shared.u16 %0, [%1];\n}\n"
         : "+r"(h), "+r"(pa), "+r"(state)
         : "r"(c), "r"(bit));
 }
@@ -1949,8 +1971,7 @@ __device__ __forceinline__ void sxs_advance16(unsigned& h, unsigned& pa, unsigne
 __device__ __forceinline__ void sxs_emit16(unsigned& oa, unsigned f, unsigned fprev, unsigned c)
 {
     asm volatile(
-        "{\n .reg .pred q;\n .reg .b16 t;\n setp.ne.u32 q, %1, %2;\n cvt.u16.u32 t, %3;\n"
-        " @q st.shared.u16 [%0], t;\n @q add.u32 %0, %0, 2;\n}\n"
+        "{\n .reg .pred q;\n setp.ne.u32 q, %1, %2;\n @q st.shared.u16 [%0], %3;\n @q add.u32 %0, %0, 2;\n}\n"
         : "+r"(oa)
         : "r"(f), "r"(fprev), "r"(c)
         : "memory");
