@@ -2104,28 +2104,50 @@ __global__ void __launch_bounds__(256) sx_wseg16_kernel(SxBoolArgs A, SxSweepSta
     __syncwarp();  // the begins read above are overwritten below
     const bool staged = fits && copied && (E == 0 || (long long)xmax - (long long)xmin <= SXW16_SPAN);
     bool bad = false;
-    // 3. keys in place: begin word j becomes interval j's key pair
+    // 3. keys in place: begin word j becomes interval j's key pair.  The row
+    //    of interval j counts the leaf's row starts at or below j (seven
+    //    compares against registers, no branch); j starts a row when its row
+    //    differs from interval j - 1's (taken from the lane below, or carried
+    //    over from the previous chunk).
     if (staged) {
 #pragma unroll
         for (int l = 0; l < K; ++l) {
             const int* o = off + l * os;
             const int g0 = o[0];
+            int rs[7];
+#pragma unroll
+            for (int i = 0; i < 7; ++i) rs[i] = i + 1 < nrows ? o[i + 1] - g0 : INT_MAX;
+            bool disordered = false;  // row offsets must rise from 0 to n[l]
+#pragma unroll
+            for (int i = 0; i < 7; ++i)
+                disordered = disordered || rs[i] < 0 || (rs[i] != INT_MAX && rs[i] > n[l]) ||
+                             (i < 6 && rs[i] > rs[i + 1]);
+            if (disordered) bad = true;
             unsigned* rb = raw + rawb[l];
             const unsigned* re = raw + rawe[l];
-            int rc = 0;
+            int carry_r = -1, carry_e = 0;
             for (int j0 = 0; j0 < n[l]; j0 += 32) {
                 const int j = j0 + lane;
-                int r = rc;
-                if (j < n[l]) {
-                    while (r + 1 < nrows && o[r + 1] - g0 <= j) ++r;
-                    const int b = (int)rb[j], e = (int)re[j];
-                    const bool first = j == o[r] - g0;
-                    if (!(b < e) || (!first && !((int)re[j - 1] < b)) || o[r] - g0 > j) bad = true;
+                const bool in = j < n[l];
+                const int b = in ? (int)rb[j] : 0, e = in ? (int)re[j] : 0;
+                int r = 0;
+#pragma unroll
+                for (int i = 0; i < 7; ++i) r += j >= rs[i] ? 1 : 0;
+                int rprev = __shfl_up_sync(0xFFFFFFFFu, r, 1);
+                int eprev = __shfl_up_sync(0xFFFFFFFFu, e, 1);
+                if (lane == 0) {
+                    rprev = carry_r;
+                    eprev = carry_e;
+                }
+                const bool first = r != rprev;
+                if (in && (!(b < e) || (!first && !(eprev < b)))) bad = true;
+                if (in) {
                     const unsigned rk = (unsigned)r << SXW16_XBITS;
                     rb[j] = (rk | ((unsigned)(b - xmin) & SXW16_XMASK)) |
                             ((rk | ((unsigned)(e - xmin) & SXW16_XMASK)) << 16);
                 }
-                rc = __shfl_sync(0xFFFFFFFFu, r, 31);
+                carry_r = __shfl_sync(0xFFFFFFFFu, r, 31);
+                carry_e = __shfl_sync(0xFFFFFFFFu, e, 31);
             }
             if (lane == 0) rb[n[l]] = 0xFFFFFFFFu;  // the list's sentinel
         }
