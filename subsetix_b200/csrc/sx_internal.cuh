@@ -30,15 +30,16 @@ struct SxBoolArgs {
     int* result;  // written by the last block: [0] total intervals, [1] SXF_* flags
     SxScanState scan;
     // launch tuning (0 = automatic): kernel 1 = global-memory sweep, 2 = staged
-    // sweep, 3 = merge-path tiles, 4 = segmented sweep (the default for
-    // tables); blocks_per_sm caps residency (via shared-memory padding);
-    // staging_cap is the staged kernel's per-warp element capacity, or keys
-    // per tile for kernels 3 and 4
+    // sweep, 3 = merge-path tiles, 4 = segmented sweep in block tiles, 5 =
+    // segmented sweep in warp tiles (the default for tables), 6 = kernel 5
+    // with 16-bit keys; blocks_per_sm caps residency (via shared-memory
+    // padding); staging_cap is the staged kernel's per-warp element capacity,
+    // or boundaries per tile for kernels 3 to 6
     int tune_kernel;
     int tune_blocks_per_sm;
     int tune_staging_cap;
-    int tune_warps;      // segmented sweep: warps per tile block
-    int tune_tile_rows;  // segmented sweep: rows per tile (16 or 32)
+    int tune_warps;      // segmented sweeps: warps per block
+    int tune_tile_rows;  // segmented sweeps: rows per tile (at most 32; 8 for kernel 6)
 };
 
 struct SxRowList {
