@@ -666,6 +666,23 @@ __device__ __forceinline__ SxRowReader sx_row_reader(int j, int je, const int* _
     return r;
 }
 
+// Value index of column x in the reader's row (advancing the reader), or
+// -1 when x is outside the row's intervals, the domain or the active cells.
+__device__ __forceinline__ int sx_row_index(SxRowReader& r, int x, int width, const int* __restrict__ b,
+                                            const int* __restrict__ e, const int* __restrict__ coff, bool act)
+{
+    while (r.j < r.je && r.ce <= x) {
+        ++r.j;
+        if (r.j < r.je) {
+            r.cb = b[r.j];
+            r.ce = e[r.j];
+            r.cc = coff[r.j];
+        }
+    }
+    if (!act || r.j >= r.je || r.cb > x || x < 0 || x >= width) return -1;
+    return r.cc + (x - r.cb);
+}
+
 template <typename T>
 __device__ __forceinline__ T sx_row_take(SxRowReader& r, int x, int width, const int* __restrict__ b,
                                          const int* __restrict__ e, const int* __restrict__ coff,
@@ -752,6 +769,21 @@ __global__ void __launch_bounds__(256) sx_upwind_chunk_kernel(const int* __restr
         }
         SxRowReader dn{p1.x, p1.y, p1.z, p1.w, p2.x};
         SxRowReader upc{p2.y, p2.z, p2.w, p3.x, p3.y};
+        // neighbour-row value indices of all four sub-rounds first, then all
+        // their loads at once, so the chunk waits for one round trip
+        int idn[SX_CHUNK_SUB], iup[SX_CHUNK_SUB];
+#pragma unroll
+        for (int q = 0; q < SX_CHUNK_SUB; ++q) {
+            const int x = x0 + 32 * q + lane;
+            idn[q] = sx_row_index(dn, x, width, b, e, coff, x < ie);
+            iup[q] = sx_row_index(upc, x, width, b, e, coff, x < ie);
+        }
+        T vdn[SX_CHUNK_SUB], vup[SX_CHUNK_SUB];
+#pragma unroll
+        for (int q = 0; q < SX_CHUNK_SUB; ++q) {
+            vdn[q] = idn[q] >= 0 ? v[idn[q]] : (T)0;
+            vup[q] = iup[q] >= 0 ? v[iup[q]] : (T)0;
+        }
         T prev_last = (T)0;  // lane 31's centre of the previous sub-round
 #pragma unroll
         for (int q = 0; q < SX_CHUNK_SUB; ++q) {
@@ -772,8 +804,8 @@ __global__ void __launch_bounds__(256) sx_upwind_chunk_kernel(const int* __restr
             else left = (act && (touch & 1) && lin) ? v[c - 1] : (T)0;
             if (x + 1 < ie) right = rin ? ((lane < 31 || q + 1 < SX_CHUNK_SUB) ? from_right : v[c + 1]) : (T)0;
             else right = (act && (touch & 2) && rin) ? v[c + 1] : (T)0;
-            const T down = sx_row_take<T>(dn, x, width, b, e, coff, v, act);
-            const T up = sx_row_take<T>(upc, x, width, b, e, coff, v, act);
+            const T down = vdn[q];
+            const T up = vup[q];
             if (act) {
                 const T du_dx = a >= (T)0 ? sx_over(sx_sub(center, left), dx, pow2) : sx_over(sx_sub(right, center), dx, pow2);
                 const T du_dy = bb >= (T)0 ? sx_over(sx_sub(center, down), dy, pow2) : sx_over(sx_sub(up, center), dy, pow2);
@@ -817,7 +849,25 @@ __global__ void __launch_bounds__(256) sx_upwind_adjoint_chunk_kernel(const int*
         }
         SxRowReader dn{p1.x, p1.y, p1.z, p1.w, p2.x};
         SxRowReader upr{p2.y, p2.z, p2.w, p3.x, p3.y};
-        SxRowReader dn2 = dn, up2 = upr;
+        // neighbour-row value indices of all four sub-rounds first, then all
+        // their loads at once.  u reads need the forward's domain test (made by
+        // the index), w reads need this cell's domain as well (jdom).
+        const bool rdom = row >= 0 && row < height;
+        int idn[SX_CHUNK_SUB], iup[SX_CHUNK_SUB];
+#pragma unroll
+        for (int q = 0; q < SX_CHUNK_SUB; ++q) {
+            const int x = x0 + 32 * q + lane;
+            idn[q] = sx_row_index(dn, x, width, b, e, coff, x < ie);
+            iup[q] = sx_row_index(upr, x, width, b, e, coff, x < ie);
+        }
+        T wdn[SX_CHUNK_SUB], wup[SX_CHUNK_SUB], udn[SX_CHUNK_SUB], uup[SX_CHUNK_SUB];
+#pragma unroll
+        for (int q = 0; q < SX_CHUNK_SUB; ++q) {
+            udn[q] = idn[q] >= 0 ? u[idn[q]] : (T)0;
+            uup[q] = iup[q] >= 0 ? u[iup[q]] : (T)0;
+            wdn[q] = idn[q] >= 0 && rdom ? w[idn[q]] : (T)0;
+            wup[q] = iup[q] >= 0 && rdom ? w[iup[q]] : (T)0;
+        }
         T wprev = (T)0, uprev = (T)0;
 #pragma unroll
         for (int q = 0; q < SX_CHUNK_SUB; ++q) {
@@ -862,10 +912,7 @@ __global__ void __launch_bounds__(256) sx_upwind_adjoint_chunk_kernel(const int*
             }
             // rows above and below: w in-set needs jdom only (x is then inside the domain, so the
             // reader's domain test is the same), u needs the forward's domain test
-            const T w_dn = sx_row_take<T>(dn, x, width, b, e, coff, w, act && jdom);
-            const T w_up = sx_row_take<T>(upr, x, width, b, e, coff, w, act && jdom);
-            const T u_dn = sx_row_take<T>(dn2, x, width, b, e, coff, u, act);
-            const T u_up = sx_row_take<T>(up2, x, width, b, e, coff, u, act);
+            const T w_dn = wdn[q], w_up = wup[q], u_dn = udn[q], u_up = uup[q];
             if (act) {
                 const T c_w = wc[q];
                 T tx, ty;
