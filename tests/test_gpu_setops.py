@@ -304,3 +304,35 @@ def test_tile_boundaries_max(cuda_device):
             if lo is not None:
                 span = max(span, int(hi) - int(lo))
         assert stats[2] == span, (a, b)
+
+
+MANY = {
+    6: ("symmetric_difference", ("difference", ("union", "A", "B"), ("intersection", "C", "D")),
+        ("difference", "E", "F")),
+    7: ("symmetric_difference", ("difference", ("union", "A", "B"), ("intersection", "C", "D")),
+        ("union", ("difference", "E", "F"), "G")),
+    8: ("symmetric_difference", ("difference", ("union", "A", "B"), ("intersection", "C", "D")),
+        ("union", ("difference", "E", "F"), ("intersection", "G", "H"))),
+}
+
+
+@pytest.mark.parametrize("k", [6, 7, 8])
+@pytest.mark.parametrize("tuning", [{}, {"kernel": 3}, {"kernel": 4}, {"kernel": 5}, {"kernel": 6}])
+def test_many_leaf_expressions(cuda_device, k, tuning):
+    # six to eight leaves: the truth table spans several words
+    from subsetix_b200 import _core
+
+    rng = np.random.default_rng(100 + k)
+    names = "ABCDEFGH"[:k]
+    hs = [_random_canonical(rng, 1500, 0, 6.0) for _ in names]
+    leaves_h = {n: iset(h) for n, h in zip(names, hs)}
+    leaves_d = {n: dev_set(h) for n, h in zip(names, hs)}
+    saved = dict(_core.TUNING)
+    try:
+        _core.TUNING.clear()
+        _core.TUNING.update(tuning)
+        got = sc.evaluate(_build(MANY[k], leaves_d))
+    finally:
+        _core.TUNING.clear()
+        _core.TUNING.update(saved)
+    assert_same(got, O.evaluate(MANY[k], leaves_h), f"k={k} {tuning}")
