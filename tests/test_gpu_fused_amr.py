@@ -157,3 +157,19 @@ def test_power_of_two_spacing_matches_division(cuda_device, res):
     eng = FusedTwoLevelAMR(torch.as_tensor(u0, device="cuda"), velocity=(0.9, -0.4), cfl=0.5, dtype=torch.float64)
     eng.run(6, regrid_every=3)
     np.testing.assert_array_equal(_vals(eng.fine_values).reshape(-1), ref.fine.values)
+
+
+@pytest.mark.parametrize("res", [40, 70, 300])
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+def test_fused_step_any_width(cuda_device, res, dtype):
+    # widths that leave partial warps and blocks: the one-kernel step equals the separate kernels
+    u0 = torch.as_tensor(_gauss(res, 0.07), device="cuda")
+    runs = []
+    for fused in (True, False):
+        eng = FusedTwoLevelAMR(u0, velocity=(0.8, -0.6), cfl=0.5, refine_threshold=0.05 / res, grading=1,
+                               dtype=dtype, fused=fused)
+        eng.run(9, regrid_every=4, graph=False)
+        runs.append(eng)
+    for lvl in ("coarse_values", "fine_values"):
+        assert torch.equal(getattr(runs[0], lvl), getattr(runs[1], lvl)), lvl
+
