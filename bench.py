@@ -257,14 +257,15 @@ def amr_section(device, steps: int = 200, every: int = 10, res: int = 1024, thre
     stream = torch.cuda.current_stream(device)
     runs = {}
     # "plain": separate upwind/upwind/sync launches, no graph; "graph": one fused
-    # step kernel per step, replayed from a CUDA graph
+    # step kernel per step, each regrid period (regrid + `every` steps) replayed
+    # as one CUDA graph
     for name, dtype, graph in (("fp32_graph", torch.float32, True), ("fp64_plain", torch.float64, False),
                                ("fp64_graph", torch.float64, True), ("fp32_plain", torch.float32, False)):
         warm = make(dtype, graph)
         warm.run(3 * every, every, graph=graph)
         eng = make(dtype, graph)
         if graph:
-            eng.prepare_graphs()
+            eng.prepare_graphs(every)
         mass0 = float(eng.mass()[0])
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

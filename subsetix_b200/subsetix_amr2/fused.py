@@ -175,13 +175,47 @@ class FusedTwoLevelAMR:
             self._graphs[key] = g
         return g
 
+    def _period_graph(self, period: int, parity: int) -> torch.cuda.CUDAGraph:
+        """One graph for a whole regrid period: the regrid and ``period`` steps, from ping-pong side ``parity``."""
+        key = ("period", period, parity)
+        g = self._graphs.get(key)
+        if g is None:
+            saved = self.cur
+            self.cur = parity
+            s = torch.cuda.Stream(device=self.device)
+            s.wait_stream(torch.cuda.current_stream(self.device))
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.stream(s):
+                with torch.cuda.graph(g, stream=s):
+                    for i in range(period):
+                        self._step_body(i == 0)
+            torch.cuda.current_stream(self.device).wait_stream(s)
+            self.cur = saved
+            self._graphs[key] = g
+        return g
+
     def run(self, steps: int, regrid_every: int = 1, graph: bool = True) -> None:
-        """Advance ``steps`` steps.  With ``graph`` each step is one CUDA-graph replay."""
+        """Advance ``steps`` steps.
+
+        With ``graph``, every whole regrid period (the regrid and its
+        ``regrid_every`` steps) is one CUDA-graph replay, and the steps
+        outside whole periods are one replay each.  The launches, and so the
+        results, are the same as without graphs.
+        """
         period = max(1, int(regrid_every))
         if not self._synced:
             self._sync()
             self._synced = True
-        for _ in range(int(steps)):
+        left = int(steps)
+        while left > 0:
+            if graph and period > 1 and self.step_count % period == 0 and left >= period:
+                self._period_graph(period, self.cur).replay()
+                self.cur ^= period & 1
+                for _ in range(period):
+                    self.step_count += 1
+                    self.time += self.dt
+                left -= period
+                continue
             regrid = self.step_count % period == 0
             if graph:
                 self._graph(regrid, self.cur).replay()
@@ -190,12 +224,18 @@ class FusedTwoLevelAMR:
                 self._step_body(regrid)
             self.step_count += 1
             self.time += self.dt
+            left -= 1
 
-    def prepare_graphs(self) -> None:
-        """Capture the four step graphs ahead of time (no work is done)."""
+    def prepare_graphs(self, regrid_every: Optional[int] = None) -> None:
+        """Capture the step graphs ahead of time (no work is done): the four
+        single-step graphs and, given ``regrid_every``, the two whole-period graphs."""
         for regrid in (False, True):
             for parity in (0, 1):
                 self._graph(regrid, parity)
+        period = max(1, int(regrid_every or 1))
+        if period > 1:
+            for parity in (0, 1):
+                self._period_graph(period, parity)
 
     # ---------------------------------------------------------------- results
     @property
