@@ -376,7 +376,7 @@ __global__ void __launch_bounds__(32 * SX_SWEEP_WARPS) sx_sweep_kernel(SxBoolArg
 }
 
 // ---------------------------------------------------------------------------
-// Shared-memory form of the table sweep (the main path for set algebra).
+// Shared-memory form of the table sweep (a tuning option, sx_tuning kernel 2).
 //
 // The warp stages its 32-row tile with coalesced loads.  Each leaf's
 // segment is stored interleaved, [b0, e0, b1, e1, ...], so a lane's
@@ -583,7 +583,7 @@ __global__ void __launch_bounds__(32 * SX_SMEM_WARPS) sx_sweep_smem_kernel(SxBoo
 static size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 // ---------------------------------------------------------------------------
-// Merge-path form of the table sweep (the main path for set algebra).
+// Merge-path form of the table sweep (a tuning option, sx_tuning kernel 3).
 //
 // A block of SXM_THREADS threads owns one tile of 32 aligned rows.  Every
 // boundary of every leaf in the tile becomes a key (row, x, leaf) in shared
@@ -1061,7 +1061,9 @@ __global__ void __launch_bounds__(SXM_THREADS) sx_merge_kernel(SxBoolArgs A, SxS
 }
 
 // ---------------------------------------------------------------------------
-// Segmented sweep: the default path for set algebra.
+// Segmented sweep in block tiles (sx_tuning kernel 4; the automatic choice
+// for skewed rows).  The warp-tile forms below (kernels 5 and 6) share its
+// algorithm and are the automatic choice for even rows.
 //
 // A block owns one tile of 32 aligned rows, as in the merge-path kernel.
 // Thread 0 copies every leaf's begin and end ranges of the tile into shared
