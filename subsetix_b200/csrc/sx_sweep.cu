@@ -1995,7 +1995,7 @@ __device__ __forceinline__ int sxs_lower_bound16(const unsigned short* k, int n,
 }
 
 template <int K>
-__global__ void __launch_bounds__(256) sx_wseg16_kernel(SxBoolArgs A, SxSweepState st, int tiles, int cap_words,
+__global__ void __launch_bounds__(256, K <= 5 ? 5 : 4) sx_wseg16_kernel(SxBoolArgs A, SxSweepState st, int tiles, int cap_words,
                                                         int tr)
 {
     extern __shared__ __align__(16) unsigned char sxw_smem[];
