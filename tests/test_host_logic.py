@@ -1,0 +1,119 @@
+"""Host-side logic that needs no GPU: argument checks of the C ABI, tuning
+candidates, workload keys, truth tables and the bench's byte count."""
+
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+from subsetix_b200 import _core, _lib, autotune
+
+
+def _lib_or_skip():
+    if not os.path.exists(_lib.LIB_PATH):
+        pytest.skip("library not built")
+    import torch
+
+    if torch.cuda.is_available():
+        # the calls below pass placeholder pointers and must fail their host checks; a
+        # machine with a GPU is not the place to find out whether one ever stops doing so
+        pytest.skip("host-check tests run only without a GPU")
+    return _lib.load()
+
+
+def _one_leaf():
+    arr = (_lib.SxLeaf * 1)()
+    arr[0].begin = 16
+    arr[0].end = 16
+    arr[0].row_offsets = 16  # never dereferenced: every call below fails its checks first
+    return arr
+
+
+@pytest.mark.parametrize("field,value", [("kernel", 7), ("kernel", -1), ("warps", 9), ("tile_rows", 33),
+                                         ("tile_rows", -2), ("staging_cap", -5), ("blocks_per_sm", -1)])
+def test_bool_eval_rejects_bad_tuning_on_the_host(field, value):
+    lib = _lib_or_skip()
+    tun = _lib.SxTuning(0, 0, 0, 0, 0)
+    setattr(tun, field, value)
+    tab = (ctypes.c_uint32 * 8)(0b1110, 0, 0, 0, 0, 0, 0, 0)
+    rows = 64
+    ws = lib.sx_bool_workspace_bytes(rows)
+    rc = lib.sx_bool_eval(_one_leaf(), 1, rows, tab, _lib.MODE_TABLE, 16, 16, 16, 100, 16, 16, ws,
+                          ctypes.byref(tun), None)
+    assert rc == _lib.SX_ERR_INVALID
+    assert "tuning" in _lib.last_error()
+
+
+def test_bool_eval_rejects_a_short_workspace_on_the_host():
+    lib = _lib_or_skip()
+    tab = (ctypes.c_uint32 * 8)(0b1110, 0, 0, 0, 0, 0, 0, 0)
+    rc = lib.sx_bool_eval(_one_leaf(), 1, 1 << 20, tab, _lib.MODE_TABLE, 16, 16, 16, 100, 16, 16, 64, None, None)
+    assert rc == _lib.SX_ERR_WORKSPACE
+
+
+def test_workspace_for_small_tiles_covers_32_row_tiles():
+    lib = _lib_or_skip()
+    for rows in (1, 31, 32, 33, 1000, 1 << 20):
+        assert lib.sx_bool_workspace_bytes(rows) >= lib.sx_bool_workspace_bytes(max(1, rows // 8))
+
+
+@pytest.mark.parametrize("k,rows,a,b", [(0, 8, 8, 32), (1, -1, 8, 32), (1, 8, 0, 32), (1, 8, 8, 0)])
+def test_tile_boundaries_max_rejects_bad_arguments(k, rows, a, b):
+    lib = _lib_or_skip()
+    rc = lib.sx_tile_boundaries_max(_one_leaf(), k, rows, a, b, 16, None)
+    assert rc == _lib.SX_ERR_INVALID
+
+
+def test_tile_boundaries_max_needs_offsets():
+    lib = _lib_or_skip()
+    arr = (_lib.SxLeaf * 1)()
+    assert lib.sx_tile_boundaries_max(arr, 1, 8, 8, 32, 16, None) == _lib.SX_ERR_INVALID
+    assert "offsets" in _lib.last_error()
+
+
+def test_workload_key_buckets():
+    assert _core.workload_key([100, 100], 64) == _core.workload_key([120, 90], 64)
+    assert _core.workload_key([100, 100], 64) != _core.workload_key([100, 100, 100], 64)
+    assert _core.workload_key([100], 64) != _core.workload_key([10000], 64)
+    assert autotune.workload_key is _core.workload_key
+
+
+def test_autotune_candidates_cover_every_kernel_kind():
+    sizes = [40000] * 5
+    cands = autotune.candidates(sizes, 4096, largest_tile=5000, largest_eighth_tile=1300)
+    kinds = {c["kernel"] for c in cands}
+    assert {1, 3, 4, 5, 6} <= kinds
+    for c in cands:
+        if c["kernel"] in (5, 6):
+            assert c["tile_rows"] == 8 and 1300 <= c["staging_cap"] <= 25000
+        if c["kernel"] == 4:
+            assert c["tile_rows"] == 32 and 5000 <= c["staging_cap"] <= 25000
+
+
+def test_truth_tables_of_the_binary_operations():
+    from subsetix_b200.subsetix_cupy import expressions as E
+
+    words = {"union": 0b1110, "intersection": 0b1000, "difference": 0b0010, "symmetric_difference": 0b0110}
+    for op, word in words.items():
+        node = E._remap((op, ("leaf", 0), ("leaf", 1)), {0: 0, 1: 1})
+        assert int(E.truth_table(node, 2)[0]) == word, op
+
+
+def test_truth_table_of_eight_leaves_spans_words():
+    from subsetix_b200.subsetix_cupy import expressions as E
+
+    node = E._remap(("union", ("leaf", 7), ("intersection", ("leaf", 0), ("leaf", 1))), {i: i for i in range(8)})
+    table = [int(x) for x in E.truth_table(node, 8)]
+    for state in range(256):
+        want = bool(state & 0x80) or (bool(state & 1) and bool(state & 2))
+        assert bool((table[state >> 5] >> (state & 31)) & 1) == want, state
+
+
+def test_algorithmic_bytes_counts_inputs_once_and_the_output_once():
+    import bench
+
+    leaf = (np.zeros(10, np.int32), np.zeros(10, np.int32), np.zeros(5, np.int32), np.zeros(4, np.int32))
+    got = bench.algorithmic_bytes([leaf, leaf], n_out=7, r_out=4)
+    want = 2 * (8 * 10 + 4 * 5 + 4 * 4) + 8 * 7 + 4 * 5 + 4 * 4
+    assert got == want
