@@ -108,7 +108,8 @@ def bool_eval(leaves: Sequence[Tuple[torch.Tensor, torch.Tensor, torch.Tensor, i
         need8, need32, span8 = tile_stats(leaves, rows, device, 8, 32)
         mean8 = 2 * sum(int(leaf[0].numel()) for leaf in leaves) / max(1, (rows + 7) // 8)
         if need8 <= 3 * mean8 + 256:
-            tuning = {"kernel": 6 if span8 <= 8190 else 5, "staging_cap": min(need8, 25000), "tile_rows": 8}
+            tuning = {"kernel": 6 if span8 <= 8190 else 5, "staging_cap": min(need8, 25000), "tile_rows": 8,
+                      "warps": 2}
         else:
             tuning = {"kernel": 4, "staging_cap": min(need32, 25000), "tile_rows": 32, "warps": 4}
     ob, oe, ooff, result = bool_eval_async(leaves, rows, table, mode, device, out, tuning=tuning)
