@@ -20,9 +20,8 @@ evaluation and download (`e2e.serial` runs them one at a time).
 Multi-GPU: every rank evaluates its own batch (weak scaling, no
 collective).  Times are the max over ranks.
 
-`--impl reference` times the reference algorithm on the host CPU: the
-reference's own kernel code compiled for the host (oracle/_ref) when
-available, else the oracle port.  It reports the same metric and config.
+`--impl reference` times the reference algorithm on the host CPU (the
+oracle port, all host threads).  It reports the same metric and config.
 """
 
 from __future__ import annotations
@@ -169,32 +168,20 @@ def traffic_per_launch(copies: int, kernel: str = "sx_wseg_kernel<5>"):
 
 
 def cpu_baseline(leaves_host, seconds: float, use_ref: bool):
-    """Time the host implementation on a bounded sample (whole copies of the workload)."""
+    """Time the host implementation (the oracle port, all host threads) on a bounded sample
+    (whole copies of the workload).  ``use_ref`` is kept for the call sites: the reference is
+    a CuPy package with no host implementation of its own to run on the GPU box."""
     from oracle import oracle as O
 
-    runner = None
     kind = "port"
     cores = O.threads()
-    if use_ref:
-        try:
-            from oracle import ref_runner
-
-            if ref_runner.available():
-                runner = ref_runner
-                kind = "reference"
-                cores = ref_runner.threads()
-        except Exception:
-            runner = None
     one = [tuple(a for a in leaf) for leaf in leaves_host]
     leaves = {n: O.ISet(*h) for n, h in zip("ABCDE", one)}
     n_in = sum(int(h[0].size) for h in one)
     done = 0
     t0 = time.perf_counter()
     while True:
-        if runner is not None:
-            runner.evaluate(SPEC, leaves)
-        else:
-            O.evaluate(SPEC, leaves)
+        O.evaluate(SPEC, leaves)
         done += 1
         if time.perf_counter() - t0 >= seconds:
             break
