@@ -430,6 +430,36 @@ int sx_value_runs(int type, const void* values, const int32_t* cell_offsets, int
 int sx_gather_i32(const int32_t* index, int32_t count, const int32_t* src, int32_t* dst, void* stream);
 
 /* ---------------------------------------------------------------------------
+ * Coupling of nested levels by index tables, for the composite multi-level
+ * advection and its adjoint (subsetix_b200/adjoint.py).  dtype SX_F32 or
+ * SX_F64; index tables are int32 positions into value arrays.
+ *   sx_index_copy            dst[dst_idx[i]] = src[src_idx[i]], i < n (a null
+ *                            table means the identity): ghost cells take their
+ *                            coarse parent's value, the injection of
+ *                            prolong_field (subsetix_cupy/multilevel.py:365-407);
+ *   sx_index_block_mean      out[out_idx[j]] = (sum over m < group, in order, of
+ *                            in[in_idx[j*group+m]]) * norm: restrict_field's
+ *                            mean (multilevel.py:410-479, kernels.py:458-527);
+ *   sx_index_block_mean_adj  the transpose: in_bar[in_idx[j*group+m]] +=
+ *                            out_bar[out_idx[j]] * norm, then out_bar[out_idx[j]]
+ *                            = 0; in_idx entries must be distinct;
+ *   sx_index_segment_add     dst[dst_idx[s]] += sum over t in [seg_off[s],
+ *                            seg_off[s+1]) of src[src_idx[t]], in order, and
+ *                            src[src_idx[t]] = 0 when zero_src: the transpose
+ *                            of sx_index_copy when parents repeat.
+ * The reference has no multi-level coupling of this form (its AMR driver has
+ * two whole-grid levels) and no derivatives.
+ * ------------------------------------------------------------------------- */
+int sx_index_copy(int dtype, int64_t n, const int32_t* dst_idx, const int32_t* src_idx, const void* src, void* dst,
+                  void* stream);
+int sx_index_block_mean(int dtype, int64_t n, int32_t group, double norm, const int32_t* out_idx,
+                        const int32_t* in_idx, const void* in, void* out, void* stream);
+int sx_index_block_mean_adj(int dtype, int64_t n, int32_t group, double norm, const int32_t* out_idx,
+                            const int32_t* in_idx, void* out_bar, void* in_bar, void* stream);
+int sx_index_segment_add(int dtype, int64_t nseg, const int32_t* seg_off, const int32_t* src_idx,
+                         const int32_t* dst_idx, void* src, void* dst, int zero_src, void* stream);
+
+/* ---------------------------------------------------------------------------
  * Two-level AMR on full grids, batched: arrays are [batch][height][width]
  * (coarse) and [batch][height*ratio][width*ratio] (fine).  In the
  * reference's AMR2Simulation both levels are full rectangles, and these are

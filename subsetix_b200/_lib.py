@@ -132,6 +132,13 @@ _SIGNATURES = {
     "sx_value_runs": (ctypes.c_int, [ctypes.c_int, c_vp, c_vp, ctypes.c_int64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
                                      c_vp]),
     "sx_gather_i32": (ctypes.c_int, [c_vp, ctypes.c_int32, c_vp, c_vp, c_vp]),
+    "sx_index_copy": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "sx_index_block_mean": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, ctypes.c_int32, ctypes.c_double, c_vp, c_vp,
+                                           c_vp, c_vp, c_vp]),
+    "sx_index_block_mean_adj": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, ctypes.c_int32, ctypes.c_double, c_vp,
+                                               c_vp, c_vp, c_vp, c_vp]),
+    "sx_index_segment_add": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.c_int,
+                                            c_vp]),
     "sx_upwind_full": (ctypes.c_int, [ctypes.c_int, c_vp, c_vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                       ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                       ctypes.c_double, c_vp]),

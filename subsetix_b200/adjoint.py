@@ -10,13 +10,24 @@ the velocity (time step held fixed).  Forward states are kept only every
 its checkpoint, so memory holds ``steps / checkpoint_every + checkpoint_every``
 states per level instead of ``steps``.
 
+``advect_composite`` couples nested levels the way a composite AMR step does
+(:class:`Hierarchy`): before each step the ghost ring of every finer level
+takes its coarse parents' values (injection), every level is advanced on its
+cells plus that ring, and after the step the coarse cells under a finer level
+take the mean of their children (restriction, finest level first).  Each
+coupling is a gather or a block mean over index tables built once for the
+fixed geometry (``sx_index_copy``, ``sx_index_block_mean``); the backward
+pass applies their transposes (``sx_index_segment_add``,
+``sx_index_block_mean_adj``) around the adjoint upwind kernel, in reverse
+order.
+
 There is no counterpart in the reference, which has no derivatives.
 """
 
 from __future__ import annotations
 
 from dataclasses import dataclass
-from typing import List, Sequence, Tuple
+from typing import List, Optional, Sequence, Tuple
 
 import torch
 
@@ -154,4 +165,253 @@ def advect(velocity: torch.Tensor, levels: Sequence[Level], u0: Sequence[torch.T
     return _Advect.apply(velocity, tuple(levels), float(dt), int(steps), int(checkpoint_every), *u0)
 
 
-__all__ = ["Level", "advect"]
+# ---------------------------------------------------------------------------------------------------------------
+# Nested levels coupled by ghost filling and restriction
+# ---------------------------------------------------------------------------------------------------------------
+
+def _cells(s: IntervalSet, cell_off: torch.Tensor):
+    """(rows, cols) of every cell of ``s`` in value order, as int32 device tensors."""
+    b, e, off, rows = _t(s.begin), _t(s.end), _t(s.row_offsets), _t(s.rows)
+    n = int(b.numel())
+    total = int(cell_off[-1].item()) if n else 0
+    dev = off.device
+    if total == 0:
+        z = torch.zeros(0, dtype=torch.int32, device=dev)
+        return z, z.clone()
+    iv = torch.repeat_interleave(torch.arange(n, device=dev), (e - b).to(torch.int64))
+    x = b[iv] + (torch.arange(total, device=dev, dtype=torch.int32) - cell_off[:-1][iv])
+    irow = torch.repeat_interleave(rows, (off[1:] - off[:-1]).to(torch.int64))
+    return irow[iv].to(torch.int32), x.to(torch.int32)
+
+
+def _positions(s: IntervalSet, cell_off: torch.Tensor, rows: torch.Tensor, cols: torch.Tensor) -> torch.Tensor:
+    """Value index of each cell (rows, cols) in a field on ``s``; -1 where the cell is not in ``s``."""
+    from .subsetix_cupy.interval_field import IntervalField, locate_interval_cells
+
+    if rows.numel() == 0:
+        return rows.clone()
+    f = IntervalField(interval_set=s, values=torch.empty(0, device=rows.device), interval_cell_offsets=cell_off)
+    iv = torch.as_tensor(locate_interval_cells(f, rows, cols)).to(torch.int64)
+    found = iv >= 0
+    ivc = iv.clamp_min(0)
+    pos = cell_off[ivc].to(torch.int64) + (cols.to(torch.int64) - _t(s.begin)[ivc].to(torch.int64))
+    return torch.where(found, pos, torch.full_like(pos, -1)).to(torch.int32)
+
+
+class Hierarchy:
+    """Nested interval sets on grids refined by ``ratio`` per level, coupled as a composite AMR step.
+
+    ``sets[k]`` lies in the ``(width * ratio**k) x (height * ratio**k)`` grid
+    of level ``k``.  Every finer level needs its ghost ring (the cells next
+    to it, left/right/below/above, inside the grid) to have parents in the
+    coarser level's set, and every coarse cell under it to have all its
+    ``ratio x ratio`` children in it; building a level from the prolongation
+    of a coarse set that keeps a one-cell margin satisfies both.  Fields
+    given to and returned by :func:`advect_composite` hold the cells of
+    ``sets[k]`` in their usual order.
+    """
+
+    def __init__(self, sets: Sequence[IntervalSet], width: int, height: int, *, ratio: int = 2,
+                 extent: Tuple[float, float] = (1.0, 1.0)):
+        from .subsetix_cupy import (clip_interval_set, dilate_interval_set, evaluate, make_input, make_union,
+                                    restrict_set)
+
+        if not sets:
+            raise ValueError("a hierarchy needs at least one level")
+        self.ratio = r = int(ratio)
+        if r < 2:
+            raise ValueError("levels must be refined by a ratio of at least 2")
+        self.levels: List[Level] = []
+        self.inner: List[torch.Tensor] = []
+        self.inner_cells: List[int] = []
+        self.ghost: List[Optional[tuple]] = []
+        self.cover: List[Optional[tuple]] = []
+        for k, s in enumerate(sets):
+            W, H = int(width) * r ** k, int(height) * r ** k
+            if k == 0:
+                ext = s
+            else:
+                cross = evaluate(make_union(make_input(dilate_interval_set(s, 1, 0)),
+                                            make_input(dilate_interval_set(s, 0, 1))))
+                ext = clip_interval_set(cross, width=W, height=H)
+            lvl = Level(ext, W, H, extent[0] / W, extent[1] / H)
+            self.levels.append(lvl)
+            s_off, _ = _core.cell_offsets(_t(s.begin), _t(s.end), lvl.device)
+            ys, xs = _cells(s, s_off)
+            inner = _positions(ext, lvl.cell_off, ys, xs)
+            if bool((inner < 0).any()):
+                raise ValueError(f"level {k}: the set is not inside its grid")
+            self.inner.append(inner)
+            self.inner_cells.append(int(inner.numel()))
+            if k == 0:
+                self.ghost.append(None)
+                self.cover.append(None)
+                continue
+            prev, prev_set = self.levels[k - 1], sets[k - 1]
+            # ghost ring: cells of the extended set outside the set, with their parents on level k-1
+            is_inner = torch.zeros(lvl.cells, dtype=torch.bool, device=lvl.device)
+            is_inner[inner.to(torch.int64)] = True
+            ey, ex = _cells(ext, lvl.cell_off)
+            gpos = torch.nonzero(~is_inner).reshape(-1).to(torch.int32)
+            py, px = torch.div(ey[gpos.to(torch.int64)], r, rounding_mode="floor"), \
+                torch.div(ex[gpos.to(torch.int64)], r, rounding_mode="floor")
+            ppos = _positions(prev.interval_set, prev.cell_off, py.to(torch.int32), px.to(torch.int32))
+            p_set_off, _ = _core.cell_offsets(_t(prev_set.begin), _t(prev_set.end), lvl.device)
+            if bool((ppos < 0).any()) or bool((_positions(prev_set, p_set_off, py.to(torch.int32),
+                                                          px.to(torch.int32)) < 0).any()):
+                raise ValueError(f"level {k}: its ghost ring is not covered by level {k - 1}")
+            order = torch.argsort(ppos.to(torch.int64), stable=True)
+            sp = ppos[order]
+            uniq, counts = torch.unique_consecutive(sp, return_counts=True)
+            seg_off = torch.zeros(uniq.numel() + 1, dtype=torch.int32, device=lvl.device)
+            seg_off[1:] = torch.cumsum(counts, 0).to(torch.int32)
+            self.ghost.append((gpos.contiguous(), ppos.contiguous(), seg_off, gpos[order].contiguous(),
+                               uniq.to(torch.int32).contiguous()))
+            # restriction: coarse cells under level k and their r x r children (sub-row outer, column inner)
+            covered = restrict_set(s, r)
+            c_off, _ = _core.cell_offsets(_t(covered.begin), _t(covered.end), lvl.device)
+            cy, cx = _cells(covered, c_off)
+            cpos = _positions(prev.interval_set, prev.cell_off, cy, cx)
+            dy = torch.arange(r, device=lvl.device).repeat_interleave(r)
+            dx = torch.arange(r, device=lvl.device).repeat(r)
+            chy = (cy.to(torch.int64)[:, None] * r + dy[None, :]).reshape(-1).to(torch.int32)
+            chx = (cx.to(torch.int64)[:, None] * r + dx[None, :]).reshape(-1).to(torch.int32)
+            child = _positions(s, s_off, chy, chx)
+            if bool((cpos < 0).any()) or bool((child < 0).any()):
+                raise ValueError(f"level {k}: a coarse cell under it does not have all its children in it")
+            child = inner[child.to(torch.int64)]
+            self.cover.append((cpos.contiguous(), child.contiguous()))
+
+    # -- the coupled step and its transpose ------------------------------------------------------------------------
+    def _fill_ghosts(self, u: List[torch.Tensor]) -> None:
+        lib = _lib.load()
+        for k in range(1, len(self.levels)):
+            gpos, ppos = self.ghost[k][0], self.ghost[k][1]
+            _lib.check(lib.sx_index_copy(_code(u[k]), int(gpos.numel()), ptr(gpos), ptr(ppos), ptr(u[k - 1]),
+                                         ptr(u[k]), stream_handle(u[k].device)), "sx_index_copy")
+
+    def _restrict(self, u: List[torch.Tensor]) -> None:
+        lib = _lib.load()
+        r2 = self.ratio * self.ratio
+        for k in range(len(self.levels) - 1, 0, -1):
+            cpos, child = self.cover[k]
+            _lib.check(lib.sx_index_block_mean(_code(u[k]), int(cpos.numel()), r2, 1.0 / r2, ptr(cpos), ptr(child),
+                                               ptr(u[k]), ptr(u[k - 1]), stream_handle(u[k].device)),
+                       "sx_index_block_mean")
+
+    def step(self, u: List[torch.Tensor], a: float, b: float, dt: float) -> Tuple[List[torch.Tensor], List[torch.Tensor]]:
+        """One coupled step of the extended-level fields ``u``; returns (new fields, upwind inputs)."""
+        self._fill_ghosts(u)
+        new = [lvl.step(x, torch.empty_like(x), a, b, dt) for lvl, x in zip(self.levels, u)]
+        self._restrict(new)
+        return new, u
+
+    def step_adjoint(self, w: List[torch.Tensor], inputs: List[torch.Tensor], a: float, b: float, dt: float,
+                     grad_ab: torch.Tensor) -> List[torch.Tensor]:
+        """Transpose of :meth:`step` applied to ``w`` (modified); ``inputs`` are that step's upwind inputs."""
+        lib = _lib.load()
+        r2 = self.ratio * self.ratio
+        for k in range(1, len(self.levels)):
+            cpos, child = self.cover[k]
+            _lib.check(lib.sx_index_block_mean_adj(_code(w[k]), int(cpos.numel()), r2, 1.0 / r2, ptr(cpos),
+                                                   ptr(child), ptr(w[k - 1]), ptr(w[k]), stream_handle(w[k].device)),
+                       "sx_index_block_mean_adj")
+        w = [lvl.adjoint(x, u, a, b, dt, grad_ab) for lvl, x, u in zip(self.levels, w, inputs)]
+        for k in range(len(self.levels) - 1, 0, -1):
+            _, _, seg_off, src, dst = self.ghost[k]
+            _lib.check(lib.sx_index_segment_add(_code(w[k]), int(dst.numel()), ptr(seg_off), ptr(src), ptr(dst),
+                                                ptr(w[k]), ptr(w[k - 1]), 1, stream_handle(w[k].device)),
+                       "sx_index_segment_add")
+        return w
+
+    # -- fields on the sets <-> fields on the extended sets ----------------------------------------------------------
+    def extend(self, fields: Sequence[torch.Tensor]) -> List[torch.Tensor]:
+        out = []
+        lib = _lib.load()
+        for lvl, inner, f in zip(self.levels, self.inner, fields):
+            x = torch.zeros(lvl.cells, dtype=f.dtype, device=lvl.device)
+            f = f.contiguous()
+            _lib.check(lib.sx_index_copy(_code(x), int(inner.numel()), ptr(inner), None, ptr(f), ptr(x),
+                                         stream_handle(lvl.device)), "sx_index_copy")
+            out.append(x)
+        return out
+
+    def interior(self, fields: Sequence[torch.Tensor]) -> List[torch.Tensor]:
+        out = []
+        lib = _lib.load()
+        for inner, x in zip(self.inner, fields):
+            y = torch.empty(int(inner.numel()), dtype=x.dtype, device=x.device)
+            _lib.check(lib.sx_index_copy(_code(x), int(inner.numel()), None, ptr(inner), ptr(x), ptr(y),
+                                         stream_handle(x.device)), "sx_index_copy")
+            out.append(y)
+        return out
+
+
+def _code(t: torch.Tensor) -> int:
+    return _lib.SX_F64 if t.dtype == torch.float64 else _lib.SX_F32
+
+
+def _run_composite(h: Hierarchy, states: List[torch.Tensor], a: float, b: float, dt: float, n: int, keep: bool):
+    """``n`` coupled steps; with ``keep`` also the upwind inputs of every step."""
+    inputs = []
+    cur = list(states)
+    for _ in range(n):
+        cur, used = h.step(cur, a, b, dt)
+        if keep:
+            inputs.append(used)
+    return cur, inputs
+
+
+class _AdvectComposite(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, velocity: torch.Tensor, h: Hierarchy, dt: float, steps: int, every: int, *u0):
+        a, b = (float(v) for v in velocity.detach().cpu().tolist())
+        cur = h.extend([u.detach() for u in u0])
+        checkpoints = [[x.clone() for x in cur]]
+        done = 0
+        while done < steps:
+            n = min(every, steps - done)
+            cur, _ = _run_composite(h, cur, a, b, dt, n, keep=False)
+            done += n
+            if done < steps:
+                checkpoints.append([x.clone() for x in cur])
+        ctx.h, ctx.dt, ctx.steps, ctx.every, ctx.ab = h, dt, steps, every, (a, b)
+        ctx.checkpoints = checkpoints
+        ctx.vel = (velocity.dtype, velocity.device)
+        return tuple(h.interior(cur))
+
+    @staticmethod
+    def backward(ctx, *grad_out):
+        h, dt, steps, every = ctx.h, ctx.dt, ctx.steps, ctx.every
+        a, b = ctx.ab
+        zeros = [torch.zeros(n, dtype=c.dtype, device=c.device) for n, c in zip(h.inner_cells, ctx.checkpoints[0])]
+        w = h.extend([g if g is not None else z for g, z in zip(grad_out, zeros)])
+        grad_ab = torch.zeros(2, dtype=torch.float64, device=h.levels[0].device)
+        starts = list(range(0, steps, every))
+        for si in reversed(range(len(starts))):
+            n = min(every, steps - starts[si])
+            _, inputs = _run_composite(h, [x.clone() for x in ctx.checkpoints[si]], a, b, dt, n, keep=True)
+            for j in reversed(range(n)):
+                w = h.step_adjoint(w, inputs[j], a, b, dt, grad_ab)
+        ctx.checkpoints = None
+        grads = h.interior(w)
+        return (grad_ab.to(device=ctx.vel[1], dtype=ctx.vel[0]), None, None, None, None, *grads)
+
+
+def advect_composite(velocity: torch.Tensor, hierarchy: Hierarchy, u0: Sequence[torch.Tensor], *, dt: float,
+                     steps: int, checkpoint_every: int = 10) -> Tuple[torch.Tensor, ...]:
+    """``steps`` coupled steps of a :class:`Hierarchy`; differentiable in ``velocity`` (2 values) and ``u0``.
+
+    ``u0[k]`` holds the cells of level ``k``'s set; so does each returned field.
+    """
+    if len(u0) != len(hierarchy.levels):
+        raise ValueError("one initial field per level")
+    for k, (u, n) in enumerate(zip(u0, hierarchy.inner_cells)):
+        if int(u.numel()) != n:
+            raise ValueError(f"level {k}: expected {n} values, got {int(u.numel())}")
+    if steps < 0 or checkpoint_every < 1:
+        raise ValueError("steps must be >= 0 and checkpoint_every >= 1")
+    return _AdvectComposite.apply(velocity, hierarchy, float(dt), int(steps), int(checkpoint_every), *u0)
+
+
+__all__ = ["Level", "advect", "Hierarchy", "advect_composite"]

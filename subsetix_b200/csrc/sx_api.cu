@@ -683,6 +683,59 @@ int sx_gather_i32(const int32_t* index, int32_t count, const int32_t* src, int32
     return SX_OK;
 }
 
+static int coupling_check(const char* what, int dtype, long long n)
+{
+    if (dtype != SX_F32 && dtype != SX_F64) return fail(SX_ERR_INVALID, "%s: dtype must be SX_F32 or SX_F64", what);
+    if (n < 0) return fail(SX_ERR_INVALID, "%s: negative count", what);
+    return SX_OK;
+}
+
+int sx_index_copy(int dtype, int64_t n, const int32_t* dst_idx, const int32_t* src_idx, const void* src, void* dst,
+                  void* stream)
+{
+    if (int rc = coupling_check("sx_index_copy", dtype, n)) return rc;
+    if (n == 0) return SX_OK;
+    if (!src || !dst) return fail(SX_ERR_INVALID, "sx_index_copy: null value array");
+    cudaError_t err = sx_index_copy_launch(dtype, n, dst_idx, src_idx, src, dst, (cudaStream_t)stream);
+    return err == cudaSuccess ? SX_OK : cuda_fail(err, "sx_index_copy");
+}
+
+int sx_index_block_mean(int dtype, int64_t n, int32_t group, double norm, const int32_t* out_idx,
+                        const int32_t* in_idx, const void* in, void* out, void* stream)
+{
+    if (int rc = coupling_check("sx_index_block_mean", dtype, n)) return rc;
+    if (n == 0) return SX_OK;
+    if (group < 1) return fail(SX_ERR_INVALID, "sx_index_block_mean: group must be positive");
+    if (!out_idx || !in_idx || !in || !out) return fail(SX_ERR_INVALID, "sx_index_block_mean: null argument");
+    cudaError_t err = sx_index_block_mean_launch(dtype, n, group, norm, out_idx, in_idx, in, out, (cudaStream_t)stream);
+    return err == cudaSuccess ? SX_OK : cuda_fail(err, "sx_index_block_mean");
+}
+
+int sx_index_block_mean_adj(int dtype, int64_t n, int32_t group, double norm, const int32_t* out_idx,
+                            const int32_t* in_idx, void* out_bar, void* in_bar, void* stream)
+{
+    if (int rc = coupling_check("sx_index_block_mean_adj", dtype, n)) return rc;
+    if (n == 0) return SX_OK;
+    if (group < 1) return fail(SX_ERR_INVALID, "sx_index_block_mean_adj: group must be positive");
+    if (!out_idx || !in_idx || !out_bar || !in_bar)
+        return fail(SX_ERR_INVALID, "sx_index_block_mean_adj: null argument");
+    cudaError_t err =
+        sx_index_block_mean_adj_launch(dtype, n, group, norm, out_idx, in_idx, out_bar, in_bar, (cudaStream_t)stream);
+    return err == cudaSuccess ? SX_OK : cuda_fail(err, "sx_index_block_mean_adj");
+}
+
+int sx_index_segment_add(int dtype, int64_t nseg, const int32_t* seg_off, const int32_t* src_idx,
+                         const int32_t* dst_idx, void* src, void* dst, int zero_src, void* stream)
+{
+    if (int rc = coupling_check("sx_index_segment_add", dtype, nseg)) return rc;
+    if (nseg == 0) return SX_OK;
+    if (!seg_off || !src_idx || !dst_idx || !src || !dst)
+        return fail(SX_ERR_INVALID, "sx_index_segment_add: null argument");
+    cudaError_t err = sx_index_segment_add_launch(dtype, nseg, seg_off, src_idx, dst_idx, src, dst, zero_src,
+                                                  (cudaStream_t)stream);
+    return err == cudaSuccess ? SX_OK : cuda_fail(err, "sx_index_segment_add");
+}
+
 static int full_grid_check(const char* what, int W, int H, int batch)
 {
     if (W <= 0 || H <= 0 || batch <= 0) return fail(SX_ERR_INVALID, "%s: width, height and batch must be positive", what);

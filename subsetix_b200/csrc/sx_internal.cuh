@@ -153,3 +153,12 @@ cudaError_t sx_upwind_adjoint_chunk_launch(const int* off, const int* b, const i
                                            void* ubar, int width, int height, double a, double bb, double dt,
                                            double dx, double dy, int dbl, double* partial, double* grads,
                                            cudaStream_t stream);
+// Level coupling by index tables (sx_coupling.cu)
+cudaError_t sx_index_copy_launch(int dtype, long long n, const int* dst_idx, const int* src_idx, const void* src,
+                                 void* dst, cudaStream_t stream);
+cudaError_t sx_index_block_mean_launch(int dtype, long long n, int group, double norm, const int* out_idx,
+                                       const int* in_idx, const void* in, void* out, cudaStream_t stream);
+cudaError_t sx_index_block_mean_adj_launch(int dtype, long long n, int group, double norm, const int* out_idx,
+                                           const int* in_idx, void* out_bar, void* in_bar, cudaStream_t stream);
+cudaError_t sx_index_segment_add_launch(int dtype, long long nseg, const int* seg_off, const int* src_idx,
+                                        const int* dst_idx, void* src, void* dst, int zero_src, cudaStream_t stream);

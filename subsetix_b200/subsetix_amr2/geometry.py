@@ -1,8 +1,15 @@
 """Two-level AMR geometry (drop-in for ``subsetix_amr2.geometry``).
 
-Follows ``subsetix_amr2/geometry.py`` of the reference: the refine set,
-its prolongation (fine set) and the coarse-only remainder, all computed on
-the device with this package's set kernels.
+A :class:`TwoLevelGeometry` names four interval sets of a two-level layout on
+a regular ``width x height`` coarse grid (``subsetix_amr2/geometry.py:31-43``):
+the coarse domain, the refine region, the refine region prolonged to the fine
+grid, and the coarse cells outside the refine region.
+
+Here all four come from one :class:`~.fields.ActionField`, which keeps its
+int8 action bytes on the device and derives each set from them once
+(value runs of the REFINE bytes, their prolongation, and the runs of every
+other byte).  A geometry is therefore a cheap view of an action field, and
+rebuilding it after a regrid costs one pass over the action bytes.
 """
 
 from __future__ import annotations
@@ -10,29 +17,21 @@ from __future__ import annotations
 from dataclasses import dataclass
 from typing import TYPE_CHECKING, Optional
 
-from ..subsetix_cupy import (
-    CuPyWorkspace,
-    IntervalSet,
-    clip_interval_set,
-    dilate_interval_set,
-    evaluate,
-    make_difference,
-    make_input,
-    make_union,
-    prolong_set,
-)
+from ..subsetix_cupy import CuPyWorkspace, IntervalSet, evaluate, make_difference, make_input, prolong_set
 
 if TYPE_CHECKING:
     from .fields import ActionField
 
-
-def _clone_interval_set(interval_set: IntervalSet) -> IntervalSet:
-    return interval_set.copy()
+_MODES = ("von_neumann", "moore")
 
 
 @dataclass
 class TwoLevelGeometry:
-    """Coarse domain, refine region, fine region and coarse-only region (``geometry.py:34-124``)."""
+    """Coarse domain, refine region, fine region and coarse-only region of a two-level layout.
+
+    ``workspace`` is kept for callers that evaluate expressions against the
+    geometry's sets; the sets themselves never live in it.
+    """
 
     ratio: int
     width: int
@@ -46,40 +45,39 @@ class TwoLevelGeometry:
     @classmethod
     def from_action_field(cls, actions: "ActionField", *, workspace: Optional[CuPyWorkspace] = None
                           ) -> "TwoLevelGeometry":
-        if actions.height <= 0 or actions.width <= 0:
-            raise ValueError("action field must have positive dimensions")
-        workspace = workspace or CuPyWorkspace()
-        coarse = actions.coarse_interval_set()
-        refine = actions.refine_set()
-        fine = actions.fine_set()
-        coarse_only = evaluate(make_difference(make_input(coarse), make_input(refine)), workspace=workspace)
-        return cls(ratio=int(actions.ratio), width=actions.width, height=actions.height, coarse=coarse, refine=refine,
-                   fine=fine, coarse_only=coarse_only, workspace=workspace)
+        """Geometry of an action field (``geometry.py:45-70``): every set is the field's cached one."""
+        if min(int(actions.width), int(actions.height)) <= 0:
+            raise ValueError("an action field with an empty grid has no geometry")
+        return cls(ratio=int(actions.ratio), width=int(actions.width), height=int(actions.height),
+                   coarse=actions.coarse_interval_set(), refine=actions.refine_set(), fine=actions.fine_set(),
+                   coarse_only=actions.coarse_only_set(),
+                   workspace=workspace if workspace is not None else CuPyWorkspace())
 
     def with_action_field(self, actions: "ActionField") -> "TwoLevelGeometry":
-        return TwoLevelGeometry.from_action_field(actions, workspace=self.workspace)
+        """Geometry of ``actions`` that keeps this geometry's workspace (``geometry.py:72-81``)."""
+        return type(self).from_action_field(actions, workspace=self.workspace)
 
     def dilate_refine(self, halo: int = 1, *, mode: str = "von_neumann") -> "TwoLevelGeometry":
-        """Grow the refine region by ``halo`` cells and rebuild the geometry (``geometry.py:83-124``)."""
+        """Geometry whose refine region is grown by ``halo`` cells inside the domain (``geometry.py:83-124``).
+
+        Growing the refine region this way is the 2:1 grading step: a box
+        (``moore``) or a cross (``von_neumann``) dilation, united with the
+        region and clipped to the grid.  The grading routine computes exactly
+        that set, so it is reused here; the fine and coarse-only regions
+        follow from the grown set.  ``halo <= 0`` returns this geometry.
+        """
+        from .regrid import enforce_two_level_grading_set
+
         halo = int(halo)
         if halo <= 0:
             return self
-        if mode not in {"von_neumann", "moore"}:
-            raise ValueError("mode must be 'von_neumann' or 'moore'")
-        if mode == "moore":
-            dilated = dilate_interval_set(self.refine, halo_x=halo, halo_y=halo)
-        else:
-            horiz = dilate_interval_set(self.refine, halo_x=halo, halo_y=0)
-            vert = dilate_interval_set(self.refine, halo_x=0, halo_y=halo)
-            dilated = evaluate(make_union(make_input(horiz), make_input(vert)), workspace=self.workspace)
-        dilated = clip_interval_set(dilated, width=self.width, height=self.height)
-        refine_dense = clip_interval_set(self.refine, width=self.width, height=self.height)
-        merged = evaluate(make_union(make_input(dilated), make_input(refine_dense)), workspace=self.workspace)
-        clipped = clip_interval_set(merged, width=self.width, height=self.height)
-        fine = prolong_set(clipped, self.ratio)
-        coarse_only = evaluate(make_difference(make_input(self.coarse), make_input(clipped)), workspace=self.workspace)
+        if mode not in _MODES:
+            raise ValueError(f"unknown dilation mode {mode!r}; expected one of {_MODES}")
+        grown = enforce_two_level_grading_set(self.refine, padding=halo, mode=mode, width=self.width,
+                                              height=self.height)
+        rest = evaluate(make_difference(make_input(self.coarse), make_input(grown)))
         return TwoLevelGeometry(ratio=self.ratio, width=self.width, height=self.height, coarse=self.coarse,
-                                refine=clipped, fine=fine, coarse_only=_clone_interval_set(coarse_only),
+                                refine=grown, fine=prolong_set(grown, self.ratio), coarse_only=rest.copy(),
                                 workspace=self.workspace)
 
 

@@ -249,10 +249,13 @@ def full_interval_set(width: int, height: int) -> IntervalSet:
         z = torch.zeros(0, dtype=I32, device=device)
         return IntervalSet._trusted(z, z.clone(), torch.zeros(1, dtype=I32, device=device), z.clone())
     h = int(height)
-    return IntervalSet._trusted(torch.zeros(h, dtype=I32, device=device),
-                                torch.full((h,), int(width), dtype=I32, device=device),
-                                torch.arange(h + 1, dtype=I32, device=device),
-                                torch.arange(h, dtype=I32, device=device), h)
+    s = IntervalSet._trusted(torch.zeros(h, dtype=I32, device=device),
+                             torch.full((h,), int(width), dtype=I32, device=device),
+                             torch.arange(h + 1, dtype=I32, device=device),
+                             torch.arange(h, dtype=I32, device=device), h)
+    # Marks the set as the whole rectangle, so whole-grid fast paths need no device check.
+    object.__setattr__(s, "_full_width", int(width))
+    return s
 
 
 def _dense_empty(height: int, device, kind) -> IntervalSet:

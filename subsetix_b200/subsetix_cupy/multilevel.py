@@ -37,62 +37,65 @@ _REDUCER_CODES = {"mean": 0, "sum": 1, "min": 2, "max": 3}
 
 
 def _default_ratios(n_levels: int, base: int) -> List[int]:
+    """Ratios ``base**k`` of levels ``k = 0 .. n_levels-1`` relative to level 0."""
     if n_levels <= 0:
-        raise ValueError("n_levels must be > 0")
+        raise ValueError(f"a hierarchy needs at least one level, got {n_levels}")
     if base < 2:
-        raise ValueError("base ratio must be >= 2")
-    ratios = [1]
-    for _ in range(1, n_levels):
-        ratios.append(ratios[-1] * base)
-    return ratios
+        raise ValueError(f"the refinement factor between levels must be at least 2, got {base}")
+    return [int(base) ** k for k in range(int(n_levels))]
 
 
 def _validate_ratios(ratios: List[int]) -> None:
+    """Level 0 has ratio 1; each further ratio is a proper multiple of the one before."""
     if not ratios:
-        raise ValueError("ratios must be non-empty")
+        raise ValueError("a hierarchy needs at least one ratio")
     if ratios[0] != 1:
-        raise ValueError("ratios must start at 1 for the base level")
-    for i in range(1, len(ratios)):
-        if ratios[i] <= ratios[i - 1]:
-            raise ValueError("ratios must be strictly increasing")
-        if ratios[i] % ratios[i - 1] != 0:
-            raise ValueError("each ratio must be a multiple of the previous")
+        raise ValueError(f"level 0 must have ratio 1, got {ratios[0]}")
+    for k, (lo, hi) in enumerate(zip(ratios, ratios[1:]), start=1):
+        if hi <= lo:
+            raise ValueError(f"ratio of level {k} ({hi}) does not exceed that of level {k - 1} ({lo})")
+        if hi % lo:
+            raise ValueError(f"ratio of level {k} ({hi}) is not a multiple of that of level {k - 1} ({lo})")
+
+
+def _slot(items: list, level: int) -> int:
+    """``level`` checked against the number of slots (IndexError outside)."""
+    if not 0 <= level < len(items):
+        raise IndexError(f"level {level} outside 0..{len(items) - 1}")
+    return level
 
 
 @dataclass
 class MultiLevel2D:
-    """One optional :class:`IntervalSet` per level with ratios relative to level 0 (``multilevel.py:48-87``)."""
+    """One optional :class:`IntervalSet` per level, with each level's ratio to level 0 (``multilevel.py:48-87``)."""
 
     ratios: List[int]
     levels: List[Optional[IntervalSet]]
 
     @classmethod
     def create(cls, n_levels: int, base_ratio: int = 2) -> "MultiLevel2D":
-        return cls(ratios=_default_ratios(n_levels, base_ratio), levels=[None] * n_levels)
-
-    def validate(self) -> None:
-        _validate_ratios(self.ratios)
-        if len(self.levels) != len(self.ratios):
-            raise ValueError("levels and ratios must have the same length")
-
-    def set_level(self, level: int, interval_set: Optional[IntervalSet]) -> None:
-        if level < 0 or level >= len(self.levels):
-            raise IndexError("level out of range")
-        self.levels[level] = interval_set
-
-    def get_level(self, level: int) -> Optional[IntervalSet]:
-        if level < 0 or level >= len(self.levels):
-            raise IndexError("level out of range")
-        return self.levels[level]
+        ratios = _default_ratios(n_levels, base_ratio)
+        return cls(ratios=ratios, levels=[None for _ in ratios])
 
     @property
     def n_levels(self) -> int:
         return len(self.levels)
 
+    def validate(self) -> None:
+        _validate_ratios(self.ratios)
+        if len(self.levels) != len(self.ratios):
+            raise ValueError(f"{len(self.levels)} levels but {len(self.ratios)} ratios")
+
+    def set_level(self, level: int, interval_set: Optional[IntervalSet]) -> None:
+        self.levels[_slot(self.levels, level)] = interval_set
+
+    def get_level(self, level: int) -> Optional[IntervalSet]:
+        return self.levels[_slot(self.levels, level)]
+
 
 @dataclass
 class MultiLevelField2D:
-    """One optional :class:`IntervalField` per level (``multilevel.py:90-147``)."""
+    """One optional :class:`IntervalField` per level, on the ratios of a :class:`MultiLevel2D` (``multilevel.py:90-147``)."""
 
     ratios: List[int]
     fields: List[Optional[IntervalField]]
@@ -104,35 +107,32 @@ class MultiLevelField2D:
 
     @classmethod
     def create_from_geometry(cls, ml: MultiLevel2D, *, fill_value: float = 0.0, dtype=None) -> "MultiLevelField2D":
+        """A field on every level that has a set, filled with ``fill_value``."""
         ml.validate()
-        fields: List[Optional[IntervalField]] = []
-        for lvl in ml.levels:
-            fields.append(None if lvl is None else create_interval_field(lvl, fill_value=fill_value, dtype=dtype))
-        return cls(ratios=list(ml.ratios), fields=fields)
+        return cls(ratios=list(ml.ratios),
+                   fields=[s if s is None else create_interval_field(s, fill_value=fill_value, dtype=dtype)
+                           for s in ml.levels])
 
     def validate_against(self, ml: MultiLevel2D) -> None:
+        """Same ratios as ``ml``, and every field's row and interval counts equal to its level's set."""
         ml.validate()
         if len(self.fields) != ml.n_levels:
-            raise ValueError("field levels and geometry levels mismatch")
+            raise ValueError(f"{len(self.fields)} field levels for {ml.n_levels} geometry levels")
         if list(self.ratios) != list(ml.ratios):
-            raise ValueError("ratios mismatch between field and geometry")
-        for i, f in enumerate(self.fields):
-            s = ml.levels[i]
+            raise ValueError(f"field ratios {list(self.ratios)} differ from geometry ratios {list(ml.ratios)}")
+        for k, (f, s) in enumerate(zip(self.fields, ml.levels)):
             if f is None or s is None:
                 continue
-            if (int(f.interval_set.row_offsets.shape[0]) != int(s.row_offsets.shape[0])
-                    or int(f.interval_set.begin.shape[0]) != int(s.begin.shape[0])):
-                raise ValueError(f"level {i}: field geometry does not match IntervalSet")
+            fs = f.interval_set
+            if (int(fs.row_offsets.shape[0]), int(fs.begin.shape[0])) != (int(s.row_offsets.shape[0]),
+                                                                         int(s.begin.shape[0])):
+                raise ValueError(f"level {k}: the field's rows or intervals differ from the level's set")
 
     def set_level_field(self, level: int, field: Optional[IntervalField]) -> None:
-        if level < 0 or level >= len(self.fields):
-            raise IndexError("level out of range")
-        self.fields[level] = field
+        self.fields[_slot(self.fields, level)] = field
 
     def get_level_field(self, level: int) -> Optional[IntervalField]:
-        if level < 0 or level >= len(self.fields):
-            raise IndexError("level out of range")
-        return self.fields[level]
+        return self.fields[_slot(self.fields, level)]
 
 
 # ---------------------------------------------------------------------------
@@ -316,67 +316,61 @@ def restrict_field(field: IntervalField, ratio: int, *, reducer: str = "mean", d
 # Level helpers
 # ---------------------------------------------------------------------------
 
-def _level_ratio(ml: MultiLevel2D, level: int, what: str) -> int:
+def _pair_ratio(ml: MultiLevel2D, level: int, what: str) -> int:
+    """Ratio between ``level`` and ``level + 1`` of a valid hierarchy; IndexError when that pair does not exist."""
     ml.validate()
-    if level < 0 or level + 1 >= ml.n_levels:
-        raise IndexError(f"invalid level for {what}")
+    if not 0 <= level < ml.n_levels - 1:
+        raise IndexError(f"{what}: no level pair {level}/{level + 1} in {ml.n_levels} levels")
     return ml.ratios[level + 1] // ml.ratios[level]
 
 
+def _defined(x, what: str):
+    if x is None:
+        raise ValueError(f"{what} is not defined")
+    return x
+
+
 def prolong_level_sets(ml: MultiLevel2D, level: int) -> IntervalSet:
-    ratio = _level_ratio(ml, level, "prolongation")
-    base = ml.get_level(level)
-    if base is None:
-        raise ValueError("base level interval set is not defined")
-    fine = prolong_set(base, ratio)
-    ml.set_level(level + 1, fine)
-    return fine
+    """Set of ``level + 1`` := prolongation of the set of ``level`` (``multilevel.py:482-492``)."""
+    r = _pair_ratio(ml, level, "prolongation")
+    ml.set_level(level + 1, prolong_set(_defined(ml.get_level(level), "base level interval set"), r))
+    return ml.get_level(level + 1)
 
 
 def restrict_level_sets(ml: MultiLevel2D, level: int) -> IntervalSet:
-    ratio = _level_ratio(ml, level, "restriction")
-    fine = ml.get_level(level + 1)
-    if fine is None:
-        raise ValueError("fine level interval set is not defined")
-    coarse = restrict_set(fine, ratio)
-    ml.set_level(level, coarse)
-    return coarse
+    """Set of ``level`` := restriction of the set of ``level + 1`` (``multilevel.py:495-505``)."""
+    r = _pair_ratio(ml, level, "restriction")
+    ml.set_level(level, restrict_set(_defined(ml.get_level(level + 1), "fine level interval set"), r))
+    return ml.get_level(level)
 
 
 def prolong_level_field(ml: MultiLevel2D, mf: MultiLevelField2D, level: int) -> IntervalField:
-    ml.validate()
+    """Field of ``level + 1`` := injection of the field of ``level`` (``multilevel.py:508-519``)."""
     mf.validate_against(ml)
-    ratio = _level_ratio(ml, level, "prolongation")
-    base = mf.get_level_field(level)
-    if base is None:
-        raise ValueError("base level field is not defined")
-    fine = prolong_field(base, ratio)
-    mf.set_level_field(level + 1, fine)
-    return fine
+    r = _pair_ratio(ml, level, "prolongation")
+    mf.set_level_field(level + 1, prolong_field(_defined(mf.get_level_field(level), "base level field"), r))
+    return mf.get_level_field(level + 1)
 
 
 def restrict_level_field(ml: MultiLevel2D, mf: MultiLevelField2D, level: int, *, reducer: str = "mean"
                          ) -> IntervalField:
-    ml.validate()
+    """Field of ``level`` := ``reducer`` over the blocks of the field of ``level + 1`` (``multilevel.py:522-533``)."""
     mf.validate_against(ml)
-    ratio = _level_ratio(ml, level, "restriction")
-    fine = mf.get_level_field(level + 1)
-    if fine is None:
-        raise ValueError("fine level field is not defined")
-    coarse = restrict_field(fine, ratio, reducer=reducer)
-    mf.set_level_field(level, coarse)
-    return coarse
+    r = _pair_ratio(ml, level, "restriction")
+    fine = _defined(mf.get_level_field(level + 1), "fine level field")
+    mf.set_level_field(level, restrict_field(fine, r, reducer=reducer))
+    return mf.get_level_field(level)
 
 
 def covered_by_fine(ml: MultiLevel2D, level: int):
-    ratio = _level_ratio(ml, level, "covered_by_fine")
+    """Cells of ``level`` under the set of ``level + 1`` (its restriction), or None when that set is unset."""
+    r = _pair_ratio(ml, level, "covered_by_fine")
     fine = ml.get_level(level + 1)
-    if fine is None:
-        return None
-    return restrict_set(fine, ratio)
+    return None if fine is None else restrict_set(fine, r)
 
 
 def coarse_only(coarse_set: IntervalSet, ml: MultiLevel2D, level: int):
+    """``coarse_set`` minus the cells covered by ``level + 1`` (``coarse_set`` itself when nothing covers it)."""
     covered = covered_by_fine(ml, level)
     if covered is None or coarse_set is None:
         return coarse_set

@@ -255,3 +255,40 @@ def disk_rows(size: int, radius: float, cx: float | None = None, cy: float | Non
     rows = np.nonzero(keep)[0]
     off = np.arange(rows.size + 1, dtype=np.int64)
     return x0[keep].astype(np.int32), x1[keep].astype(np.int32), off.astype(np.int32), rows.astype(np.int32)
+
+
+def prolong_rows(s: HostSet, ratio: int) -> HostSet:
+    """``[b r, e r)`` on rows ``y r .. y r + r - 1`` for every row ``y`` of ``s`` (the set prolongation)."""
+    b, e, off, rows = s
+    r = int(ratio)
+    counts = np.diff(off.astype(np.int64))
+    fb, fe, frows, fcounts = [], [], [], []
+    for k, y in enumerate(rows):
+        lo, hi = int(off[k]), int(off[k + 1])
+        for d in range(r):
+            fb.append(b[lo:hi].astype(np.int64) * r)
+            fe.append(e[lo:hi].astype(np.int64) * r)
+            frows.append(int(y) * r + d)
+            fcounts.append(int(counts[k]))
+    fo = np.zeros(len(fcounts) + 1, np.int64)
+    np.cumsum(fcounts, out=fo[1:])
+    cat = (lambda xs: np.concatenate(xs) if xs else np.zeros(0, np.int64))
+    return (cat(fb).astype(np.int32), cat(fe).astype(np.int32), fo.astype(np.int32),
+            np.asarray(frows, np.int64).astype(np.int32))
+
+
+def nested_disk_levels(base: int, radii: Sequence[float], ratio: int = 2) -> List[HostSet]:
+    """Levels of a nested hierarchy: the whole ``base x base`` grid, then one disk per radius.
+
+    Level ``k >= 1`` is the disk of radius ``radii[k-1]`` (a fraction of the
+    domain side, centred) rasterised on level ``k-1``'s grid and prolonged by
+    ``ratio``, so that every coarse cell under it has all its children in it.
+    """
+    full = (np.zeros(base, np.int32), np.full(base, base, np.int32), np.arange(base + 1, dtype=np.int32),
+            np.arange(base, dtype=np.int32))
+    levels = [full]
+    n = base
+    for rad in radii:
+        levels.append(prolong_rows(disk_rows(n, rad * n), ratio))
+        n *= ratio
+    return levels

@@ -157,3 +157,185 @@ def test_chunked_adjoint_equals_generic(cuda_device, a, b):
                                      stream_handle(torch.device("cuda", 0))), "sx_upwind_adjoint")
     assert torch.equal(got, ref)
     assert torch.allclose(g_chunk, g_ref, rtol=1e-12, atol=0)
+
+
+# ---------------------------------------------------------------------------------------------------------------
+# Composite multi-level model: ghost filling from the coarser level, restriction onto it
+# ---------------------------------------------------------------------------------------------------------------
+
+def _hierarchy(base=24, radii=(0.3, 0.15)):
+    hosts = synth.nested_disk_levels(base, list(radii))
+    return adj.Hierarchy([dev_set(h) for h in hosts], base, base), hosts
+
+
+def _cells_of(h):
+    b, e, off, rows = h
+    ys, xs = [], []
+    for k, y in enumerate(rows):
+        for i in range(off[k], off[k + 1]):
+            x = np.arange(b[i], e[i])
+            xs.append(x)
+            ys.append(np.full(x.size, y))
+    return np.concatenate(ys), np.concatenate(xs)
+
+
+class _TorchComposite:
+    """FP64 restatement of the composite step with torch operations (the reference gradient).
+
+    Built from the host sets alone: each finer level is extended by its
+    cross-shaped ghost ring inside the grid, ghost cells take their parent's
+    value, every level takes an upwind step with zero outside its extended
+    set, and covered coarse cells take the mean of their children.
+    """
+
+    def __init__(self, hosts, base, ratio=2):
+        self.r = ratio
+        self.levels = []
+        for k, h in enumerate(hosts):
+            n = base * ratio ** k
+            ys, xs = _cells_of(h)
+            inner = set(zip(ys.tolist(), xs.tolist()))
+            cells = set(inner)
+            if k:
+                for y, x in inner:
+                    for dy, dx in ((0, 1), (0, -1), (1, 0), (-1, 0)):
+                        if 0 <= y + dy < n and 0 <= x + dx < n:
+                            cells.add((y + dy, x + dx))
+            order = sorted(cells)
+            index = {c: i for i, c in enumerate(order)}
+            nb = np.full((len(order), 4), -1, np.int64)
+            for i, (y, x) in enumerate(order):
+                for j, (dy, dx) in enumerate(((0, -1), (0, 1), (-1, 0), (1, 0))):
+                    nb[i, j] = index.get((y + dy, x + dx), -1)
+            inner_idx = np.array([index[(y, x)] for y, x in zip(ys.tolist(), xs.tolist())], np.int64)
+            lvl = dict(n=n, order=order, index=index, nb=torch.as_tensor(nb, device="cuda"),
+                       inner=torch.as_tensor(inner_idx, device="cuda"), inner_set=inner)
+            if k:
+                prev = self.levels[-1]
+                ghosts = [c for c in order if c not in inner]
+                lvl["gpos"] = torch.as_tensor([index[c] for c in ghosts], device="cuda")
+                lvl["gpar"] = torch.as_tensor([prev["index"][(y // ratio, x // ratio)] for y, x in ghosts],
+                                              device="cuda")
+                cov = sorted({(y // ratio, x // ratio) for y, x in inner})
+                lvl["cov"] = torch.as_tensor([prev["index"][c] for c in cov], device="cuda")
+                lvl["child"] = torch.as_tensor([[index[(Y * ratio + dy, X * ratio + dx)] for dy in range(ratio)
+                                                 for dx in range(ratio)] for Y, X in cov], device="cuda")
+            self.levels.append(lvl)
+
+    def _upwind(self, u, lvl, a, b, dt):
+        dx = 1.0 / lvl["n"]
+        nb = lvl["nb"]
+        z = torch.zeros(1, dtype=u.dtype, device=u.device)
+        ext = torch.cat([u, z])
+        left, right, down, up = (ext[torch.where(nb[:, j] >= 0, nb[:, j], u.numel())] for j in range(4))
+        dudx = (u - left) / dx if float(a) >= 0 else (right - u) / dx
+        dudy = (u - down) / dx if float(b) >= 0 else (up - u) / dx
+        return u - dt * (a * dudx + b * dudy)
+
+    def step(self, us, a, b, dt):
+        us = list(us)
+        for k in range(1, len(us)):
+            lvl = self.levels[k]
+            us[k] = us[k].index_put((lvl["gpos"],), us[k - 1][lvl["gpar"]])
+        us = [self._upwind(u, lvl, a, b, dt) for u, lvl in zip(us, self.levels)]
+        for k in range(len(us) - 1, 0, -1):
+            lvl = self.levels[k]
+            us[k - 1] = us[k - 1].index_put((lvl["cov"],), us[k][lvl["child"]].sum(dim=1) / (self.r * self.r))
+        return us
+
+    def run(self, u0, vel, dt, steps):
+        us = []
+        for u, lvl in zip(u0, self.levels):
+            x = torch.zeros(len(lvl["order"]), dtype=u.dtype, device=u.device)
+            us.append(x.index_put((lvl["inner"],), u))
+        for _ in range(steps):
+            us = self.step(us, vel[0], vel[1], dt)
+        return [u[lvl["inner"]] for u, lvl in zip(us, self.levels)]
+
+
+def _gauss_cells(h, n, cx, cy, sigma):
+    ys, xs = _cells_of(h)
+    x, y = (xs + 0.5) / n, (ys + 0.5) / n
+    return np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / (2 * sigma ** 2))
+
+
+def test_composite_step_matches_torch_restatement(cuda_device):
+    H, hosts = _hierarchy()
+    ref = _TorchComposite(hosts, 24)
+    rng = np.random.default_rng(2)
+    u0 = [torch.as_tensor(rng.standard_normal(n), device="cuda") for n in H.inner_cells]
+    dt = 0.5 / (1.5 * 96)
+    got = adj.advect_composite(torch.tensor([1.0, 0.5], dtype=torch.float64, device="cuda"), H, u0, dt=dt, steps=7)
+    want = ref.run(u0, (1.0, 0.5), dt, 7)
+    for g, w in zip(got, want):
+        assert float((g - w).abs().max()) <= 1e-12 * max(float(w.abs().max()), 1.0)
+
+
+def test_composite_transpose_identity(cuda_device):
+    H, _ = _hierarchy()
+    rng = np.random.default_rng(4)
+    for a, b in ((0.7, 0.4), (-0.6, 0.9), (0.5, -1.1)):
+        v = [torch.as_tensor(rng.standard_normal(n), device="cuda") for n in H.inner_cells]
+        w = [torch.as_tensor(rng.standard_normal(n), device="cuda") for n in H.inner_cells]
+        new, inputs = H.step(H.extend(v), a, b, 1e-3)
+        mv = H.interior(new)
+        g = torch.zeros(2, dtype=torch.float64, device="cuda")
+        mtw = H.interior(H.step_adjoint(H.extend(w), inputs, a, b, 1e-3, g))
+        lhs = sum(float(torch.dot(x, y)) for x, y in zip(mv, w))
+        rhs = sum(float(torch.dot(x, y)) for x, y in zip(v, mtw))
+        assert abs(lhs - rhs) <= 1e-12 * max(abs(lhs), 1.0)
+
+
+def test_composite_gradient_matches_torch_autograd(cuda_device):
+    """The hand-written adjoint against torch autograd through the FP64 restatement (the reference gradient)."""
+    H, hosts = _hierarchy()
+    ref = _TorchComposite(hosts, 24)
+    rng = np.random.default_rng(6)
+    steps, dt = 12, 0.5 / (1.5 * 96)
+    u0 = [torch.as_tensor(_gauss_cells(h, 24 * 2 ** k, 0.5, 0.5, 0.12), device="cuda") for k, h in enumerate(hosts)]
+    tg = [torch.as_tensor(rng.standard_normal(n) * 0.1, device="cuda") for n in H.inner_cells]
+
+    def loss(out):
+        return sum(0.5 * torch.sum((u - t) ** 2) for u, t in zip(out, tg))
+
+    vel = torch.tensor([1.0, 0.5], dtype=torch.float64, device="cuda", requires_grad=True)
+    ua = [u.clone().requires_grad_(True) for u in u0]
+    loss(adj.advect_composite(vel, H, ua, dt=dt, steps=steps, checkpoint_every=5)).backward()
+    vr = torch.tensor([1.0, 0.5], dtype=torch.float64, device="cuda", requires_grad=True)
+    ur = [u.clone().requires_grad_(True) for u in u0]
+    loss(ref.run(ur, vr, dt, steps)).backward()
+    assert float((vel.grad - vr.grad).abs().max()) <= 1e-9 * float(vr.grad.abs().max())
+    for a, b in zip(ua, ur):
+        assert float((a.grad - b.grad).abs().max()) <= 1e-10 * max(float(b.grad.abs().max()), 1e-30)
+
+
+def test_composite_gradient_against_central_differences(cuda_device):
+    """FP32 adjoint of the composite model against FP64 central differences on 32 seeded directions."""
+    H, hosts = _hierarchy(32)
+    steps, every = 10, 4
+    dt = 0.5 / (1.5 * 128)
+    target = [torch.as_tensor(_gauss_cells(h, 32 * 2 ** k, 0.55, 0.525, 0.1), device="cuda")
+              for k, h in enumerate(hosts)]
+    u0 = [torch.as_tensor(_gauss_cells(h, 32 * 2 ** k, 0.5, 0.5, 0.1), device="cuda") for k, h in enumerate(hosts)]
+
+    def loss(vel, us, dtype):
+        out = adj.advect_composite(vel, H, [u.to(dtype) for u in us], dt=dt, steps=steps, checkpoint_every=every)
+        return sum(0.5 * torch.sum((u.double() - t) ** 2) for u, t in zip(out, target))
+
+    vel0 = torch.tensor([1.0, 0.5], dtype=torch.float64, device="cuda")
+    vel = vel0.clone().requires_grad_(True)
+    u32 = [u.float().requires_grad_(True) for u in u0]
+    loss(vel, u32, torch.float32).backward()
+    rng = np.random.default_rng(5)
+    eps = 1e-6
+    errs = []
+    for _ in range(32):
+        dv = torch.as_tensor(rng.standard_normal(2), device="cuda")
+        du = [torch.as_tensor(rng.standard_normal(u.numel()), device="cuda") for u in u0]
+        dirder = float(torch.dot(vel.grad, dv)) + sum(float(torch.dot(g.grad.double(), d)) for g, d in zip(u32, du))
+        with torch.no_grad():
+            lp = loss(vel0 + eps * dv, [u + eps * d for u, d in zip(u0, du)], torch.float64)
+            lm = loss(vel0 - eps * dv, [u - eps * d for u, d in zip(u0, du)], torch.float64)
+        fd = (float(lp) - float(lm)) / (2 * eps)
+        errs.append(abs(dirder - fd) / max(abs(fd), 1e-12))
+    assert max(errs) < 1e-4, max(errs)
