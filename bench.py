@@ -12,16 +12,25 @@ batch in one fused launch.
 Metric: input intervals per second (Gintervals/s), the reference's
 convention (subsetix_cupy/benchmarks/cases.py:88).  `value` is device-timed
 with the inputs resident in HBM.  `e2e` goes through the public API
-(subsetix_cupy.evaluate) with pinned host buffers: H2D copies of the
-operands, evaluation, then D2H of the result, all inside the timed region;
-consecutive steps overlap one step's upload with the previous step's
-evaluation and download (`e2e.serial` runs them one at a time).
+(subsetix_cupy.evaluate) with pinned host buffers allocated once: H2D copies
+of the operands, evaluation, then D2H of the result, all inside the timed
+region; consecutive steps overlap one step's upload with the previous step's
+evaluation and download (`e2e.serial` runs them one at a time), and the
+copies' own bandwidth is reported beside it.  Once, outside the timed region,
+the full output is compared with the oracle bit for bit.
+
+Beside the headline: `reference_gpu` times the reference's own kernels
+(compiled from its sources with NVRTC, launched with torch host operations
+in the reference's order) on the same batch; the AMR, adjoint and batched
+sections of the other workloads, each with a CPU baseline.
 
 Multi-GPU: every rank evaluates its own batch (weak scaling, no
 collective).  Times are the max over ranks.
 
-`--impl reference` times the reference algorithm on the host CPU (the
-oracle port, all host threads).  It reports the same metric and config.
+`--impl reference` times the reference algorithm on the host CPU (the oracle
+port of the reference's kernels, all host threads) on the same batch.  It
+reports the same metric and config.  `--section setops` runs the headline
+launch alone (the command behind the ncu captures in profiles/).
 """
 
 from __future__ import annotations
@@ -54,10 +63,10 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=5)
     p.add_argument("--cpu-seconds", type=float, default=10.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--no-amr", action="store_true", help="skip the two-level AMR step section")
+    p.add_argument("--no-amr", action="store_true", help="skip the AMR, adjoint and batched sections")
     p.add_argument("--no-autotune", action="store_true", help="use the automatic launch choice")
-    p.add_argument("--section", default="all", choices=["all", "amr", "adjoint", "batched"],
-                   help="run only the AMR or the adjoint section (for profiling)")
+    p.add_argument("--section", default="all", choices=["all", "setops", "amr", "adjoint", "batched"],
+                   help="run one part alone (profiling); setops = the headline launch only")
     return p.parse_args()
 
 
@@ -155,29 +164,37 @@ KERNELS = {1: "sx_sweep_kernel<5,0>", 2: "sx_sweep_smem_kernel<5>", 3: "sx_merge
            5: "sx_wseg_kernel<5>", 6: "sx_wseg16_kernel<5>"}
 
 
-def traffic_per_launch(copies: int, kernel: str = "sx_wseg_kernel<5>"):
-    """DRAM bytes of one fused launch, from the committed ncu summary of that kernel (scaled by copies)."""
+def traffic_per_launch(copies: int, kernel: str):
+    """DRAM bytes of one fused launch from the committed ncu summary of that kernel, scaled by the copy count.
+
+    Returns ``(bytes, source)``; the summary records the copy count of its
+    capture and the bytes per copy (traffic grows with the copies).
+    """
     path = os.path.join(REPO, "profiles", kernel.split("<")[0] + "_shapes4096.md")
+    per_copy = captured = None
     try:
         for line in open(path):
             if line.startswith("traffic_bytes_per_copy:"):
-                return int(float(line.split(":")[1]) * copies)
+                per_copy = float(line.split(":")[1])
+            elif line.startswith("traffic_capture_copies:"):
+                captured = int(line.split(":")[1])
     except OSError:
         pass
-    return None
+    if per_copy is None:
+        return None, None
+    return int(per_copy * copies), f"ncu dram__bytes of {os.path.relpath(path, REPO)} ({captured or '?'} copies), scaled to {copies}"
 
 
-def cpu_baseline(leaves_host, seconds: float, use_ref: bool):
-    """Time the host implementation (the oracle port, all host threads) on a bounded sample
-    (whole copies of the workload).  ``use_ref`` is kept for the call sites: the reference is
-    a CuPy package with no host implementation of its own to run on the GPU box."""
+def _oracle_leaves(leaves_host):
     from oracle import oracle as O
 
-    kind = "port"
-    cores = O.threads()
-    one = [tuple(a for a in leaf) for leaf in leaves_host]
-    leaves = {n: O.ISet(*h) for n, h in zip("ABCDE", one)}
-    n_in = sum(int(h[0].size) for h in one)
+    return O, {n: O.ISet(*h) for n, h in zip("ABCDE", leaves_host)}
+
+
+def cpu_baseline(leaves_host, seconds: float):
+    """Time the oracle port (all host threads) on a bounded sample: whole copies of the workload, repeated."""
+    O, leaves = _oracle_leaves(leaves_host)
+    n_in = sum(int(h[0].size) for h in leaves_host)
     done = 0
     t0 = time.perf_counter()
     while True:
@@ -186,45 +203,61 @@ def cpu_baseline(leaves_host, seconds: float, use_ref: bool):
         if time.perf_counter() - t0 >= seconds:
             break
     dt = time.perf_counter() - t0
-    return {"value": n_in * done / dt / 1e9, "unit": UNIT, "cores": int(cores), "kind": kind,
+    return {"value": n_in * done / dt / 1e9, "unit": UNIT, "cores": int(O.threads()), "kind": "port",
             "sample": f"{done} evaluations of one 4096x4096 copy ({n_in} input intervals), {dt:.1f} s"}
 
 
 def run_reference(args, rank, world):
+    """The reference algorithm on the host CPU, on the same per-rank batch as the GPU arm (rank 0 only)."""
     if rank != 0:
         return
-    from subsetix_b200 import synth
-
-    one = [synth.stack_rows(s, 1, 4096) for s in synth.shape_operands(4096)]
-    vals = []
-    base = None
+    leaves_host = workload(args.copies)
+    O, leaves = _oracle_leaves(leaves_host)
+    n_in = sum(int(h[0].size) for h in leaves_host)
     for _ in range(args.warmup):
-        cpu_baseline(one, 0.0, True)
+        O.evaluate(SPEC, leaves)
+    times = []
     for _ in range(args.steps):
-        base = cpu_baseline(one, 0.0, True)
-        vals.append(base["value"])
-    value = float(statistics.median(vals)) if vals else 0.0
-    n_in = sum(int(h[0].size) for h in one)
+        t0 = time.perf_counter()
+        O.evaluate(SPEC, leaves)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = n_in * args.steps / total / 1e9
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": n_in / (value * 1e9) * 1e3 if value else None,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-        "config": {"workload": "shapes4096 ((A|B)-(C&D))^E, one copy per step on the host CPU", "copies": 1,
-                   "input_intervals_per_step": n_in},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": base["cores"] if base else None,
-                         "kind": base["kind"] if base else None, "sample": "one copy per step"},
+        "config": {"workload": f"shapes4096 ((A|B)-(C&D))^E x{args.copies} stacked copies per rank",
+                   "copies": args.copies, "input_intervals_per_step": n_in,
+                   "l2": "host memory (CPU run)", "parallelism": "rank 0 host threads"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": int(O.threads()), "kind": "port",
+                         "sample": f"{args.steps} evaluations of the {args.copies}-copy batch"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
-def amr_section(device, steps: int = 200, every: int = 10, res: int = 1024, threshold: float = 0.05):
+# ---------------------------------------------------------------------------------------------------------------
+# Sections beside the headline
+# ---------------------------------------------------------------------------------------------------------------
+
+def _gauss_grid(res, sigma=0.05):
+    xs = (np.arange(res) + 0.5) / res
+    gx, gy = np.meshgrid(xs, xs)
+    return np.exp(-((gx - 0.5) ** 2 + (gy - 0.5) ** 2) / (2 * sigma ** 2))
+
+
+def amr_section(device, steps: int = 200, every: int = 10, res: int = 1024, threshold: float = 0.05,
+                oracle_res: int = 256, dropin: bool = True):
     """Two-level AMR advection, Gaussian blob exp(-r^2 / (2 * 0.05^2)) on a res^2 coarse grid.
 
     Velocity (1.0, 0.5), CFL 0.5, regrid with 2:1 grading every `every`
     steps, `steps` steps.  FP32 with CUDA-graph replay against FP64 without
-    graphs (the plain FP64 step) and FP64 with graphs; FP32 error against
-    the FP64 run, compensated FP64 mass integrals and restriction defect.
+    graphs (the plain FP64 step) and FP64 with graphs; FP32 error against the
+    FP64 run, and at `oracle_res`^2 against the independent FP64 oracle (the
+    CPU restatement of the reference's loop); compensated FP64 mass integrals
+    and the restriction defect; the drop-in AMR2Simulation.run timed on the
+    same run; the oracle's FP32 loop timed on the host as the CPU baseline.
 
     `threshold` applies to the reference's gradient (half the central
     difference, not divided by dx).  At 0.05 the Gaussian's steepest cell
@@ -233,15 +266,14 @@ def amr_section(device, steps: int = 200, every: int = 10, res: int = 1024, thre
     """
     import torch
 
+    from oracle import oracle as O
     from subsetix_b200.subsetix_amr2.fused import FusedTwoLevelAMR
 
-    xs = (np.arange(res) + 0.5) / res
-    gx, gy = np.meshgrid(xs, xs)
-    u0 = np.exp(-((gx - 0.5) ** 2 + (gy - 0.5) ** 2) / (2 * 0.05 ** 2))
+    u0 = _gauss_grid(res)
 
-    def make(dtype, fused):
-        return FusedTwoLevelAMR(torch.as_tensor(u0, dtype=dtype, device=device), velocity=(1.0, 0.5), cfl=0.5,
-                                refine_threshold=threshold, grading=1, dtype=dtype, fused=fused)
+    def make(dtype, fused, r=res, u=u0, thr=threshold):
+        return FusedTwoLevelAMR(torch.as_tensor(u, dtype=dtype, device=device), velocity=(1.0, 0.5), cfl=0.5,
+                                refine_threshold=thr, grading=1, dtype=dtype, fused=fused)
 
     stream = torch.cuda.current_stream(device)
     runs = {}
@@ -288,61 +320,115 @@ def amr_section(device, steps: int = 200, every: int = 10, res: int = 1024, thre
         out[f"fp32_linf_{lvl.split('_')[0]}"] = float((a - b).abs().max())
     out["speedup_fp32_graph_vs_fp64_plain"] = out["fp64_plain"]["ms_per_step"] / out["fp32_graph"]["ms_per_step"]
     out["fp64_reference"] = "the FP64 run of the same kernels (bit-identical to the FP64 oracle at test sizes)"
+
+    # the drop-in API on the same run: AMR2Simulation.run with no callbacks
+    if dropin:
+        from subsetix_b200.subsetix_amr2 import AMR2Simulation, SimulationConfig
+        from subsetix_b200.subsetix_cupy import create_interval_field, full_interval_set
+
+        def dropin_run():
+            sim = AMR2Simulation(SimulationConfig(coarse_resolution=res, velocity=(1.0, 0.5), cfl=0.5,
+                                                  refine_threshold=threshold))
+            f = create_interval_field(full_interval_set(res, res), fill_value=0.0, dtype=np.float32)
+            f.values.copy_(torch.as_tensor(u0.reshape(-1), dtype=torch.float32, device=device))
+            sim.set_initial_field(f)
+            return sim
+
+        warm = dropin_run()
+        warm.run(steps=3 * every, regrid_every=every)
+        sim = dropin_run()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        state, _ = sim.run(steps=steps, regrid_every=every)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        same = bool(torch.equal(state.coarse_field.values, runs["fp32_graph"][0].coarse_values[0].reshape(-1)))
+        out["dropin_amr2simulation"] = {
+            "ms_per_step": ms / steps, "gcell_updates_per_s": cells * steps / (ms / 1e3) / 1e9,
+            "vs_fp32_graph": (ms / steps) / out["fp32_graph"]["ms_per_step"], "bit_equal_to_fp32_graph": same,
+            "note": "subsetix_amr2.AMR2Simulation.run (the public API), graph captures done in the warm-up run"}
+
+    # FP32 against the independent FP64 oracle (the CPU restatement of the reference's loop) at oracle_res^2
+    thr_o = threshold * res / oracle_res if threshold < 0.05 else threshold
+    u0o = _gauss_grid(oracle_res)
+    oracle_steps = steps
+    ref64 = O.AMR2(oracle_res, (1.0, 0.5), cfl=0.5, threshold=thr_o, grading_pad=1, dtype=np.float64)
+    ref64.init(u0o)
+    ref64.run(oracle_steps, every)
+    eng = make(torch.float32, True, r=oracle_res, u=u0o, thr=thr_o)
+    eng.run(oracle_steps, every)
+    torch.cuda.synchronize()
+    err = {}
+    for lvl, want in (("coarse", ref64.coarse.values), ("fine", ref64.fine.values)):
+        got = getattr(eng, f"{lvl}_values")[0].double().reshape(-1).cpu().numpy()
+        err[f"rel_l2_{lvl}"] = float(np.linalg.norm(got - want) / np.linalg.norm(want))
+        err[f"linf_{lvl}"] = float(np.abs(got - want).max())
+    out["fp32_vs_fp64_oracle"] = {"resolution": oracle_res, "steps": oracle_steps, "refine_threshold": thr_o, **err,
+                                  "oracle": "oracle.AMR2 in float64 (CPU restatement of the reference's loop)"}
+    # CPU baseline: the oracle's FP32 loop (the reference's algorithm on the host), bounded sample
+    cpu = O.AMR2(oracle_res, (1.0, 0.5), cfl=0.5, threshold=thr_o, grading_pad=1, dtype=np.float32)
+    cpu.init(u0o)
+    t0 = time.perf_counter()
+    n_cpu = 2 * every
+    cpu.run(n_cpu, every)
+    dt_cpu = time.perf_counter() - t0
+    cells_o = oracle_res * oracle_res * 5
+    out["cpu_baseline"] = {"value": cells_o * n_cpu / dt_cpu / 1e9, "unit": "Gcell-upd/s", "cores": int(O.threads()),
+                           "kind": "port", "sample": f"{n_cpu} steps of the oracle's FP32 AMR loop at "
+                                                     f"{oracle_res}^2 coarse, {dt_cpu:.1f} s"}
     return out
 
 
 def adjoint_section(device, base: int = 2048, steps: int = 50, every: int = 10, directions: int = 32):
-    """Adjoint advection on fixed three-level geometry.
+    """Adjoint advection on fixed three-level composite geometry.
 
-    Level 0 is the full base^2 grid, levels 1 and 2 are seeded nested disks of
-    radius 0.3 and 0.15 (unit square) refined x2 and x4.  FP32 fields, 50
-    upwind steps at CFL 0.5 on the finest level, loss 0.5 ||u_T - u_target||^2
-    with u_target a shifted Gaussian; gradient with respect to u_0 and the
-    velocity by the adjoint kernel with checkpoints every 10 steps, checked
-    against FP64 central finite differences (eps 1e-6) on seeded directions.
+    Level 0 is the full base^2 grid; levels 1 and 2 are nested disks of
+    radius 0.3 and 0.15 (unit square) rasterised on the coarser level and
+    refined x2 each.  The levels are coupled every step: ghost rings filled
+    from the coarser level, covered coarse cells restricted from the finer
+    one.  FP32 fields, 50 upwind steps at CFL 0.5 on the finest level, loss
+    0.5 ||u_T - u_target||^2 over every level, u_target a shifted Gaussian;
+    gradient with respect to u_0 and the velocity by the adjoint kernels with
+    checkpoints every 10 steps, checked against FP64 central finite
+    differences (eps 1e-6) on seeded directions.
     """
     import torch
 
+    from oracle import oracle as O
     from subsetix_b200 import adjoint as adj
     from subsetix_b200 import synth
     from subsetix_b200.subsetix_cupy.expressions import IntervalSet
 
-    def level(h, res):
-        s = IntervalSet._trusted(*(torch.as_tensor(a, device=device) for a in h))
-        return adj.Level(s, res, res, 1.0 / res, 1.0 / res)
+    hosts = synth.nested_disk_levels(base, [0.3, 0.15])
+    sets = [IntervalSet._trusted(*(torch.as_tensor(a, device=device) for a in h)) for h in hosts]
+    H = adj.Hierarchy(sets, base, base)
 
-    full = (np.zeros(base, np.int32), np.full(base, base, np.int32), np.arange(base + 1, dtype=np.int32),
-            np.arange(base, dtype=np.int32))
-    levels = [level(full, base), level(synth.disk_rows(2 * base, 0.3 * 2 * base), 2 * base),
-              level(synth.disk_rows(4 * base, 0.15 * 4 * base), 4 * base)]
-
-    def gauss(lvl, cx, cy, dtype):
-        s = lvl.interval_set
-        b, e, off, rows = (x.long() for x in (s.begin, s.end, s.row_offsets, s.rows))
-        lens = e - b
-        per_row = torch.repeat_interleave(rows, off[1:] - off[:-1])
-        ys = torch.repeat_interleave(per_row, lens)
-        starts = torch.repeat_interleave(b, lens)
-        first = torch.repeat_interleave(torch.cumsum(lens, 0) - lens, lens)
-        xs = starts + torch.arange(int(lens.sum()), device=device) - first
-        x = (xs.double() + 0.5) / lvl.width
-        y = (ys.double() + 0.5) / lvl.height
-        return torch.exp(-((x - cx) ** 2 + (y - cy) ** 2) / (2 * 0.05 ** 2)).to(dtype)
+    def gauss(k, cx, cy, dtype):
+        b, e, off, rows = hosts[k]
+        n = base * 2 ** k
+        lens = (e - b).astype(np.int64)
+        ys = np.repeat(np.repeat(rows, np.diff(off)), lens)
+        xs = np.concatenate([np.arange(x0, x1) for x0, x1 in zip(b, e)])
+        x, y = (xs + 0.5) / n, (ys + 0.5) / n
+        return torch.as_tensor(np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / (2 * 0.05 ** 2)), dtype=dtype,
+                               device=device)
 
     vel0 = torch.tensor([1.0, 0.5], dtype=torch.float64, device=device)
-    dt = 0.5 / (1.0 / levels[-1].dx + 0.5 / levels[-1].dy)
-    cells = sum(l.cells for l in levels)
+    finest = base * 4
+    dt = 0.5 / (1.0 * finest + 0.5 * finest)
+    cells = sum(H.inner_cells)
 
     def loss(vel, u0, targets):
-        uT = adj.advect(vel, levels, u0, dt=dt, steps=steps, checkpoint_every=every)
+        uT = adj.advect_composite(vel, H, u0, dt=dt, steps=steps, checkpoint_every=every)
         return sum(0.5 * torch.sum((u.double() - t.double()) ** 2) for u, t in zip(uT, targets))
 
-    u0_32 = [gauss(l, 0.5, 0.5, torch.float32) for l in levels]
-    tg_32 = [gauss(l, 0.52, 0.51, torch.float32) for l in levels]
-    # warm-up, then time forward + backward in FP32
+    u0_32 = [gauss(k, 0.5, 0.5, torch.float32) for k in range(3)]
+    tg_32 = [gauss(k, 0.55, 0.525, torch.float32) for k in range(3)]
     vel = vel0.clone().requires_grad_(True)
     u0 = [u.clone().requires_grad_(True) for u in u0_32]
-    loss(vel, u0, tg_32).backward()
+    loss(vel, u0, tg_32).backward()  # warm-up
     torch.cuda.synchronize()
     stream = torch.cuda.current_stream(device)
     e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
@@ -356,7 +442,6 @@ def adjoint_section(device, base: int = 2048, steps: int = 50, every: int = 10, 
     torch.cuda.synchronize()
     fwd_ms, bwd_ms = e0.elapsed_time(e1), e1.elapsed_time(e2)
     g_v, g_u = vel.grad.clone(), [u.grad.double() for u in u0]
-    # FP64 central differences on seeded directions
     u0_64 = [u.double() for u in u0_32]
     tg_64 = [t.double() for t in tg_32]
     gen = torch.Generator(device=device)
@@ -372,24 +457,36 @@ def adjoint_section(device, base: int = 2048, steps: int = 50, every: int = 10, 
             fd = (float(lp) - float(lm)) / (2 * eps)
             dd = float(torch.dot(g_v, dv)) + sum(float(torch.dot(g, d)) for g, d in zip(g_u, du))
             errs.append(abs(dd - fd) / max(abs(fd), 1e-30))
-    return {"workload": f"3 levels: {base}^2 full grid, disks r=0.3 at x2 and r=0.15 at x4; {steps} FP32 upwind "
-                        f"steps, checkpoints every {every}", "cells": cells,
-            "forward_ms": fwd_ms, "backward_ms": bwd_ms,
+    # CPU baseline: one FP32 upwind step of every level with the oracle (forward only; no CPU adjoint exists)
+    t0 = time.perf_counter()
+    for k, h in enumerate(hosts):
+        s = O.ISet(*h)
+        f = O.Field(s, u0_32[k].cpu().numpy(), O.cell_offsets(s))
+        n = base * 2 ** k
+        O.upwind(f, width=n, height=n, a=1.0, b=0.5, dt=dt, dx=1.0 / n, dy=1.0 / n)
+    dt_cpu = time.perf_counter() - t0
+    return {"workload": f"3 coupled levels: {base}^2 full grid, disks r=0.3 at x2 and r=0.15 at x4 (ghost fill from "
+                        f"the coarser level, restriction onto it); {steps} FP32 steps, checkpoints every {every}",
+            "cells": cells, "forward_ms": fwd_ms, "backward_ms": bwd_ms,
             "forward_gcell_updates_per_s": cells * steps / (fwd_ms / 1e3) / 1e9,
             "fd_directions": directions, "fd_eps": eps,
             "fd_rel_err_max": max(errs), "fd_rel_err_median": statistics.median(errs),
-            "check": "FP32 adjoint gradient vs FP64 central differences of the same loss"}
+            "check": "FP32 adjoint gradient vs FP64 central differences of the same loss",
+            "cpu_baseline": {"value": cells / dt_cpu / 1e9, "unit": "Gcell-upd/s", "cores": int(O.threads()),
+                             "kind": "port", "sample": f"one FP32 upwind step of the three levels (uncoupled), "
+                                                       f"{dt_cpu:.2f} s"}}
 
 
-def batched_section(device, count: int = 256, repeats: int = 10):
+def batched_section(device, count: int = 256, repeats: int = 20):
     """Batched uneven sets: `count` sets with sides log-uniform in [128, 4096] and lognormal(1.5, 1.0)
-    intervals per row.  Every set gets a union and an intersection with its partner and one FP32
-    upwind step; each of the three is one launch of the set or stencil kernel over the whole batch
-    (rows of set i on band i), through the public API (host synchronisations included)."""
+    intervals per row.  Every set gets a union and an intersection with its partner and one FP32 upwind
+    step with its own dx = 1/side and CFL-0.5 time step: three launches on fixed buffers, captured once
+    as a CUDA graph and replayed (no host synchronisation inside a step)."""
     import torch
 
+    from oracle import oracle as O
     from subsetix_b200 import synth
-    from subsetix_b200.batch import SetBatch, batched_binary, batched_upwind
+    from subsetix_b200.batch import BatchStep, SetBatch
     from subsetix_b200.subsetix_cupy.expressions import IntervalSet
 
     sides, a_sets = synth.batched_uneven_sets(count=count, seed=3)
@@ -405,43 +502,96 @@ def batched_section(device, count: int = 256, repeats: int = 10):
     gen = torch.Generator(device=device)
     gen.manual_seed(5)
     vals = torch.rand(cells, device=device, generator=gen)
-    out = torch.empty_like(vals)
-    width = max(sides)
-    dt, dx = 0.25 / width, 1.0 / width
-
-    def step():
-        u = batched_binary(A, B, "union")
-        i = batched_binary(A, B, "intersection")
-        batched_upwind(A, vals, width=width, a=1.0, b=0.5, dt=dt, dx=dx, dy=dx, out=out)
-        return u, i
-
+    dx = [1.0 / s for s in sides]
+    dts = [0.5 / (1.0 / h + 0.5 / h) for h in dx]
+    step = BatchStep(A, B, vals, width=sides, a=1.0, b=0.5, dt=dts, dx=dx, dy=dx)
+    step()
+    graph = step.graph()
     for _ in range(3):
-        step()
+        graph.replay()
     torch.cuda.synchronize()
     stream = torch.cuda.current_stream(device)
-    marks = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-    t_u = t_i = t_w = 0.0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(repeats):
+        graph.replay()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_step = e0.elapsed_time(e1) / repeats
+    # the parts, for the roofline of the stencil
+    marks = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    from subsetix_b200 import _lib
+    from subsetix_b200.batch import _upwind_bands
+    t_w = 0.0
     for _ in range(repeats):
         marks[0].record(stream)
-        batched_binary(A, B, "union")
+        _upwind_bands(A, step.plan, step.table, vals, step.out, step.width, 1.0, 0.5)
         marks[1].record(stream)
-        batched_binary(A, B, "intersection")
-        marks[2].record(stream)
-        batched_upwind(A, vals, width=width, a=1.0, b=0.5, dt=dt, dx=dx, dy=dx, out=out)
-        marks[3].record(stream)
         torch.cuda.synchronize()
-        t_u += marks[0].elapsed_time(marks[1])
-        t_i += marks[1].elapsed_time(marks[2])
-        t_w += marks[2].elapsed_time(marks[3])
-    t_u, t_i, t_w = t_u / repeats, t_i / repeats, t_w / repeats
+        t_w += marks[0].elapsed_time(marks[1])
+    t_w /= repeats
+    R = int(A.combined.rows.numel())
+    nA = int(A.combined.begin.numel())
+    upwind_bytes = 2 * 4 * cells + 16 * nA + 4 * (R + 1)
+    peak, _ = peak_hbm()
+    unions = step.union()
+    # CPU baseline: the oracle on a bounded sample of sets (union, intersection, upwind per set)
+    t0 = time.perf_counter()
+    done_cells = done_in = 0
+    k = 0
+    while k < count and time.perf_counter() - t0 < 5.0:
+        sa, sb = O.ISet(*a_sets[k]), O.ISet(*b_sets[k])
+        O.union(sa, sb)
+        O.intersection(sa, sb)
+        f = O.create_field(sa, 0.5, np.float32)
+        O.upwind(f, width=sides[k], height=sides[k], a=1.0, b=0.5, dt=dts[k], dx=dx[k], dy=dx[k])
+        done_cells += int(f.values.size)
+        done_in += int(sa.begin.size + sb.begin.size)
+        k += 1
+    dt_cpu = time.perf_counter() - t0
     return {"workload": f"{count} sets, sides log-uniform [128, 4096], lognormal(1.5, 1.0) intervals per row; "
-                        "union + intersection + one FP32 upwind step per set, one launch each for the batch",
-            "sets": count, "rows": int(sum(sides)), "input_intervals": n_in, "cells": cells,
-            "union_ms": t_u, "intersection_ms": t_i, "upwind_ms": t_w, "batch_step_ms": t_u + t_i + t_w,
-            "setops_gintervals_per_s": 2 * n_in / ((t_u + t_i) / 1e3) / 1e9,
+                        "union + intersection + one FP32 upwind step per set (dx = 1/side, CFL 0.5 per set)",
+            "sets": count, "rows": R, "input_intervals": n_in, "cells": cells,
+            "batch_step_ms": t_step, "upwind_ms": t_w,
+            "step_gintervals_per_s": n_in / (t_step / 1e3) / 1e9,
             "upwind_gcell_updates_per_s": cells / (t_w / 1e3) / 1e9,
-            "timing": "device events around the public calls (host synchronisations of the API included)"}
+            "upwind_hbm_frac": upwind_bytes / (t_w / 1e3) / 1e9 / peak,
+            "union_output_intervals": int(unions.combined.begin.numel()),
+            "timing": "device events around graph replays of the whole step (3 launches, no host sync); "
+                      "upwind alone timed by events around its launch",
+            "cpu_baseline": {"value": done_cells / dt_cpu / 1e9, "unit": "Gcell-upd/s", "cores": int(O.threads()),
+                             "kind": "port", "sample": f"{k} of the {count} sets (union, intersection and upwind "
+                                                       f"each), {dt_cpu:.1f} s; {done_in} input intervals"}}
 
+
+def reference_gpu_section(device, leaves_dev, n_in: int, steps: int = 5):
+    """The reference's own kernels, NVRTC-compiled, on the same batch: one count/scan/read/write launch
+    group per binary node, as the reference's Expr trees run (expressions.py:446-528)."""
+    import torch
+
+    from oracle import refgpu
+
+    if not refgpu.available():
+        return {"unavailable": "reference cubins not built (oracle/build_ref_nvrtc.py needs the reference checkout)"}
+    R = refgpu.RefKernels(device)
+    leaves = {n: t for n, t in zip("ABCDE", leaves_dev)}
+    R.evaluate(SPEC, leaves)
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        out = R.evaluate(SPEC, leaves)
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+    ms = statistics.median(times) * 1e3
+    return {"value": n_in / (ms / 1e3) / 1e9, "unit": UNIT, "ms_per_step": ms, "steps": steps,
+            "output_intervals": int(out[0].numel()),
+            "impl": "reference kernels + torch host ops: the reference's CUDA-C kernel strings compiled unchanged "
+                    "with NVRTC (its options), launched with its grid shapes; host steps restated with torch",
+            "timing": "wall clock per evaluation (the reference reads each node's total on the host)"}
+
+
+# ---------------------------------------------------------------------------------------------------------------
 
 def main():
     args = parse()
@@ -495,10 +645,12 @@ def main():
     off_buf = torch.empty(R + 1, dtype=torch.int32, device=device)
 
     tuning = {}
-    if not args.no_autotune:
+    if not args.no_autotune and args.section != "setops":
         from subsetix_b200 import autotune
 
         tuning = autotune.tune_bool_eval(specs, R, table, device)
+    elif args.section == "setops":
+        tuning = _core.auto_tuning(specs, R, device)
     launch_tuning = {k: v for k, v in tuning.items() if k not in ("ms", "key")} or None
 
     def step():
@@ -511,6 +663,28 @@ def main():
     if flags:
         raise SystemExit(f"fused kernel raised flags {flags}")
     algo = algorithmic_bytes(leaves_host, total, R)
+
+    if args.section == "setops":
+        # the headline launch alone: warm-up, then `steps` launches (the command of the ncu captures)
+        for _ in range(args.warmup + args.steps):
+            step()
+        torch.cuda.synchronize()
+        if rank == 0:
+            print(json.dumps({"setops": {"copies": args.copies, "launches": args.warmup + args.steps + 1,
+                                         "tuning": launch_tuning, "input_intervals": n_in}}), flush=True)
+        return
+
+    # parity of the full output with the oracle, once, outside the timed region
+    parity = None
+    if rank == 0 and not args.no_cpu_baseline:
+        O, oleaves = _oracle_leaves(leaves_host)
+        want = O.evaluate(SPEC, oleaves)
+        got = (ob[:total].cpu().numpy(), oe[:total].cpu().numpy(), ooff.cpu().numpy())
+        same = all(np.array_equal(x, y) for x, y in zip(got, want[:3])) and np.array_equal(want[3], leaves_host[0][3])
+        parity = {"checked_against": "oracle (CPU restatement of the reference's kernels)", "bit_exact": bool(same),
+                  "output_intervals": total}
+        if not same:
+            raise SystemExit("headline output differs from the oracle")
 
     for _ in range(args.warmup):
         step()
@@ -532,47 +706,23 @@ def main():
     elapsed_ms = max_over_ranks(ev[0].elapsed_time(ev[-1]), device)
     value = world * n_in * args.steps / (elapsed_ms / 1e3) / 1e9
 
-    # end to end through the public API with pinned host buffers
+    # ---- end to end through the public API, pinned host buffers allocated once ----
     pinned = [tuple(torch.as_tensor(a).pin_memory() for a in h) for h in leaves_host]
     h2d = sum(sum(int(t.numel()) * 4 for t in h) for h in pinned)
-    e2e_times = []
-    d2h = 0
-    for i in range(args.e2e_steps + 1):
-        s0 = torch.cuda.Event(enable_timing=True)
-        s1 = torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        s0.record(stream)
-        sets = []
-        for b, e, off, rows in pinned:
-            tb, te, to, tr = (x.to(device, non_blocking=True) for x in (b, e, off, rows))
-            s = E.IntervalSet._trusted(tb, te, to, tr, R)
-            sets.append(s)
-        A, B, C, D, F = [E.make_input(s) for s in sets]
-        res = E.evaluate(E.make_symmetric_difference(E.make_difference(E.make_union(A, B), E.make_intersection(C, D)), F))
-        outs = [torch.empty(x.shape, dtype=x.dtype, pin_memory=True) for x in (res.begin, res.end, res.row_offsets)]
-        for o, x in zip(outs, (res.begin, res.end, res.row_offsets)):
-            o.copy_(x, non_blocking=True)
-        s1.record(stream)
-        torch.cuda.synchronize()
-        d2h = sum(int(o.numel()) * 4 for o in outs)
-        if i > 0:
-            e2e_times.append(s0.elapsed_time(s1))
-    e2e_serial_ms = max_over_ranks(statistics.median(e2e_times), device)
-
-    # Pipelined, as a streaming caller would run it: step i+1's inputs go up on a
-    # second stream while step i is evaluated and its result comes down (the two
-    # copy directions overlap).  Every step's copies are inside the timed region,
-    # from the first upload to the last download.
+    # two result slots (double buffering), each with room for every possible output interval
+    slots = [tuple(torch.empty(n, dtype=torch.int32, pin_memory=True) for n in (cap, cap, R + 1)) for _ in range(2)]
     copy_stream = torch.cuda.Stream(device=device)
 
     def upload():
         with torch.cuda.stream(copy_stream):
+            u0 = torch.cuda.Event(enable_timing=True)
+            u0.record(copy_stream)
             dev_in = [tuple(x.to(device, non_blocking=True) for x in h) for h in pinned]
-        ready = torch.cuda.Event()
-        ready.record(copy_stream)
-        return dev_in, ready
+            u1 = torch.cuda.Event(enable_timing=True)
+            u1.record(copy_stream)
+        return dev_in, u1, (u0, u1)
 
-    def evaluate_step(dev_in, ready):
+    def evaluate_step(dev_in, ready, slot):
         stream.wait_event(ready)
         for t in dev_in:
             for x in t:
@@ -580,13 +730,38 @@ def main():
         sets = [E.IntervalSet._trusted(tb, te, to, tr, R) for tb, te, to, tr in dev_in]
         A, B, C, D, F = [E.make_input(s) for s in sets]
         res = E.evaluate(E.make_symmetric_difference(E.make_difference(E.make_union(A, B), E.make_intersection(C, D)), F))
-        outs = [torch.empty(x.shape, dtype=x.dtype, pin_memory=True) for x in (res.begin, res.end, res.row_offsets)]
-        for o, x in zip(outs, (res.begin, res.end, res.row_offsets)):
-            o.copy_(x, non_blocking=True)
-        return outs
+        d0 = torch.cuda.Event(enable_timing=True)
+        d0.record(stream)
+        n = int(res.begin.numel())
+        for o, x in zip(slot, (res.begin, res.end, res.row_offsets)):
+            o[: x.numel()].copy_(x, non_blocking=True)
+        d1 = torch.cuda.Event(enable_timing=True)
+        d1.record(stream)
+        return n, (d0, d1)
 
+    # serial: one step at a time
+    serial = []
+    d2h = 0
+    h2d_ms, d2h_ms = [], []
+    for i in range(args.e2e_steps + 1):
+        torch.cuda.synchronize()
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        dev_in, ready, up = upload()
+        n, down = evaluate_step(dev_in, ready, slots[i % 2])
+        s1.record(stream)
+        torch.cuda.synchronize()
+        d2h = 4 * (2 * n + R + 1)
+        if i > 0:
+            serial.append(s0.elapsed_time(s1))
+            h2d_ms.append(up[0].elapsed_time(up[1]))
+            d2h_ms.append(down[0].elapsed_time(down[1]))
+    e2e_serial_ms = max_over_ranks(statistics.median(serial), device)
+
+    # pipelined, as a streaming caller would run it: step i+1's inputs go up on the copy
+    # stream while step i is evaluated and its result comes down into the other slot
     n_pipe = max(2, args.e2e_steps)
-    evaluate_step(*upload())  # warm-up
     torch.cuda.synchronize()
     p0 = torch.cuda.Event(enable_timing=True)
     p1 = torch.cuda.Event(enable_timing=True)
@@ -596,7 +771,7 @@ def main():
         current = pending
         if i + 1 < n_pipe:
             pending = upload()
-        evaluate_step(*current)
+        evaluate_step(current[0], current[1], slots[i % 2])
     p1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(p0.elapsed_time(p1) / n_pipe, device)
@@ -606,6 +781,7 @@ def main():
     kname = KERNELS[int(tuning.get("kernel", 0)) or 5]
     peak, peak_kind = peak_hbm()
     achieved = algo / (kernel_ms / 1e3) / 1e9
+    traffic, traffic_src = traffic_per_launch(args.copies, kname)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -616,25 +792,30 @@ def main():
                    "tuning": {k: v for k, v in tuning.items() if k != "ms"}},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e_ms, "steps": n_pipe,
-                "mode": "public evaluate() from pinned host buffers; step i+1's H2D on a second stream overlaps "
-                        "step i's evaluation and D2H; timed from the first upload to the last download",
+                "mode": "public evaluate() from pinned host buffers allocated once; step i+1's H2D on a second "
+                        "stream overlaps step i's evaluation and D2H into alternating result buffers; timed from "
+                        "the first upload to the last download",
+                "h2d_gbs": h2d / (statistics.median(h2d_ms) / 1e3) / 1e9,
+                "d2h_gbs": d2h / (statistics.median(d2h_ms) / 1e3) / 1e9,
                 "serial": {"value": world * n_in / (e2e_serial_ms / 1e3) / 1e9, "ms_per_step": e2e_serial_ms,
                            "mode": "one step at a time: H2D, evaluate, D2H (median of steps)"}},
         "gpu_launches": args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic_per_launch(args.copies, kname),
+                     "frac": achieved / peak, "traffic": traffic, "traffic_source": traffic_src,
                      "peak_source": peak_kind, "algorithmic_bytes": algo, "kernel": kname,
                      "kernel_ms": kernel_ms},
         "clocks": clocks.summary(),
     }
+    if parity is not None:
+        line["parity"] = parity
+    line["reference_gpu"] = reference_gpu_section(device, dev, n_in)
     if not args.no_amr:
         line["amr_step"] = amr_section(device)
         line["amr_step_refined"] = amr_section(device, threshold=0.05 / 1024)
         line["adjoint"] = adjoint_section(device)
         line["batched"] = batched_section(device)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        one = [synth_one for synth_one in workload(1)]
-        line["cpu_baseline"] = cpu_baseline(one, args.cpu_seconds, True)
+        line["cpu_baseline"] = cpu_baseline(workload(1), args.cpu_seconds)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

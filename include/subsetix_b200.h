@@ -99,13 +99,21 @@ typedef struct sx_leaf {
  * warp of the staged sweep, or boundaries per tile of kernels 3 to 6; warps:
  * warps per block of kernels 4 to 6 (in 5 and 6 each warp owns a tile);
  * tile_rows: rows per tile of kernels 4 to 6 (at most 32, at most 8 for 6).
- * Results never depend on the tuning. */
+ * Results never depend on the tuning.
+ * Two fields exist for tests of the failure path and are zero otherwise:
+ * wait_limit caps the polls of every look-back wait of kernels 4 to 6 (0 =
+ * the built-in limit of 2^22 polls); withhold_tile = t + 1 makes tile t of
+ * those kernels never publish its look-back status, so the tiles after it
+ * wait until the limit, give up and report SX_FLAG_TIMEOUT (their outputs
+ * are then invalid; every write stays inside the caller's buffers). */
 typedef struct sx_tuning {
     int32_t kernel;
     int32_t blocks_per_sm;
     int32_t staging_cap;
     int32_t warps;
     int32_t tile_rows;
+    int32_t wait_limit;
+    int32_t withhold_tile;
 } sx_tuning;
 
 /* Workspace for sx_bool_eval: the size returned here lets every kernel use
@@ -358,6 +366,19 @@ int sx_upwind_chunked(int dtype, const int32_t* row_offsets, const int32_t* begi
                       const int32_t* cell_offsets, const int32_t* chunk_info, int64_t chunks, const int32_t* lookup,
                       const void* values, void* out, int32_t width, int32_t height, double a, double b, double dt,
                       double dx, double dy, void* stream);
+/* Banded form for batches of independent sets laid on row bands (subsetix_b200/batch.py): every row
+ * belongs to band row_band[row] (device, `height` entries) with its own spacing and time step, so
+ * each set keeps the dx = 1/side and CFL time step of its own step_upwind_interval call
+ * (subsetix_cupy/interval_stencil.py:126-219).  sx_upwind_band_table turns host triples
+ * (dx, dy, dt) into the kernel's table (host, 4 * nbands values of dtype), which the caller
+ * uploads once; chunks in rows whose band index is outside [0, nbands) are left unwritten.
+ * No reference counterpart for the batching. */
+int sx_upwind_band_table(int dtype, const double* spacing, int32_t nbands, void* table);
+int sx_upwind_chunked_bands(int dtype, const int32_t* row_offsets, const int32_t* begin, const int32_t* end,
+                            const int32_t* cell_offsets, const int32_t* chunk_info, int64_t chunks,
+                            const int32_t* lookup, const void* values, void* out, int32_t width, int32_t height,
+                            double a, double b, const int32_t* row_band, const void* band_table, int32_t nbands,
+                            void* stream);
 int sx_upwind_f32(const int32_t* rows, const int32_t* row_offsets, int32_t row_count, const int32_t* begin,
                   const int32_t* end, const int32_t* cell_offsets, int64_t n, int64_t cells, const int32_t* lookup,
                   const float* values, float* out, int32_t width, int32_t height, float a, float b, float dt, float dx,

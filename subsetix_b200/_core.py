@@ -80,6 +80,23 @@ def _default_keys(leaves, rows: int, tile_rows: int = 32) -> int:
     return avg + avg // 4 + 64
 
 
+def auto_tuning(leaves, rows: int, device) -> dict:
+    """The automatic launch shape of a truth-table sweep (one launch and one read-back).
+
+    Even rows: 8-row warp tiles with buffers sized for the largest tile (no
+    tile leaves the staged sweep, no buffer larger than needed).  Skewed rows
+    (the largest 8-row tile far above the mean): 32-row block tiles sized for
+    their largest tile, which evens out the load.  Tiles spanning at most
+    8190 columns take 16-bit keys (half the shared memory per tile, twice the
+    tiles in flight).
+    """
+    need8, need32, span8 = tile_stats(leaves, rows, device, 8, 32)
+    mean8 = 2 * sum(int(leaf[0].numel()) for leaf in leaves) / max(1, (rows + 7) // 8)
+    if need8 <= 3 * mean8 + 256:
+        return {"kernel": 6 if span8 <= 8190 else 5, "staging_cap": min(need8, 25000), "tile_rows": 8, "warps": 2}
+    return {"kernel": 4, "staging_cap": min(need32, 25000), "tile_rows": 32, "warps": 4}
+
+
 def bool_eval(leaves: Sequence[Tuple[torch.Tensor, torch.Tensor, torch.Tensor, int]], rows: int, table: Sequence[int],
               mode: int, device, out: Optional[Tuple[torch.Tensor, torch.Tensor]] = None):
     """Run the row sweep (sx_bool_eval) and read back its result pair.
@@ -99,19 +116,7 @@ def bool_eval(leaves: Sequence[Tuple[torch.Tensor, torch.Tensor, torch.Tensor, i
             tr = int(tuning.get("tile_rows", 0)) or (8 if tuning["kernel"] >= 5 else 32)
             tuning["staging_cap"] = min(max_tile_boundaries(leaves, rows, device, tile_rows=tr), 25000)
     elif mode == _lib.MODE_TABLE and not TUNING and rows > 0:
-        # Even rows: 8-row warp tiles with buffers sized for the largest tile
-        # (no tile leaves the staged sweep, no buffer larger than needed).
-        # Skewed rows (the largest 8-row tile far above the mean): 32-row
-        # block tiles sized for their largest tile, which evens out the load.
-        # Tiles spanning at most 8190 columns take 16-bit keys (half the
-        # shared memory per tile, twice the tiles in flight).
-        need8, need32, span8 = tile_stats(leaves, rows, device, 8, 32)
-        mean8 = 2 * sum(int(leaf[0].numel()) for leaf in leaves) / max(1, (rows + 7) // 8)
-        if need8 <= 3 * mean8 + 256:
-            tuning = {"kernel": 6 if span8 <= 8190 else 5, "staging_cap": min(need8, 25000), "tile_rows": 8,
-                      "warps": 2}
-        else:
-            tuning = {"kernel": 4, "staging_cap": min(need32, 25000), "tile_rows": 32, "warps": 4}
+        tuning = auto_tuning(leaves, rows, device)
     ob, oe, ooff, result = bool_eval_async(leaves, rows, table, mode, device, out, tuning=tuning)
     if result is None:
         return ob, oe, ooff, 0, 0
@@ -122,11 +127,13 @@ def bool_eval(leaves: Sequence[Tuple[torch.Tensor, torch.Tensor, torch.Tensor, i
 def bool_eval_async(leaves: Sequence[Tuple[torch.Tensor, torch.Tensor, torch.Tensor, int]], rows: int,
                     table: Sequence[int], mode: int, device, out: Optional[Tuple[torch.Tensor, torch.Tensor]] = None,
                     result: Optional[torch.Tensor] = None, offsets: Optional[torch.Tensor] = None,
-                    tuning: Optional[dict] = None):
+                    tuning: Optional[dict] = None, scratch: Optional[torch.Tensor] = None):
     """Enqueue the row sweep without waiting.
 
     Returns ``(begin, end, offsets, result)``; ``result`` is the device pair
-    ``(total, flags)``, or None when there are no rows.
+    ``(total, flags)``, or None when there are no rows.  ``scratch`` (bytes,
+    at least ``sx_bool_workspace_bytes(rows)``) replaces the per-stream
+    workspace, for launches captured in a graph.
     """
     lib = _lib.load()
     k = len(leaves)
@@ -157,10 +164,16 @@ def bool_eval_async(leaves: Sequence[Tuple[torch.Tensor, torch.Tensor, torch.Ten
         arr[i].widen = int(widen)
         arr[i].scale = int(scale)
     tab = (ctypes.c_uint32 * 8)(*[int(x) & 0xFFFFFFFF for x in (list(table) + [0] * 8)[:8]])
-    wsp, wsn = workspace(device, lib.sx_bool_workspace_bytes(int(rows)))
+    if scratch is None:
+        wsp, wsn = workspace(device, lib.sx_bool_workspace_bytes(int(rows)))
+    else:
+        if int(scratch.numel()) < int(lib.sx_bool_workspace_bytes(int(rows))):
+            raise ValueError("scratch below sx_bool_workspace_bytes(rows)")
+        wsp, wsn = scratch.data_ptr(), int(scratch.numel())
     t = TUNING if tuning is None else tuning
     tun = _lib.SxTuning(int(t.get("kernel", 0)), int(t.get("blocks_per_sm", 0)), int(t.get("staging_cap", 0)),
-                        int(t.get("warps", 0)), int(t.get("tile_rows", 0)))
+                        int(t.get("warps", 0)), int(t.get("tile_rows", 0)), int(t.get("wait_limit", 0)),
+                        int(t.get("withhold_tile", 0)))
     rc = lib.sx_bool_eval(arr, k, int(rows), tab, int(mode), ptr(ob), ptr(oe), ptr(ooff), cap, ptr(result), wsp, wsn,
                           ctypes.byref(tun), stream_handle(device))
     _lib.check(rc, "sx_bool_eval")

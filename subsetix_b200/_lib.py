@@ -40,7 +40,8 @@ class SxLeaf(ctypes.Structure):
 
 class SxTuning(ctypes.Structure):
     _fields_ = [("kernel", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32), ("staging_cap", ctypes.c_int32),
-                ("warps", ctypes.c_int32), ("tile_rows", ctypes.c_int32)]
+                ("warps", ctypes.c_int32), ("tile_rows", ctypes.c_int32), ("wait_limit", ctypes.c_int32),
+                ("withhold_tile", ctypes.c_int32)]
 
 
 class SxRowList(ctypes.Structure):
@@ -132,6 +133,10 @@ _SIGNATURES = {
     "sx_value_runs": (ctypes.c_int, [ctypes.c_int, c_vp, c_vp, ctypes.c_int64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
                                      c_vp]),
     "sx_gather_i32": (ctypes.c_int, [c_vp, ctypes.c_int32, c_vp, c_vp, c_vp]),
+    "sx_upwind_band_table": (ctypes.c_int, [ctypes.c_int, c_vp, ctypes.c_int32, c_vp]),
+    "sx_upwind_chunked_bands": (ctypes.c_int, [ctypes.c_int, c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.c_int64, c_vp, c_vp,
+                                               c_vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
+                                               c_vp, c_vp, ctypes.c_int32, c_vp]),
     "sx_index_copy": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "sx_index_block_mean": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, ctypes.c_int32, ctypes.c_double, c_vp, c_vp,
                                            c_vp, c_vp, c_vp]),

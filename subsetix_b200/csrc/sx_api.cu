@@ -99,8 +99,10 @@ int sx_bool_eval(const sx_leaf* leaves, int k, int32_t rows, const uint32_t* tab
     if (tuning) {
         if (tuning->kernel < 0 || tuning->kernel > 6 || tuning->blocks_per_sm < 0 || tuning->staging_cap < 0 ||
             tuning->warps < 0 || tuning->warps > 8 ||
-            tuning->tile_rows < 0 || tuning->tile_rows > 32)
+            tuning->tile_rows < 0 || tuning->tile_rows > 32 || tuning->wait_limit < 0 || tuning->withhold_tile < 0)
             return fail(SX_ERR_INVALID, "sx_bool_eval: bad tuning");
+        A.wait_limit = (unsigned)tuning->wait_limit;
+        A.withhold_tile = tuning->withhold_tile;
         A.tune_kernel = tuning->kernel;
         A.tune_blocks_per_sm = tuning->blocks_per_sm;
         A.tune_staging_cap = tuning->staging_cap;
@@ -525,6 +527,43 @@ int sx_upwind_chunked(int dtype, const int32_t* row_offsets, const int32_t* begi
     cudaError_t err = sx_upwind_chunk_launch(row_offsets, begin, end, cell_offsets, chunk_info, chunks, lookup, values,
                                              out, width, height, a, b, dt, dx, dy, dtype == SX_F64, (cudaStream_t)stream);
     if (err != cudaSuccess) return cuda_fail(err, "sx_upwind_chunked");
+    return SX_OK;
+}
+
+int sx_upwind_band_table(int dtype, const double* spacing, int32_t nbands, void* table)
+{
+    if (dtype != SX_F32 && dtype != SX_F64) return fail(SX_ERR_INVALID, "sx_upwind_band_table: dtype %d", dtype);
+    if (nbands < 0) return fail(SX_ERR_INVALID, "sx_upwind_band_table: negative band count");
+    if (nbands == 0) return SX_OK;
+    if (!spacing || !table) return fail(SX_ERR_INVALID, "sx_upwind_band_table: null argument");
+    for (int q = 0; q < nbands; ++q)
+        if (!(spacing[3 * q] > 0.0) || !(spacing[3 * q + 1] > 0.0))
+            return fail(SX_ERR_INVALID, "sx_upwind_band_table: band %d has a spacing that is not positive", q);
+    sx_upwind_band_table_fill(dtype == SX_F64, spacing, nbands, table);
+    return SX_OK;
+}
+
+int sx_upwind_chunked_bands(int dtype, const int32_t* row_offsets, const int32_t* begin, const int32_t* end,
+                            const int32_t* cell_offsets, const int32_t* chunk_info, int64_t chunks,
+                            const int32_t* lookup, const void* values, void* out, int32_t width, int32_t height,
+                            double a, double b, const int32_t* row_band, const void* band_table, int32_t nbands,
+                            void* stream)
+{
+    if (dtype != SX_F32 && dtype != SX_F64) return fail(SX_ERR_INVALID, "sx_upwind_chunked_bands: dtype %d", dtype);
+    if (width <= 0 || height <= 0)
+        return fail(SX_ERR_INVALID, "sx_upwind_chunked_bands: width and height must be positive");
+    if (chunks < 0 || nbands < 0) return fail(SX_ERR_INVALID, "sx_upwind_chunked_bands: bad size");
+    if (chunks == 0) return SX_OK;
+    if (!row_offsets || !begin || !end || !cell_offsets || !chunk_info || !lookup || !values || !out || !row_band ||
+        !band_table)
+        return fail(SX_ERR_INVALID, "sx_upwind_chunked_bands: null argument");
+    if (((uintptr_t)chunk_info & 15u) != 0)
+        return fail(SX_ERR_INVALID, "sx_upwind_chunked_bands: chunk_info must be 16-byte aligned");
+    if (values == out) return fail(SX_ERR_INVALID, "sx_upwind_chunked_bands: out must not alias values");
+    cudaError_t err = sx_upwind_chunk_bands_launch(row_offsets, begin, end, cell_offsets, chunk_info, chunks, lookup,
+                                                   values, out, width, height, a, b, row_band, band_table, nbands,
+                                                   dtype == SX_F64, (cudaStream_t)stream);
+    if (err != cudaSuccess) return cuda_fail(err, "sx_upwind_chunked_bands");
     return SX_OK;
 }
 

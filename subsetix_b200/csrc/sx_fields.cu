@@ -745,14 +745,20 @@ __global__ void sx_chunk_info_kernel(const int* __restrict__ rows, const int* __
     }
 }
 
-template <typename T>
+// With BANDS, every row belongs to a band (row_band[row]) with its own
+// spacing and time step: band_table[4 q .. 4 q + 3] = dx, dy (or their
+// exact reciprocals), dt, and 1 when the reciprocals are given.  Chunks of a
+// row whose band index is outside [0, nbands) are left unwritten.
+template <typename T, bool BANDS>
 __global__ void __launch_bounds__(256) sx_upwind_chunk_kernel(const int* __restrict__ off,
                                                               const int* __restrict__ b, const int* __restrict__ e,
                                                               const int* __restrict__ coff,
                                                               const int* __restrict__ info, long long chunks,
                                                               const int* __restrict__ lookup,
                                                               const T* __restrict__ v, T* __restrict__ out, int width,
-                                                              int height, T a, T bb, T dt, T dx, T dy, int pow2)
+                                                              int height, T a, T bb, T dt_all, T dx_all, T dy_all,
+                                                              int pow2_all, const int* __restrict__ row_band,
+                                                              const T* __restrict__ band_table, int nbands)
 {
     const int lane = threadIdx.x & 31;
     const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
@@ -761,6 +767,16 @@ __global__ void __launch_bounds__(256) sx_upwind_chunk_kernel(const int* __restr
         const int4 p0 = __ldg(pl), p1 = __ldg(pl + 1), p2 = __ldg(pl + 2), p3 = __ldg(pl + 3);
         const int x0 = p0.x, ie = p0.y, touch = p0.w, ib = p3.w;
         const long long c0 = p0.z;
+        T dt = dt_all, dx = dx_all, dy = dy_all;
+        int pow2 = pow2_all;
+        if (BANDS) {
+            const int q = __ldg(row_band + p3.z);
+            if (q < 0 || q >= nbands) continue;
+            dx = __ldg(band_table + 4 * q);
+            dy = __ldg(band_table + 4 * q + 1);
+            dt = __ldg(band_table + 4 * q + 2);
+            pow2 = __ldg(band_table + 4 * q + 3) != (T)0;
+        }
         T cen[SX_CHUNK_SUB];
 #pragma unroll
         for (int q = 0; q < SX_CHUNK_SUB; ++q) {
@@ -1498,17 +1514,56 @@ cudaError_t sx_upwind_chunk_launch(const int* off, const int* b, const int* e, c
     if (dbl) {
         double ddx = dx, ddy = dy;
         const int p = sx_pow2_pair(ddx, ddy);
-        sx_upwind_chunk_kernel<double><<<(int)blocks, 256, 0, stream>>>(off, b, e, coff, info, chunks, lookup,
-                                                                        (const double*)v, (double*)out, width, height,
-                                                                        a, bb, dt, ddx, ddy, p);
+        sx_upwind_chunk_kernel<double, false><<<(int)blocks, 256, 0, stream>>>(
+            off, b, e, coff, info, chunks, lookup, (const double*)v, (double*)out, width, height, a, bb, dt, ddx, ddy,
+            p, nullptr, nullptr, 0);
     } else {
         float fdx = (float)dx, fdy = (float)dy;
         const int p = sx_pow2_pair(fdx, fdy);
-        sx_upwind_chunk_kernel<float><<<(int)blocks, 256, 0, stream>>>(off, b, e, coff, info, chunks, lookup,
-                                                                       (const float*)v, (float*)out, width, height,
-                                                                       (float)a, (float)bb, (float)dt, fdx, fdy, p);
+        sx_upwind_chunk_kernel<float, false><<<(int)blocks, 256, 0, stream>>>(
+            off, b, e, coff, info, chunks, lookup, (const float*)v, (float*)out, width, height, (float)a, (float)bb,
+            (float)dt, fdx, fdy, p, nullptr, nullptr, 0);
     }
     return cudaGetLastError();
+}
+
+cudaError_t sx_upwind_chunk_bands_launch(const int* off, const int* b, const int* e, const int* coff, const int* info,
+                                         long long chunks, const int* lookup, const void* v, void* out, int width,
+                                         int height, double a, double bb, const int* row_band, const void* band_table,
+                                         int nbands, int dbl, cudaStream_t stream)
+{
+    if (chunks <= 0) return cudaSuccess;
+    long long blocks = (chunks + 7) / 8;
+    if (blocks > 148 * 64) blocks = 148 * 64;
+    if (dbl)
+        sx_upwind_chunk_kernel<double, true><<<(int)blocks, 256, 0, stream>>>(
+            off, b, e, coff, info, chunks, lookup, (const double*)v, (double*)out, width, height, a, bb, 0.0, 1.0, 1.0,
+            0, row_band, (const double*)band_table, nbands);
+    else
+        sx_upwind_chunk_kernel<float, true><<<(int)blocks, 256, 0, stream>>>(
+            off, b, e, coff, info, chunks, lookup, (const float*)v, (float*)out, width, height, (float)a, (float)bb,
+            0.0f, 1.0f, 1.0f, 0, row_band, (const float*)band_table, nbands);
+    return cudaGetLastError();
+}
+
+// Host: per-band table of the banded launch in the kernel's precision.
+template <typename T>
+static void sx_band_table_fill(const double* spacing, int nbands, T* table)
+{
+    for (int q = 0; q < nbands; ++q) {
+        T dx = (T)spacing[3 * q], dy = (T)spacing[3 * q + 1];
+        const int p = sx_pow2_pair(dx, dy);
+        table[4 * q] = dx;
+        table[4 * q + 1] = dy;
+        table[4 * q + 2] = (T)spacing[3 * q + 2];
+        table[4 * q + 3] = (T)p;
+    }
+}
+
+void sx_upwind_band_table_fill(int dbl, const double* spacing, int nbands, void* table)
+{
+    if (dbl) sx_band_table_fill<double>(spacing, nbands, (double*)table);
+    else sx_band_table_fill<float>(spacing, nbands, (float*)table);
 }
 
 int sx_upwind_adjoint_chunk_parts(long long chunks)

@@ -40,6 +40,8 @@ struct SxBoolArgs {
     int tune_staging_cap;
     int tune_warps;      // segmented sweeps: warps per block
     int tune_tile_rows;  // segmented sweeps: rows per tile (at most 32; 8 for kernel 6)
+    unsigned wait_limit; // look-back polls before giving up (0: SX_LOOKBACK_SPIN_LIMIT); tests of the failure path
+    int withhold_tile;   // t + 1: tile t never publishes its look-back status (tests of the failure path)
 };
 
 struct SxRowList {
@@ -147,6 +149,11 @@ cudaError_t sx_upwind_plan_fill_launch(const int* rows, const int* off, int row_
 cudaError_t sx_upwind_chunk_launch(const int* off, const int* b, const int* e, const int* coff, const int* info,
                                    long long chunks, const int* lookup, const void* v, void* out, int width, int height,
                                    double a, double bb, double dt, double dx, double dy, int dbl, cudaStream_t stream);
+cudaError_t sx_upwind_chunk_bands_launch(const int* off, const int* b, const int* e, const int* coff, const int* info,
+                                         long long chunks, const int* lookup, const void* v, void* out, int width,
+                                         int height, double a, double bb, const int* row_band, const void* band_table,
+                                         int nbands, int dbl, cudaStream_t stream);
+void sx_upwind_band_table_fill(int dbl, const double* spacing, int nbands, void* table);
 int sx_upwind_adjoint_chunk_parts(long long chunks);
 cudaError_t sx_upwind_adjoint_chunk_launch(const int* off, const int* b, const int* e, const int* coff, const int* info,
                                            long long chunks, const int* lookup, const void* w, const void* u,

@@ -17,7 +17,11 @@
 // fault or, where the GPU can reach host memory, use the wrong memory.  The
 // real device address is fetched once per device with
 // cudaGetSymbolAddress, with that device current, on the first call made
-// on it.
+// on it (so that first call should come before any stream capture).  The
+// address is kept together with the CUDA context it was fetched in; after a
+// device reset, or when the primary context was destroyed and created
+// again, the next call sees a different context and fetches it anew instead
+// of writing through a stale address.
 
 #include <cstdio>
 #include <mutex>
@@ -37,6 +41,28 @@ namespace {
 
 std::mutex g_static_mutex;
 void* g_static_ptr[SX_STATIC_MAX_DEVICES] = {nullptr};
+void* g_static_ctx[SX_STATIC_MAX_DEVICES] = {nullptr};
+
+// The current driver context, reached through the runtime's entry-point
+// query so that the library needs no link against the driver library.
+typedef int (*CtxGetCurrentFn)(void**);
+
+void* current_context()
+{
+    static CtxGetCurrentFn fn = nullptr;
+    static bool looked = false;
+    if (!looked) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (CtxGetCurrentFn)p;
+        looked = true;
+    }
+    void* ctx = nullptr;
+    if (fn && fn(&ctx) != 0) ctx = nullptr;
+    return ctx;
+}
 
 }  // namespace
 
@@ -63,8 +89,13 @@ extern "C" int sx_bool_eval_static(const sx_leaf* leaves, int k, int32_t rows, c
     void* scratch = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_static_mutex);
+        if (g_static_ptr[dev]) {
+            // a cached address is valid only in the context it was fetched in
+            void* ctx = current_context();
+            if (ctx != g_static_ctx[dev]) g_static_ptr[dev] = nullptr;
+        }
         if (!g_static_ptr[dev]) {
-            // once per device, with that device current
+            // once per device (and context), with that device current
             err = cudaGetSymbolAddress(&g_static_ptr[dev], sx_static_scratch);
             if (err != cudaSuccess) {
                 g_static_ptr[dev] = nullptr;
@@ -72,6 +103,7 @@ extern "C" int sx_bool_eval_static(const sx_leaf* leaves, int k, int32_t rows, c
                 snprintf(msg, sizeof(msg), "sx_bool_eval_static: cudaGetSymbolAddress: %s", cudaGetErrorString(err));
                 return sx_set_error(SX_ERR_CUDA, msg);
             }
+            g_static_ctx[dev] = current_context();
         }
         scratch = g_static_ptr[dev];
     }

@@ -1169,13 +1169,14 @@ __device__ __forceinline__ bool sxs_bar_wait(unsigned long long* bar)
 // Wait until a tile status word is published, backing off from 32 ns to
 // 512 ns between polls so that waiting warps leave the issue slots to the
 // warps that sweep; bounded by SX_LOOKBACK_SPIN_LIMIT polls.
-__device__ __forceinline__ unsigned long long sxs_wait_status(const unsigned long long* p, bool& timed_out)
+__device__ __forceinline__ unsigned long long sxs_wait_status(const unsigned long long* p, bool& timed_out,
+                                                             unsigned limit)
 {
     unsigned sleep = 32;
     for (unsigned spins = 0;; ++spins) {
         const unsigned long long w = sx_ld_status(p);
         if ((w >> 32) & 3ull) return w;
-        if (spins > SX_LOOKBACK_SPIN_LIMIT) {
+        if (spins > limit) {
             timed_out = true;
             return (SX_KIND_PREFIX << 32);  // treat as a zero prefix so the kernel finishes
         }
@@ -1191,22 +1192,28 @@ __device__ __forceinline__ unsigned long long sxs_wait_status(const unsigned lon
 // its 32 nearest predecessors at once (each wait bounded) and adds values up
 // to the nearest inclusive prefix, 32 tiles per step.  Returns the exclusive
 // prefix; `flags` comes back as the OR over this tile and all before it.
-__device__ __forceinline__ int sxs_lookback(const SxSweepState& st, int tile, int aggregate, unsigned& flags)
+// A.wait_limit (when set) bounds every wait instead of SX_LOOKBACK_SPIN_LIMIT,
+// and the tile A.withhold_tile - 1 publishes nothing: both exist only so that
+// tests can make the waits give up.
+__device__ __forceinline__ int sxs_lookback(const SxBoolArgs& A, const SxSweepState& st, int tile, int aggregate,
+                                            unsigned& flags)
 {
     const int lane = threadIdx.x & 31;
+    const unsigned limit = A.wait_limit ? A.wait_limit : SX_LOOKBACK_SPIN_LIMIT;
+    const bool publish = A.withhold_tile != tile + 1;
     const unsigned long long own = ((unsigned long long)(flags & 15u) << 34) | (unsigned long long)(unsigned)aggregate;
     if (tile == 0) {
-        if (lane == 0) atomicExch(&st.tile_status[0], own | (SX_KIND_PREFIX << 32));
+        if (lane == 0 && publish) atomicExch(&st.tile_status[0], own | (SX_KIND_PREFIX << 32));
         return 0;
     }
-    if (lane == 0) atomicExch(&st.tile_status[tile], own | (SX_KIND_AGG << 32));
+    if (lane == 0 && publish) atomicExch(&st.tile_status[tile], own | (SX_KIND_AGG << 32));
     int exclusive = 0;
     unsigned fl = flags;
     bool timed_out = false;
     for (int pos = tile - 1;; pos -= 32) {
         const int t = pos - lane;
         unsigned long long w = SX_KIND_PREFIX << 32;  // before tile 0: an empty prefix
-        if (t >= 0) w = sxs_wait_status(&st.tile_status[t], timed_out);
+        if (t >= 0) w = sxs_wait_status(&st.tile_status[t], timed_out, limit);
         const unsigned pm = __ballot_sync(0xFFFFFFFFu, ((w >> 32) & 3ull) == SX_KIND_PREFIX);
         const int stop = pm ? __ffs(pm) - 1 : 32;
         int v = lane <= stop ? (int)(unsigned)(w & 0xFFFFFFFFull) : 0;
@@ -1221,7 +1228,7 @@ __device__ __forceinline__ int sxs_lookback(const SxSweepState& st, int tile, in
         if (pm) break;
     }
     if (__any_sync(0xFFFFFFFFu, timed_out)) fl |= SXF_TIMEOUT;
-    if (lane == 0)
+    if (lane == 0 && publish)
         atomicExch(&st.tile_status[tile], ((unsigned long long)(fl & 15u) << 34) | (SX_KIND_PREFIX << 32) |
                                               (unsigned long long)(unsigned)(exclusive + aggregate));
     flags = fl;
@@ -1593,7 +1600,7 @@ __global__ void __launch_bounds__(SXS_MAX_THREADS) sx_seg_kernel(SxBoolArgs A, S
     //    its output boundaries from the output area into the key area
     if (wid == 0) {
         unsigned f = S.flags;
-        const int base = sxs_lookback(st, tile, total >> 1, f);
+        const int base = sxs_lookback(A, st, tile, total >> 1, f);
         if (lane == 0) {
             S.base = base;
             S.flags = f;
@@ -1896,7 +1903,7 @@ __global__ void __launch_bounds__(256) sx_wseg_kernel(SxBoolArgs A, SxSweepState
         total = 2 * tot;
     }
     // 6. look-back, then pack the output boundaries into the key area
-    const int base = sxs_lookback(st, tile, total >> 1, flags);
+    const int base = sxs_lookback(A, st, tile, total >> 1, flags);
     bool over = false;
     if (staged) {
         unsigned* packed = Wd + (int)RNl;  // the key lists are dead after the sweep
@@ -2240,7 +2247,7 @@ __global__ void __launch_bounds__(256, K <= 5 ? 5 : 4) sx_wseg16_kernel(SxBoolAr
         total = 2 * tot;
     }
     // 6. look-back, then pack the output boundaries over the dead key lists
-    const int base = sxs_lookback(st, tile, total >> 1, flags);
+    const int base = sxs_lookback(A, st, tile, total >> 1, flags);
     bool over = false;
     if (staged) {
         unsigned short* packed = h16;

@@ -173,3 +173,43 @@ def test_fused_step_any_width(cuda_device, res, dtype):
     for lvl in ("coarse_values", "fine_values"):
         assert torch.equal(getattr(runs[0], lvl), getattr(runs[1], lvl)), lvl
 
+
+
+def test_batched_upwind_per_set_spacing_and_graph_step(cuda_device):
+    """Config 4's form: every set with dx = 1/side and its own CFL time step, against the oracle per set;
+    the graph-captured BatchStep equals the direct calls."""
+    from subsetix_b200 import synth
+    from subsetix_b200.batch import BatchStep, SetBatch, batched_binary, batched_upwind
+    from tests.gpu_util import dev_set, iset
+
+    sides, sets_a = synth.batched_uneven_sets(count=20, seed=3, side_hi=700)
+    _, sets_b = synth.batched_uneven_sets(count=20, seed=4, side_hi=700)
+    A = SetBatch.from_sets([dev_set(h) for h in sets_a], sides)
+    B = SetBatch.from_sets([dev_set(h) for h in sets_b], sides)
+    rng = np.random.default_rng(11)
+    fields, values = [], []
+    for h in sets_a:
+        f = O.create_field(iset(h), 0.0, np.float32)
+        f.values[...] = rng.uniform(0, 1, f.values.size).astype(np.float32)
+        fields.append(f)
+        values.append(f.values)
+    vals = torch.as_tensor(np.concatenate(values), device="cuda")
+    dx = [1.0 / s for s in sides]
+    dt = [0.5 / (1.0 / d + 0.5 / d) for d in dx]
+    got = _vals(batched_upwind(A, vals, width=sides, a=1.0, b=0.5, dt=dt, dx=dx, dy=dx))
+    pos = 0
+    for f, side, h, t in zip(fields, sides, dx, dt):
+        exp = O.upwind(f, width=side, height=side, a=1.0, b=0.5, dt=t, dx=h, dy=h)
+        np.testing.assert_array_equal(got[pos:pos + exp.size], exp)
+        pos += exp.size
+    step = BatchStep(A, B, vals, width=sides, a=1.0, b=0.5, dt=dt, dx=dx, dy=dx)
+    step()
+    g = step.graph()
+    step.out.zero_()
+    g.replay()
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(_vals(step.out), got)
+    for mine, ref in ((step.union(), batched_binary(A, B, "union")),
+                      (step.intersection(), batched_binary(A, B, "intersection"))):
+        for x, y in zip(mine.split(), ref.split()):
+            assert_same(x, tuple(t.cpu().numpy() for t in (y.begin, y.end, y.row_offsets, y.rows)))

@@ -87,3 +87,67 @@ def test_static_scratch_rejects_oversized_input(cuda_device):
                                  stream_handle(cuda_device))
     assert rc == _lib.SX_ERR_CAPACITY
     assert "3944448" in _lib.last_error()
+
+
+def _sparse_rows(rng, rows, mean):
+    """Vectorised random rows: Poisson(mean) intervals per row, gaps and lengths of at least one cell."""
+    counts = rng.poisson(mean, rows)
+    n = int(counts.sum())
+    off = np.zeros(rows + 1, np.int64)
+    np.cumsum(counts, out=off[1:])
+    steps = rng.geometric(1 / 4.0, size=2 * n).reshape(n, 2)
+    row_of = np.repeat(np.arange(rows), counts)
+    # positions restart at every row: cumulative sums within each row
+    flat = steps.reshape(-1).cumsum()
+    start_of_row = np.zeros(rows, np.int64)
+    first = off[:-1][counts > 0]
+    base = np.where(first > 0, flat[2 * first - 1], 0)
+    start_of_row[counts > 0] = base
+    pos = flat - np.repeat(start_of_row[row_of], 2)
+    b = pos[0::2].astype(np.int32)
+    e = pos[1::2].astype(np.int32)
+    return b, e, off.astype(np.int32)
+
+
+def test_static_scratch_large_input_takes_32_row_tiles(cuda_device):
+    """Above about a million rows the built-in array holds only 32-row tiles' look-back state."""
+    lib = _lib.load()
+    rng = np.random.default_rng(21)
+    rows = 1_100_000
+    leaves = [tuple(torch.as_tensor(a, device=cuda_device) for a in _sparse_rows(rng, rows, m)) for m in (0.6, 1.0, 1.4)]
+    specs = [(b, e, off, 0) for b, e, off in leaves]
+    ob, oe, ooff, total, flags = _core.bool_eval(specs, rows, TABLE, _lib.MODE_TABLE, cuda_device)
+    assert flags == 0
+    for _ in range(2):
+        got_b, got_e, got_off, got_flags = _static_call(lib, leaves, rows, cuda_device)
+        assert got_flags == 0
+        assert torch.equal(got_b, ob[:total].cpu())
+        assert torch.equal(got_e, oe[:total].cpu())
+        assert torch.equal(got_off, ooff.cpu())
+
+
+def test_static_scratch_union_mode(cuda_device):
+    """The merged union of widened leaves (the dilation sweep) through the static entry point."""
+    lib = _lib.load()
+    rows, leaves = _leaves(cuda_device, 13)
+    arr = (_lib.SxLeaf * len(leaves))()
+    for i, (b, e, off) in enumerate(leaves):
+        arr[i].begin, arr[i].end, arr[i].row_offsets, arr[i].widen = ptr(b), ptr(e), ptr(off), i
+    specs = [(b, e, off, i) for i, (b, e, off) in enumerate(leaves)]
+    ob, oe, ooff, total, flags = _core.bool_eval(specs, rows, [0] * 8, _lib.MODE_UNION, cuda_device)
+    assert flags == 0
+    cap = max(1, sum(int(b.numel()) for b, _, _ in leaves))
+    for _ in range(2):
+        sb = torch.full((cap,), -7, dtype=torch.int32, device=cuda_device)
+        se = torch.full((cap,), -7, dtype=torch.int32, device=cuda_device)
+        soff = torch.full((rows + 1,), -7, dtype=torch.int32, device=cuda_device)
+        res = torch.full((2,), -7, dtype=torch.int32, device=cuda_device)
+        tab = (ctypes.c_uint32 * 8)(*([0] * 8))
+        rc = lib.sx_bool_eval_static(arr, len(leaves), rows, tab, _lib.MODE_UNION, ptr(sb), ptr(se), ptr(soff), cap,
+                                     ptr(res), stream_handle(cuda_device))
+        assert rc == _lib.SX_OK, _lib.last_error()
+        n, f = (int(x) for x in res.cpu())
+        assert f == 0 and n == total
+        assert torch.equal(sb[:n].cpu(), ob[:total].cpu())
+        assert torch.equal(se[:n].cpu(), oe[:total].cpu())
+        assert torch.equal(soff.cpu(), ooff.cpu())
