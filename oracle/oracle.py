@@ -618,6 +618,27 @@ def gradient_tag_threshold(values, width, height, threshold, epsilon=1e-8) -> IS
                                max(float(threshold), float(epsilon)))
 
 
+def gradient_tag_set(values, width, height, frac_high, epsilon=1e-8) -> ISet:
+    """Runs of the top ``frac_high`` fraction of the positive values (regrid.py:353-383).
+
+    The threshold is the value of rank ``n - ceil(n * frac)`` among the
+    ``n`` values above ``epsilon`` (a k-th order statistic, the same for any
+    partition algorithm); cells with ``value >= max(threshold, epsilon)`` are
+    tagged.
+    """
+    frac = float(max(0.0, min(1.0, frac_high)))
+    if frac <= 0.0:
+        return ISet(np.zeros(0, I32), np.zeros(0, I32), np.zeros(height + 1, I32), np.arange(height, dtype=I32))
+    v = np.asarray(values, np.float32).reshape(-1)
+    pos = v[v > np.float32(epsilon)]
+    if pos.size == 0:
+        return ISet(np.zeros(0, I32), np.zeros(0, I32), np.zeros(height + 1, I32), np.arange(height, dtype=I32))
+    count = max(1, min(int(pos.size), int(np.ceil(pos.size * frac))))
+    idx = int(pos.size) - count
+    thr = float(np.partition(pos, idx)[idx])
+    return threshold_intervals(v, width, height, max(thr, float(epsilon)))
+
+
 def grading(refine: ISet, padding: int = 1, mode: str = "von_neumann", *, width: int, height: int) -> ISet:
     """Two-level grading dilation (regrid.py:404-442)."""
     padding = int(padding)

@@ -100,11 +100,17 @@ def domain_set(rng, width, height, max_per_row=4):
             np.asarray(offsets, np.int32), np.arange(height, dtype=np.int32))
 
 
+FILES = ("setops", "morph", "multilevel", "stencil_regrid", "amr", "levels", "amr_large")
+
+
 def main():
     parser = argparse.ArgumentParser()
     parser.add_argument("--reference", default="/root/reference")
+    parser.add_argument("--only", nargs="*", choices=FILES, default=list(FILES),
+                        help="write only these fixture files (each file's inputs come from its own seeds)")
     args = parser.parse_args()
     _setup(args.reference)
+    only = set(args.only)
 
     import cupy as cp  # the NumPy-backed stand-in
     import subsetix_cupy as sc
@@ -198,7 +204,8 @@ def main():
         put_host(rec, f"shape512/{name}", host)
     leaves = {name: mk(h) for name, h in zip("ABCDE", shapes)}
     rec.put_set("shape512/e0", sc.evaluate(build(exprs["e0"], leaves)))
-    rec.save("setops.npz")
+    if "setops" in only:
+        rec.save("setops.npz")
 
     # ------------------------------------------------------------- morphology
     rec = Recorder()
@@ -223,7 +230,8 @@ def main():
         rec.put_set(f"cfg1/dilate_{hx}_{hy}", sx_morph.dilate_interval_set(A, halo_x=hx, halo_y=hy))
         rec.put_set(f"cfg1/erode_{hx}_{hy}", sx_morph.erode_interval_set(A, halo_x=hx, halo_y=hy, width=256, height=256))
     put_host(rec, "cfg1/A", a_host)
-    rec.save("morph.npz")
+    if "morph" in only:
+        rec.save("morph.npz")
 
     # ------------------------------------------------------------- multilevel
     rec = Recorder()
@@ -272,7 +280,8 @@ def main():
                 rec.put(f"f{fcase}/restrict_{r}_{red}/values", out.values)
         fcase += 1
     rec.put("field_count", np.array(fcase))
-    rec.save("multilevel.npz")
+    if "multilevel" in only:
+        rec.save("multilevel.npz")
 
     # ----------------------------------------------------- stencil and regrid
     rec = Recorder()
@@ -315,7 +324,8 @@ def main():
                     tags, padding=pad, mode=mode, width=width, height=height))
             gcase += 1
     rec.put("regrid_count", np.array(gcase))
-    rec.save("stencil_regrid.npz")
+    if "stencil_regrid" in only:
+        rec.save("stencil_regrid.npz")
 
     # ---------------------------------------------------------- AMR drivers
     rec = Recorder()
@@ -356,7 +366,90 @@ def main():
                                                     min_level=2, max_level=3, refine_threshold=0.05, grading=1), init_fn)
     rec.put("runner/coarse", field.coarse_field.values)
     rec.put("runner/fine", field.fine_field.values)
-    rec.save("amr.npz")
+    if "amr" in only:
+        rec.save("amr.npz")
+
+    # ------------------------------------------- percentile tagging and level helpers
+    if "levels" in only:
+        lrng = np.random.default_rng(4321)
+        rec = Recorder()
+        tcase = 0
+        for width, height in [(4, 4), (16, 12), (40, 33)]:
+            for kind in ("golden", "uniform", "signed", "zeros"):
+                if kind == "golden" and (width, height) != (4, 4):
+                    continue
+                data = np.zeros((height, width), np.float32)
+                if kind == "golden":  # test_regrid.py:58-66
+                    data[1, 1], data[2, 2] = 0.5, 1.0
+                elif kind == "uniform":
+                    data = lrng.uniform(0, 1, (height, width)).astype(np.float32)
+                elif kind == "signed":
+                    data = lrng.standard_normal((height, width)).astype(np.float32)
+                full = sx_morph.full_interval_set(width, height)
+                field = create_interval_field(full, fill_value=0.0, dtype=cp.float32)
+                field.values[...] = cp.asarray(data.ravel())
+                rec.put(f"t{tcase}/data", data)
+                fracs = (0.0, 0.01, 0.2, 0.5, 1.0, 1.5)
+                rec.put(f"t{tcase}/fracs", np.array(fracs))
+                for j, frac in enumerate(fracs):
+                    rec.put_set(f"t{tcase}/tag_{j}", sx_regrid.gradient_tag_set(field, width=width, height=height,
+                                                                               frac_high=frac))
+                tcase += 1
+        rec.put("tag_count", np.array(tcase))
+        # three-level hierarchies: prolong / restrict of sets and fields, covered cells, coarse-only sets
+        hcase = 0
+        for _ in range(8):
+            base = random_small_set(lrng, row_lo=0, row_hi=12, max_rows=8, min_per_row=1)
+            put_host(rec, f"h{hcase}/base", base)
+            ml = sx_ml.MultiLevel2D.create(3, base_ratio=2)
+            ml.set_level(0, mk(base))
+            rec.put_set(f"h{hcase}/l1", sx_ml.prolong_level_sets(ml, 0))
+            rec.put_set(f"h{hcase}/l2", sx_ml.prolong_level_sets(ml, 1))
+            rec.put_set(f"h{hcase}/covered0", sx_ml.covered_by_fine(ml, 0))
+            rec.put_set(f"h{hcase}/coarse_only0", sx_ml.coarse_only(ml.get_level(0), ml, 0))
+            rec.put_set(f"h{hcase}/restricted1", sx_ml.restrict_level_sets(ml, 1))
+            mf = sx_ml.MultiLevelField2D.create_from_geometry(ml, fill_value=0.0, dtype=cp.float32)
+            f0 = mf.get_level_field(0)
+            f0.values[...] = cp.asarray(lrng.standard_normal(int(f0.values.size)).astype(np.float32))
+            rec.put(f"h{hcase}/f0", f0.values)
+            try:
+                rec.put(f"h{hcase}/pf1", sx_ml.prolong_level_field(ml, mf, 0).values)
+                rec.put(f"h{hcase}/pf2", sx_ml.prolong_level_field(ml, mf, 1).values)
+                f2 = mf.get_level_field(2)
+                f2.values[...] = cp.asarray(lrng.standard_normal(int(f2.values.size)).astype(np.float32))
+                rec.put(f"h{hcase}/f2", f2.values)
+                for red in ("mean", "max"):
+                    rec.put(f"h{hcase}/rf1_{red}", sx_ml.restrict_level_field(ml, mf, 1, reducer=red).values)
+            except Exception as exc:
+                rec.put_error(f"h{hcase}/fields", exc)
+            hcase += 1
+        rec.put("hier_count", np.array(hcase))
+        rec.save("levels.npz")
+
+    # --------------------------------- two-level AMR at a stated size, physical threshold
+    if "amr_large" in only:
+        rec = Recorder()
+        res, steps, every = 128, 40, 10
+        thr = 0.05 / res  # the physical gradient threshold 0.05 on the reference's per-cell difference
+        config = SimulationConfig(coarse_resolution=res, velocity=(1.0, 0.5), cfl=0.5, refine_threshold=thr,
+                                  grading=1)
+        sim = AMR2Simulation(config)
+        full = sx_morph.full_interval_set(res, res)
+        field = create_interval_field(full, fill_value=0.0, dtype=cp.float32)
+        xs = (np.arange(res) + 0.5) / res
+        gx, gy = np.meshgrid(xs, xs)
+        u0 = np.exp(-((gx - 0.5) ** 2 + (gy - 0.5) ** 2) / (2 * 0.05 ** 2)).astype(np.float32)
+        field.values[...] = cp.asarray(u0.ravel())
+        sim.set_initial_field(field)
+        rec.put("g128/u0", u0)
+        rec.put("g128/params", np.array([res, steps, every, 1.0, 0.5, sim.dt, thr], dtype=np.float64))
+        rec.put_set("g128/refine0", sim.state.actions.refine_set())
+        state, _ = sim.run(steps=steps, regrid_every=every)
+        rec.put("g128/coarse", state.coarse_field.values)
+        rec.put("g128/fine", state.fine_field.values)
+        rec.put_set("g128/refine", state.actions.refine_set())
+        rec.put_set("g128/coarse_only", state.geometry.coarse_only)
+        rec.save("amr_large.npz")
 
 
 if __name__ == "__main__":

@@ -233,3 +233,28 @@ def test_vtk_export(cuda_device, tmp_path):
     assert files == ["amr2_mesh_step0000.vtu", "amr2_mesh_step0001.vtu"]
     text = (tmp_path / files[0]).read_text()
     assert "UnstructuredGrid" in text and 'Name="value"' in text
+
+
+def test_amr2_simulation_128_physical_threshold(cuda_device):
+    """Config 3's loop at 128^2 with the physical threshold 0.05 dx (12 % of the cells refined), 40 steps,
+    regrid every 10: the drop-in AMR2Simulation and the fused engine against the reference's own run."""
+    from subsetix_b200.subsetix_amr2.fused import FusedTwoLevelAMR
+
+    data = load("amr_large.npz")
+    res, steps, every, va, vb, dt, thr = data["g128/params"].tolist()
+    res, steps, every = int(res), int(steps), int(every)
+    u0 = data["g128/u0"]
+    sim = amr.AMR2Simulation(amr.SimulationConfig(coarse_resolution=res, velocity=(va, vb), cfl=0.5,
+                                                  refine_threshold=thr, grading=1))
+    assert sim.dt == dt
+    sim.set_initial_field(_grid_field(u0))
+    assert_same(sim.state.actions.refine_set(), get_set(data, "g128/refine0"))
+    state, _ = sim.run(steps=steps, regrid_every=every)
+    np.testing.assert_array_equal(_vals(state.coarse_field.values), data["g128/coarse"])
+    np.testing.assert_array_equal(_vals(state.fine_field.values), data["g128/fine"])
+    assert_same(state.actions.refine_set(), get_set(data, "g128/refine"))
+    assert_same(state.geometry.coarse_only, get_set(data, "g128/coarse_only"))
+    eng = FusedTwoLevelAMR(torch.as_tensor(u0, device="cuda"), velocity=(va, vb), cfl=0.5, refine_threshold=thr)
+    eng.run(steps, regrid_every=every)
+    np.testing.assert_array_equal(_vals(eng.coarse_values).reshape(-1), data["g128/coarse"])
+    np.testing.assert_array_equal(_vals(eng.fine_values).reshape(-1), data["g128/fine"])

@@ -329,3 +329,50 @@ def test_upwind_padded_cell_offsets(cuda_device):
     got = sc.step_upwind_interval(fp, **kw).cpu().numpy()
     for i in range(lens.size):
         assert np.array_equal(got[padded[i]:padded[i] + lens[i]], ref[packed[i]:packed[i + 1]])
+
+
+# ------------------------------------------------ percentile tagging and level helpers (reference fixtures)
+
+def test_percentile_tagging_fixture(cuda_device):
+    from subsetix_b200.subsetix_amr2 import regrid as rg
+
+    data = load("levels.npz")
+    for c in range(int(data["tag_count"])):
+        grid = data[f"t{c}/data"]
+        h, w = grid.shape
+        f = sc.create_interval_field(sc.full_interval_set(w, h), fill_value=0.0, dtype=np.float32)
+        f.values.copy_(torch.as_tensor(grid.ravel(), device="cuda"))
+        for j, frac in enumerate(data[f"t{c}/fracs"].tolist()):
+            assert_same(rg.gradient_tag_set(f, width=w, height=h, frac_high=frac), get_set(data, f"t{c}/tag_{j}"),
+                        f"t{c} frac {frac}")
+
+
+def test_level_helpers_fixture(cuda_device):
+    from subsetix_b200.subsetix_cupy import multilevel as ml_mod
+
+    data = load("levels.npz")
+    for c in range(int(data["hier_count"])):
+        ml = ml_mod.MultiLevel2D.create(3, base_ratio=2)
+        ml.set_level(0, dev_set(get_set(data, f"h{c}/base")))
+        assert_same(ml_mod.prolong_level_sets(ml, 0), get_set(data, f"h{c}/l1"))
+        assert_same(ml_mod.prolong_level_sets(ml, 1), get_set(data, f"h{c}/l2"))
+        assert_same(ml_mod.covered_by_fine(ml, 0), get_set(data, f"h{c}/covered0"))
+        assert_same(ml_mod.coarse_only(ml.get_level(0), ml, 0), get_set(data, f"h{c}/coarse_only0"))
+        assert_same(ml_mod.restrict_level_sets(ml, 1), get_set(data, f"h{c}/restricted1"))
+        mf = ml_mod.MultiLevelField2D.create_from_geometry(ml, fill_value=0.0, dtype=np.float32)
+        mf.get_level_field(0).values.copy_(torch.as_tensor(data[f"h{c}/f0"], device="cuda"))
+        if error(data, f"h{c}/fields"):
+            with pytest.raises(ValueError):
+                ml_mod.prolong_level_field(ml, mf, 0)
+                ml_mod.prolong_level_field(ml, mf, 1)
+            continue
+        np.testing.assert_array_equal(ml_mod.prolong_level_field(ml, mf, 0).values.cpu().numpy(), data[f"h{c}/pf1"])
+        np.testing.assert_array_equal(ml_mod.prolong_level_field(ml, mf, 1).values.cpu().numpy(), data[f"h{c}/pf2"])
+        mf.get_level_field(2).values.copy_(torch.as_tensor(data[f"h{c}/f2"], device="cuda"))
+        for red in ("mean", "max"):
+            got = ml_mod.restrict_level_field(ml, mf, 1, reducer=red).values.cpu().numpy()
+            np.testing.assert_array_equal(got, data[f"h{c}/rf1_{red}"])
+    with pytest.raises(IndexError):
+        ml_mod.prolong_level_sets(ml_mod.MultiLevel2D.create(2), 1)
+    with pytest.raises(ValueError):
+        ml_mod.MultiLevel2D(ratios=[1, 3, 4], levels=[None] * 3).validate()

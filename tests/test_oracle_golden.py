@@ -157,3 +157,51 @@ def test_amr_simulation(tag):
     assert_set_equal(sim.actions.fine_set(), get_set(g, f"{tag}/fine_set"))
     assert ulp_diff32(sim.coarse.values, g[f"{tag}/coarse"]).max() <= 8
     assert ulp_diff32(sim.fine.values, g[f"{tag}/fine"]).max() <= 8
+
+
+def test_percentile_tagging():
+    g = load("levels.npz")
+    for c in range(int(g["tag_count"])):
+        data = g[f"t{c}/data"]
+        h, w = data.shape
+        for j, frac in enumerate(g[f"t{c}/fracs"].tolist()):
+            assert_set_equal(O.gradient_tag_set(data.ravel(), w, h, frac), get_set(g, f"t{c}/tag_{j}"), f"t{c} {j}")
+
+
+def test_level_helpers():
+    g = load("levels.npz")
+    for c in range(int(g["hier_count"])):
+        l0 = iset(get_set(g, f"h{c}/base"))
+        l1 = O.prolong_set(l0, 2)
+        l2 = O.prolong_set(l1, 2)
+        assert_set_equal(l1, get_set(g, f"h{c}/l1"))
+        assert_set_equal(l2, get_set(g, f"h{c}/l2"))
+        covered = O.restrict_set(l1, 2)
+        assert_set_equal(covered, get_set(g, f"h{c}/covered0"))
+        assert_set_equal(O.difference(l0, covered), get_set(g, f"h{c}/coarse_only0"))
+        assert_set_equal(O.restrict_set(l2, 2), get_set(g, f"h{c}/restricted1"))
+        if error(g, f"h{c}/fields"):
+            continue
+        f0 = O.Field(l0, g[f"h{c}/f0"], O.cell_offsets(l0))
+        p1 = O.prolong_field(f0, 2)
+        np.testing.assert_array_equal(p1.values, g[f"h{c}/pf1"])
+        p2 = O.prolong_field(p1, 2)
+        np.testing.assert_array_equal(p2.values, g[f"h{c}/pf2"])
+        f2 = O.Field(p2.iset, g[f"h{c}/f2"], p2.offsets)
+        for red in ("mean", "max"):
+            assert ulp_diff32(O.restrict_field(f2, 2, red).values, g[f"h{c}/rf1_{red}"]).max(initial=0) <= FP32_ULP
+
+
+def test_amr_simulation_128_physical_threshold():
+    """Config 3's loop at 128^2 with the physical threshold 0.05 dx (12 % refined), 40 steps."""
+    g = load("amr_large.npz")
+    res, steps, every, va, vb, dt, thr = g["g128/params"].tolist()
+    sim = O.AMR2(int(res), (va, vb), cfl=0.5, threshold=thr, grading_pad=1)
+    assert abs(sim.dt - dt) < 1e-15
+    sim.init(g["g128/u0"])
+    assert_set_equal(sim.actions.refine, get_set(g, "g128/refine0"))
+    sim.run(int(steps), int(every))
+    assert_set_equal(sim.actions.refine, get_set(g, "g128/refine"))
+    assert_set_equal(sim.coarse_only, get_set(g, "g128/coarse_only"))
+    assert ulp_diff32(sim.coarse.values, g["g128/coarse"]).max() <= 8
+    assert ulp_diff32(sim.fine.values, g["g128/fine"]).max() <= 8
