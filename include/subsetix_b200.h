@@ -450,6 +450,17 @@ int sx_value_runs(int type, const void* values, const int32_t* cell_offsets, int
 /* dst[p] = src[index[p]] for p < count (row offsets of derived sets). */
 int sx_gather_i32(const int32_t* index, int32_t count, const int32_t* src, int32_t* dst, void* stream);
 
+/* VTK export of an interval field (subsetix_cupy/export_vtk.py:205-316, the
+ * quads of _interval_field_chunk): for every cell c (value order) four corner
+ * points (x, y, 0) into points[12 c .. 12 c + 11] and its value as float32
+ * into out_values[c].  Corners in float32, each operation rounded once:
+ * x_left = ox + col * dx, x_right = x_left + dx, y_bottom = oy + row * dy,
+ * y_top = y_bottom + dy.  dtype SX_F32 or SX_F64 for `values`. */
+int sx_cell_quads(int dtype, const int32_t* row_offsets, const int32_t* rows, int32_t row_count,
+                  const int32_t* begin, const int32_t* end, const int32_t* cell_offsets, int32_t n,
+                  const void* values, float dx, float dy, float ox, float oy, float* points, float* out_values,
+                  void* stream);
+
 /* ---------------------------------------------------------------------------
  * Coupling of nested levels by index tables, for the composite multi-level
  * advection and its adjoint (subsetix_b200/adjoint.py).  dtype SX_F32 or

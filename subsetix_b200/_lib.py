@@ -137,6 +137,8 @@ _SIGNATURES = {
     "sx_upwind_chunked_bands": (ctypes.c_int, [ctypes.c_int, c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.c_int64, c_vp, c_vp,
                                                c_vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
                                                c_vp, c_vp, ctypes.c_int32, c_vp]),
+    "sx_cell_quads": (ctypes.c_int, [ctypes.c_int, c_vp, c_vp, ctypes.c_int32, c_vp, c_vp, c_vp, ctypes.c_int32, c_vp,
+                                     ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, c_vp, c_vp, c_vp]),
     "sx_index_copy": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "sx_index_block_mean": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, ctypes.c_int32, ctypes.c_double, c_vp, c_vp,
                                            c_vp, c_vp, c_vp]),

@@ -722,6 +722,22 @@ int sx_gather_i32(const int32_t* index, int32_t count, const int32_t* src, int32
     return SX_OK;
 }
 
+int sx_cell_quads(int dtype, const int32_t* row_offsets, const int32_t* rows, int32_t row_count,
+                  const int32_t* begin, const int32_t* end, const int32_t* cell_offsets, int32_t n,
+                  const void* values, float dx, float dy, float ox, float oy, float* points, float* out_values,
+                  void* stream)
+{
+    if (dtype != SX_F32 && dtype != SX_F64) return fail(SX_ERR_INVALID, "sx_cell_quads: dtype %d", dtype);
+    if (n < 0 || row_count < 0) return fail(SX_ERR_INVALID, "sx_cell_quads: negative size");
+    if (n == 0) return SX_OK;
+    if (row_count == 0 || !row_offsets || !rows || !begin || !end || !cell_offsets || !values || !points ||
+        !out_values)
+        return fail(SX_ERR_INVALID, "sx_cell_quads: null argument");
+    cudaError_t err = sx_cell_quads_launch(dtype, row_offsets, rows, row_count, begin, end, cell_offsets, n, values,
+                                           dx, dy, ox, oy, points, out_values, (cudaStream_t)stream);
+    return err == cudaSuccess ? SX_OK : cuda_fail(err, "sx_cell_quads");
+}
+
 static int coupling_check(const char* what, int dtype, long long n)
 {
     if (dtype != SX_F32 && dtype != SX_F64) return fail(SX_ERR_INVALID, "%s: dtype must be SX_F32 or SX_F64", what);

@@ -169,3 +169,7 @@ cudaError_t sx_index_block_mean_adj_launch(int dtype, long long n, int group, do
                                            const int* in_idx, void* out_bar, void* in_bar, cudaStream_t stream);
 cudaError_t sx_index_segment_add_launch(int dtype, long long nseg, const int* seg_off, const int* src_idx,
                                         const int* dst_idx, void* src, void* dst, int zero_src, cudaStream_t stream);
+// VTK quad assembly (sx_export.cu)
+cudaError_t sx_cell_quads_launch(int dtype, const int* off, const int* rows, int row_count, const int* b, const int* e,
+                                 const int* coff, int n, const void* v, float dx, float dy, float ox, float oy,
+                                 float* pts, float* vals, cudaStream_t stream);

@@ -3,21 +3,20 @@
 ``save_two_level_vtk`` follows ``subsetix_amr2/export.py`` of the
 reference: the coarse-only cells minus a ghost band around the refine
 region, that ghost band, the fine cells and the fine ghost band are
-gathered on the device, then written as one unstructured grid of quads
-(``.vtu``, ASCII) with cell data ``value``, ``level`` and ``ghost``.
-File output is host work and is outside the GPU path.
+gathered on the device, their quads assembled on the device, and written as
+one unstructured grid (``.vtu``, raw appended data) with cell data ``level``,
+``ghost_mask`` and ``u`` (``subsetix_cupy.export_vtk``).
 """
 
 from __future__ import annotations
 
 import os
-from typing import Dict, List, Tuple
+from typing import Dict, Tuple
 
-import numpy as np
-import torch
 
 from ..subsetix_cupy import evaluate, ghost_zones, make_difference, make_input, make_intersection
 from ..subsetix_cupy.expressions import IntervalSet, _t
+from ..subsetix_cupy.export_vtk import write_unstructured_quads_vtu
 from ..subsetix_cupy.interval_field import IntervalField
 from .fields import gather_interval_subset
 
@@ -32,63 +31,6 @@ def _interval_dimensions(field: IntervalField) -> Tuple[int, int]:
     height = int(field.interval_set.row_count)
     width = 0 if int(field.interval_set.begin.shape[0]) == 0 else int(_t(field.interval_set.end).max().item())
     return height, width
-
-
-def _quads(field: IntervalField, dx: float, dy: float):
-    """Corner points and cell values of every cell of ``field`` (host arrays)."""
-    s = field.interval_set
-    b = _t(s.begin).cpu().numpy().astype(np.int64)
-    e = _t(s.end).cpu().numpy().astype(np.int64)
-    off = _t(s.row_offsets).cpu().numpy()
-    rows = _t(s.rows).cpu().numpy().astype(np.int64)
-    vals = _t(field.values).cpu().numpy().astype(np.float64)
-    lengths = np.maximum(e - b, 0)
-    per_row = np.repeat(rows, np.diff(off))
-    ys = np.repeat(per_row, lengths)
-    starts = np.repeat(b, lengths)
-    local = np.arange(int(lengths.sum())) - np.repeat(np.cumsum(lengths) - lengths, lengths)
-    xs = starts + local
-    x0, y0 = xs * dx, ys * dy
-    pts = np.stack([np.stack([x0, y0], 1), np.stack([x0 + dx, y0], 1), np.stack([x0 + dx, y0 + dy], 1),
-                    np.stack([x0, y0 + dy], 1)], 1)
-    return pts.reshape(-1, 2), vals[: xs.size]
-
-
-def write_unstructured_quads_vtu(path: str, cells: List[tuple]) -> None:
-    """Write ``(field, level, dx, dy, ox, oy, ghost)`` chunks as one ``.vtu`` file of quads."""
-    points, values, levels, ghosts = [], [], [], []
-    for field, level, dx, dy, ox, oy, ghost in cells:
-        p, v = _quads(field, dx, dy)
-        p = p + np.array([ox, oy])
-        points.append(p)
-        values.append(v)
-        levels.append(np.full(v.size, level, np.int32))
-        ghosts.append(np.full(v.size, ghost, np.int32))
-    pts = np.concatenate(points) if points else np.zeros((0, 2))
-    val = np.concatenate(values) if values else np.zeros(0)
-    lev = np.concatenate(levels) if levels else np.zeros(0, np.int32)
-    gh = np.concatenate(ghosts) if ghosts else np.zeros(0, np.int32)
-    n = val.size
-    with open(path, "w") as f:
-        f.write('<?xml version="1.0"?>\n<VTKFile type="UnstructuredGrid" version="0.1" byte_order="LittleEndian">\n')
-        f.write(f'<UnstructuredGrid>\n<Piece NumberOfPoints="{4 * n}" NumberOfCells="{n}">\n')
-        f.write('<Points>\n<DataArray type="Float64" NumberOfComponents="3" format="ascii">\n')
-        xyz = np.concatenate([pts, np.zeros((pts.shape[0], 1))], 1)
-        np.savetxt(f, xyz, fmt="%.9g")
-        f.write("</DataArray>\n</Points>\n<Cells>\n")
-        f.write('<DataArray type="Int64" Name="connectivity" format="ascii">\n')
-        np.savetxt(f, np.arange(4 * n).reshape(-1, 4), fmt="%d")
-        f.write('</DataArray>\n<DataArray type="Int64" Name="offsets" format="ascii">\n')
-        np.savetxt(f, 4 * np.arange(1, n + 1), fmt="%d")
-        f.write('</DataArray>\n<DataArray type="UInt8" Name="types" format="ascii">\n')
-        np.savetxt(f, np.full(n, 9), fmt="%d")
-        f.write("</DataArray>\n</Cells>\n<CellData>\n")
-        for name, arr, typ, fmt in (("value", val, "Float64", "%.9g"), ("level", lev, "Int32", "%d"),
-                                    ("ghost", gh, "Int32", "%d")):
-            f.write(f'<DataArray type="{typ}" Name="{name}" format="ascii">\n')
-            np.savetxt(f, arr, fmt=fmt)
-            f.write("</DataArray>\n")
-        f.write("</CellData>\n</Piece>\n</UnstructuredGrid>\n</VTKFile>\n")
 
 
 def save_two_level_vtk(out_dir: str, base: str, step: int, *, coarse_field, fine_field, refine_set: IntervalSet,

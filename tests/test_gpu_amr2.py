@@ -231,8 +231,49 @@ def test_vtk_export(cuda_device, tmp_path):
     sim.run(steps=1, exporters=[exporter])
     files = sorted(p.name for p in tmp_path.iterdir())
     assert files == ["amr2_mesh_step0000.vtu", "amr2_mesh_step0001.vtu"]
-    text = (tmp_path / files[0]).read_text()
-    assert "UnstructuredGrid" in text and 'Name="value"' in text
+    raw = (tmp_path / files[0]).read_bytes()
+    assert b"UnstructuredGrid" in raw and b'Name="ghost_mask"' in raw and b'Name="u"' in raw
+    mesh = _read_vtu(tmp_path / files[0])
+    state = sim.state
+    # every coarse-only cell, ghost band included, appears once on level 0 with its value
+    n0 = int((mesh["level"] == 0).sum())
+    co = state.geometry.coarse_only
+    assert n0 == int((co.end - co.begin).sum())
+    assert mesh["points"].shape == (4 * mesh["u"].size, 3)
+
+
+def _read_vtu(path):
+    """The appended arrays of a raw-appended .vtu, by name (the layout the reference writes)."""
+    import re
+
+    raw = path.read_bytes()
+    head, _, data = raw.partition(b"<AppendedData encoding=\"raw\">")
+    data = data[data.index(b"_") + 1:]
+    out = {}
+    for m in re.finditer(rb'<DataArray type="(\w+)"(?: Name="(\w+)")?[^>]*offset="(\d+)"', head):
+        typ, name, off = m.group(1).decode(), (m.group(2) or b"points").decode(), int(m.group(3))
+        n = int(np.frombuffer(data[off:off + 8], "<u8")[0])
+        dt = {"Int32": "<i4", "Float32": "<f4", "UInt8": "u1"}[typ]
+        arr = np.frombuffer(data[off + 8:off + 8 + n], dt)
+        out[name] = arr.reshape(-1, 3) if name == "points" else arr
+    return out
+
+
+def test_vtk_quads_device_equal_host(cuda_device, tmp_path):
+    """Device quad assembly of an interval field equals the host assembly of the same cells as a mask."""
+    from subsetix_b200.subsetix_cupy import export_vtk as vtk
+
+    rng = np.random.default_rng(8)
+    grid = rng.uniform(-1, 1, (24, 40)).astype(np.float32)
+    f = _grid_field(grid)
+    a = vtk.interval_field_quads(f, 1, 0.125, 0.25, 0.5, -1.0, 0)
+    b = vtk.mask_quads(np.ones_like(grid, dtype=bool), grid, 1, 0.125, 0.25, 0.5, -1.0)
+    np.testing.assert_array_equal(a.points, b.points)
+    np.testing.assert_array_equal(a.values, b.values)
+    vtk.write_unstructured_quads_vtu(str(tmp_path / "m.vtu"), [(f, 1, 0.125, 0.25, 0.5, -1.0, 1)])
+    mesh = _read_vtu(tmp_path / "m.vtu")
+    np.testing.assert_array_equal(mesh["u"], grid.ravel())
+    assert set(mesh["ghost_mask"].tolist()) == {1} and set(mesh["types"].tolist()) == {9}
 
 
 def test_amr2_simulation_128_physical_threshold(cuda_device):

@@ -117,3 +117,27 @@ def test_algorithmic_bytes_counts_inputs_once_and_the_output_once():
     got = bench.algorithmic_bytes([leaf, leaf], n_out=7, r_out=4)
     want = 2 * (8 * 10 + 4 * 5 + 4 * 4) + 8 * 7 + 4 * 5 + 4 * 4
     assert got == want
+
+
+def test_vtr_and_pvd_writers(tmp_path):
+    """Rectilinear grids and collections are host files: their structure is checked without a GPU."""
+    import xml.etree.ElementTree as ET
+
+    from subsetix_b200.subsetix_cupy import export_vtk as vtk
+
+    u = np.arange(12, dtype=np.float32).reshape(3, 4)
+    vtk.write_rectilinear_grid_vtr(str(tmp_path / "a.vtr"), u, 0.5, 0.25, cell_arrays={"flag": u > 5})
+    root = ET.parse(tmp_path / "a.vtr").getroot()
+    arrays = {a.get("Name"): a for a in root.iter("DataArray")}
+    assert [float(x) for x in arrays["u"].text.split()] == u.ravel().tolist()
+    assert [int(x) for x in arrays["flag"].text.split()] == (u.ravel() > 5).astype(int).tolist()
+    assert [float(x) for x in arrays["X_COORDINATES"].text.split()] == [0.0, 0.5, 1.0, 1.5, 2.0]
+    names, entry = vtk.save_amr3_step_vtr(str(tmp_path), "s", 3, 0.5, u0=u, u1=u, u2=u, refine0=u > 6,
+                                          L1_mask=u > 2, refine1_mid=u > 8, L2_mask=u > 9, dx0=1, dy0=1, dx1=0.5,
+                                          dy1=0.5, dx2=0.25, dy2=0.25)
+    assert names == ["s_step0003_L0.vtr", "s_step0003_L1.vtr", "s_step0003_L2.vtr"] and entry == (0.5, names)
+    vtk.write_pvd(str(tmp_path / "c.pvd"), [entry])
+    sets = list(ET.parse(tmp_path / "c.pvd").getroot().iter("DataSet"))
+    assert [(d.get("part"), d.get("file")) for d in sets] == [("0", names[0]), ("1", names[1]), ("2", names[2])]
+    q = vtk.mask_quads(u > 9, u, 2, 0.25, 0.25)
+    assert q.cells == 2 and q.points.shape == (8, 3) and q.values.tolist() == [10.0, 11.0]
