@@ -29,9 +29,10 @@
 //                      or KEEP (0), as ActionField.set_from_interval_set
 //                      writes it (fields.py:520-546).
 //
-// Float formulas use explicit round-to-nearest operations, so results are
-// bit-identical to the interval kernels (and to the reference) on the same
-// inputs, in float32 and in float64.
+// Float formulas use explicit rounding intrinsics, including the float32
+// fusions the reference's NVRTC build makes (sx_upwind_update and
+// sx_grad_norm), so results are bit-identical to the interval kernels (and
+// to the reference) on the same inputs, in float32 and in float64.
 
 #include <cmath>
 
@@ -74,7 +75,7 @@ __global__ void __launch_bounds__(256) sx_upwind_full_kernel(const T* __restrict
     const T u = y + 1 < H ? v[idx + W] : (T)0;
     const T du_dx = a >= (T)0 ? sxa_over(sxa_sub(c, l), dx, pow2) : sxa_over(sxa_sub(r, c), dx, pow2);
     const T du_dy = b >= (T)0 ? sxa_over(sxa_sub(c, d), dy, pow2) : sxa_over(sxa_sub(u, c), dy, pow2);
-    o[idx] = sxa_sub(c, sxa_mul(dt, sxa_add(sxa_mul(a, du_dx), sxa_mul(b, du_dy))));
+    o[idx] = sx_upwind_update(c, du_dx, du_dy, a, b, dt);
 }
 
 // One thread per coarse cell.  R is the refinement ratio (template for the
@@ -116,7 +117,7 @@ __device__ __forceinline__ T sxa_upwind_cell(T c, T l, T r, T d, T u, T a, T b, 
 {
     const T du_dx = a >= (T)0 ? sxa_over(sxa_sub(c, l), dx, pow2) : sxa_over(sxa_sub(r, c), dx, pow2);
     const T du_dy = b >= (T)0 ? sxa_over(sxa_sub(c, d), dy, pow2) : sxa_over(sxa_sub(u, c), dy, pow2);
-    return sxa_sub(c, sxa_mul(dt, sxa_add(sxa_mul(a, du_dx), sxa_mul(b, du_dy))));
+    return sx_upwind_update(c, du_dx, du_dy, a, b, dt);
 }
 
 template <typename T>
@@ -201,7 +202,7 @@ __global__ void __launch_bounds__(256) sx_amr_tag_full_kernel(const T* __restric
         else if (y == H - 1) gy = __fsub_rn(c, (float)v[idx - W]);
         else gy = __fmul_rn(__fsub_rn((float)v[idx + W], (float)v[idx - W]), 0.5f);
     }
-    t[idx] = __fsqrt_rn(__fadd_rn(__fmul_rn(gx, gx), __fmul_rn(gy, gy))) >= thr ? 1 : 0;
+    t[idx] = sx_grad_norm(gx, gy) >= thr ? 1 : 0;
 }
 
 // mode 0: von Neumann (row or column within p), 1: Moore (box), 2: no grading

@@ -159,3 +159,30 @@ __device__ __forceinline__ int sx_block_exclusive_scan(int v, int* s_warp, int* 
     __syncthreads();
     return result;
 }
+
+// ---------------------------------------------------------------------------
+// The reference's float32 formulas with the contraction its NVRTC build
+// applies.  The reference compiles its kernels with NVRTC's default
+// --fmad=true, which fuses each multiply into the add that consumes it:
+//   upwind  c - dt * (a * du_dx + b * du_dy)  ->  fma(-dt, fma(a, du_dx, b * du_dy), c)
+//   |grad|  sqrtf(gx * gx + gy * gy)           ->  sqrt(fma(gx, gx, gy * gy))
+// (interval_stencil.py:105-111, regrid.py:196-217; established on a B200 by
+// running the reference's own kernels, compiled with its NVRTC options,
+// against every candidate grouping: only this one agrees on every cell).
+// Float64 has no reference counterpart and rounds every operation once.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float sx_upwind_update(float c, float du_dx, float du_dy, float a, float b, float dt)
+{
+    return __fmaf_rn(-dt, __fmaf_rn(a, du_dx, __fmul_rn(b, du_dy)), c);
+}
+
+__device__ __forceinline__ double sx_upwind_update(double c, double du_dx, double du_dy, double a, double b, double dt)
+{
+    return __dsub_rn(c, __dmul_rn(dt, __dadd_rn(__dmul_rn(a, du_dx), __dmul_rn(b, du_dy))));
+}
+
+__device__ __forceinline__ float sx_grad_norm(float gx, float gy)
+{
+    return __fsqrt_rn(__fmaf_rn(gx, gx, __fmul_rn(gy, gy)));
+}
+

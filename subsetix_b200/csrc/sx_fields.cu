@@ -4,11 +4,13 @@
 //
 // A field stores one value per active cell, row by row, with int32 cell
 // offsets per interval (subsetix_cupy/interval_field.py:19-89).  Every
-// float formula below follows the reference's source order.  It is written
-// with explicit round-to-nearest intrinsics, so the compiler cannot fuse a
-// multiply and an add.  Results are therefore reproducible bit for bit
-// against a host build without FMA contraction, and the same code serves
-// FP32 and FP64.
+// float formula below follows the reference's source order and is written
+// with explicit rounding intrinsics, so the compiler makes no choice of its
+// own.  Where the reference's NVRTC build fuses a multiply into an add (the
+// upwind update and the gradient norm in float32), the fusion is written
+// out as the same FMA (sx_upwind_update, sx_grad_norm in sx_common.cuh), so
+// float32 results equal the reference's on the GPU bit for bit; float64
+// rounds every operation once.
 
 #include <climits>
 #include <cmath>
@@ -441,7 +443,7 @@ __global__ void __launch_bounds__(256) sx_upwind_kernel(const int* __restrict__ 
         const T up = sx_sample<T>(row + 1, x, height, width, lookup, off, b, e, coff, v);
         const T du_dx = a >= (T)0 ? sx_div(sx_sub(center, left), dx) : sx_div(sx_sub(right, center), dx);
         const T du_dy = bb >= (T)0 ? sx_div(sx_sub(center, down), dy) : sx_div(sx_sub(up, center), dy);
-        out[c] = sx_sub(center, sx_mul(dt, sx_add(sx_mul(a, du_dx), sx_mul(bb, du_dy))));
+        out[c] = sx_upwind_update(center, du_dx, du_dy, a, bb, dt);
     }
 }
 
@@ -825,7 +827,7 @@ __global__ void __launch_bounds__(256) sx_upwind_chunk_kernel(const int* __restr
             if (act) {
                 const T du_dx = a >= (T)0 ? sx_over(sx_sub(center, left), dx, pow2) : sx_over(sx_sub(right, center), dx, pow2);
                 const T du_dy = bb >= (T)0 ? sx_over(sx_sub(center, down), dy, pow2) : sx_over(sx_sub(up, center), dy, pow2);
-                out[c] = sx_sub(center, sx_mul(dt, sx_add(sx_mul(a, du_dx), sx_mul(bb, du_dy))));
+                out[c] = sx_upwind_update(center, du_dx, du_dy, a, bb, dt);
             }
         }
     }
@@ -1006,7 +1008,7 @@ __device__ __forceinline__ bool sx_pred(const float* __restrict__ d, int x, int 
         else if (y == height - 1) gy = __fsub_rn(c, d[idx - width]);
         else gy = __fmul_rn(__fsub_rn(d[idx + width], d[idx - width]), 0.5f);
     }
-    return __fsqrt_rn(__fadd_rn(__fmul_rn(gx, gx), __fmul_rn(gy, gy))) >= thr;
+    return sx_grad_norm(gx, gy) >= thr;
 }
 
 template <bool GRAD>
@@ -1299,7 +1301,7 @@ __global__ void sx_gradient_kernel(const float* __restrict__ d, int width, int h
             else if (y == height - 1) gy = __fsub_rn(c, d[idx - width]);
             else gy = __fmul_rn(__fsub_rn(d[idx + width], d[idx - width]), 0.5f);
         }
-        out[idx] = __fsqrt_rn(__fadd_rn(__fmul_rn(gx, gx), __fmul_rn(gy, gy)));
+        out[idx] = sx_grad_norm(gx, gy);
     }
 }
 

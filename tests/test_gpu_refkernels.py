@@ -145,7 +145,7 @@ def test_gradient_and_tags_bit_exact_vs_reference_kernels(ref, case):
 @pytest.mark.parametrize("ratio", [2, 3, 4])
 def test_prolong_restrict_f32_bit_exact_vs_reference_kernels(ref, ratio):
     rng = np.random.default_rng(20 + ratio)
-    coarse_h = rand_set(60, 3.0, seed=40 + ratio, max_col=200, row0=0)
+    coarse_h = rand_set(60, 3.0, seed=40 + ratio, max_col=200, row0=0, min_per_row=1)
     coarse = O.ISet(*coarse_h)
     cvals = rng.uniform(-2, 2, int((coarse.end - coarse.begin).sum())).astype(np.float32)
     s, f = _field(coarse_h, cvals)

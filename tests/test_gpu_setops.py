@@ -10,7 +10,7 @@ import torch
 from oracle import oracle as O
 from subsetix_b200 import synth
 from tests.golden_io import get_set, load
-from tests.gpu_util import assert_same, dev_set, host, iset
+from tests.gpu_util import assert_same, dev_set, host, iset, rand_set
 
 pytestmark = pytest.mark.gpu
 
