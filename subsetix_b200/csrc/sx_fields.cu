@@ -779,11 +779,14 @@ __global__ void __launch_bounds__(256) sx_upwind_chunk_kernel(const int* __restr
             dt = __ldg(band_table + 4 * q + 2);
             pow2 = __ldg(band_table + 4 * q + 3) != (T)0;
         }
+        // sub-rounds that hold cells (the same for the whole warp): chunks of
+        // short intervals skip the empty ones instead of issuing them masked
+        const int nq = min(SX_CHUNK_SUB, (ie - x0 + 31) >> 5);
         T cen[SX_CHUNK_SUB];
 #pragma unroll
         for (int q = 0; q < SX_CHUNK_SUB; ++q) {
             const int x = x0 + 32 * q + lane;
-            cen[q] = x < ie ? v[c0 + 32 * q + lane] : (T)0;
+            cen[q] = (q < nq && x < ie) ? v[c0 + 32 * q + lane] : (T)0;
         }
         SxRowReader dn{p1.x, p1.y, p1.z, p1.w, p2.x};
         SxRowReader upc{p2.y, p2.z, p2.w, p3.x, p3.y};
@@ -792,9 +795,12 @@ __global__ void __launch_bounds__(256) sx_upwind_chunk_kernel(const int* __restr
         int idn[SX_CHUNK_SUB], iup[SX_CHUNK_SUB];
 #pragma unroll
         for (int q = 0; q < SX_CHUNK_SUB; ++q) {
-            const int x = x0 + 32 * q + lane;
-            idn[q] = sx_row_index(dn, x, width, b, e, coff, x < ie);
-            iup[q] = sx_row_index(upc, x, width, b, e, coff, x < ie);
+            idn[q] = iup[q] = -1;
+            if (q < nq) {
+                const int x = x0 + 32 * q + lane;
+                idn[q] = sx_row_index(dn, x, width, b, e, coff, x < ie);
+                iup[q] = sx_row_index(upc, x, width, b, e, coff, x < ie);
+            }
         }
         T vdn[SX_CHUNK_SUB], vup[SX_CHUNK_SUB];
 #pragma unroll
@@ -805,6 +811,7 @@ __global__ void __launch_bounds__(256) sx_upwind_chunk_kernel(const int* __restr
         T prev_last = (T)0;  // lane 31's centre of the previous sub-round
 #pragma unroll
         for (int q = 0; q < SX_CHUNK_SUB; ++q) {
+            if (q >= nq) break;
             const int x = x0 + 32 * q + lane;
             const bool act = x < ie;
             const long long c = c0 + 32 * q + lane;
@@ -985,11 +992,14 @@ __global__ void sx_row_lookup_kernel(const int* __restrict__ rows, int row_count
 // Gradient magnitude and threshold run-length encoding on a full
 // width x height grid (regrid.py:20-124,172-223).  The gradient uses
 // central differences inside and one-sided ones at the borders, with no
-// /dx, and is sqrt(gx*gx + gy*gy).  A run is a stretch of
-// value >= threshold.  One warp per row, 32 columns per step: a ballot
-// gives the mask, and the run starts and stops come from the mask and the
-// carry bit.  Each run end is written once (see DESIGN.md 5.2 for the
-// reference's double write).
+// /dx, and is sqrt(fma(gx, gx, gy*gy)) as the reference's GPU build
+// computes it.  A run is a stretch of value >= threshold.  One warp per
+// row, 32 columns per step: a ballot gives the mask, and the run starts and
+// stops come from the mask and the carry bit.  Each run end is written once;
+// when the width is not a multiple of 32 and a row's last cell is set, the
+// reference writes that row's final end a second time into the next row's
+// first slot (a race between its row blocks, regrid.py:66-124), which
+// equals this result when its blocks retire in order.
 // ---------------------------------------------------------------------------
 template <bool GRAD>
 __device__ __forceinline__ bool sx_pred(const float* __restrict__ d, int x, int y, int width, int height, float thr)
