@@ -116,9 +116,12 @@ typedef struct sx_tuning {
     int32_t withhold_tile;
 } sx_tuning;
 
-/* Workspace for sx_bool_eval: the size returned here lets every kernel use
- * its preferred tiles; sx_bool_eval accepts down to 8 bytes per 32 rows plus
- * a few KiB (the look-back state of 32-row tiles) and then uses 32-row tiles. */
+/* Workspace for sx_bool_eval: the size returned here (the look-back state of
+ * 1-row tiles) fits every tuning.  Without an explicit tile_rows,
+ * sx_bool_eval accepts down to 8 bytes per 32 rows plus a few KiB (the
+ * look-back state of 32-row tiles) and then uses 32-row tiles; with an
+ * explicit tile_rows a workspace too small for those tiles is refused
+ * (SX_ERR_WORKSPACE). */
 size_t sx_bool_workspace_bytes(int32_t rows);
 int sx_bool_eval(const sx_leaf* leaves /* host array of k */, int k, int32_t rows, const uint32_t* table /* host, 8 */,
                  int mode, int32_t* out_begin, int32_t* out_end, int32_t* out_offsets, int64_t capacity,

@@ -53,7 +53,7 @@ const char* sx_last_error(void) { return g_err; }
 size_t sx_bool_workspace_bytes(int32_t rows)
 {
     const long long r = rows < 1 ? 1 : rows;
-    return sx_sweep_state_bytes((r + 3) / 4);  // down to 4-row tiles of the segmented sweeps
+    return sx_sweep_state_bytes(r);  // the look-back state of 1-row tiles: every tuning fits
 }
 
 int sx_bool_eval(const sx_leaf* leaves, int k, int32_t rows, const uint32_t* table, int mode, int32_t* out_begin,
@@ -108,6 +108,14 @@ int sx_bool_eval(const sx_leaf* leaves, int k, int32_t rows, const uint32_t* tab
         A.tune_staging_cap = tuning->staging_cap;
         A.tune_warps = tuning->warps;
         A.tune_tile_rows = tuning->tile_rows;
+    }
+    if (mode == SX_MODE_TABLE && A.tune_tile_rows > 0 && (A.tune_kernel == 0 || A.tune_kernel >= 4)) {
+        // an explicit tile height is honoured exactly or refused, never changed behind the caller's back
+        const int tr = A.tune_kernel == 6 && A.tune_tile_rows > 8 ? 8 : A.tune_tile_rows;
+        const size_t need = sx_sweep_state_bytes(((long long)rows + tr - 1) / tr);
+        if (need > workspace_bytes)
+            return fail(SX_ERR_WORKSPACE, "sx_bool_eval: %d-row tiles need %zu bytes of workspace, got %zu", tr, need,
+                        workspace_bytes);
     }
     cudaError_t err = sx_sweep_launch(A, mode == SX_MODE_UNION, workspace, workspace_bytes, (cudaStream_t)stream);
     if (err != cudaSuccess) return cuda_fail(err, "sx_bool_eval");

@@ -31,10 +31,11 @@ def _one_leaf():
 
 
 @pytest.mark.parametrize("field,value", [("kernel", 7), ("kernel", -1), ("warps", 9), ("tile_rows", 33),
-                                         ("tile_rows", -2), ("staging_cap", -5), ("blocks_per_sm", -1)])
+                                         ("tile_rows", -2), ("staging_cap", -5), ("blocks_per_sm", -1),
+                                         ("wait_limit", -1), ("withhold_tile", -3)])
 def test_bool_eval_rejects_bad_tuning_on_the_host(field, value):
     lib = _lib_or_skip()
-    tun = _lib.SxTuning(0, 0, 0, 0, 0)
+    tun = _lib.SxTuning(0, 0, 0, 0, 0, 0, 0)
     setattr(tun, field, value)
     tab = (ctypes.c_uint32 * 8)(0b1110, 0, 0, 0, 0, 0, 0, 0)
     rows = 64
@@ -50,6 +51,20 @@ def test_bool_eval_rejects_a_short_workspace_on_the_host():
     tab = (ctypes.c_uint32 * 8)(0b1110, 0, 0, 0, 0, 0, 0, 0)
     rc = lib.sx_bool_eval(_one_leaf(), 1, 1 << 20, tab, _lib.MODE_TABLE, 16, 16, 16, 100, 16, 16, 64, None, None)
     assert rc == _lib.SX_ERR_WORKSPACE
+
+
+def test_explicit_tile_height_is_refused_when_its_state_does_not_fit():
+    """An explicit tile_rows is never silently replaced by 32-row tiles: a short workspace is an error."""
+    lib = _lib_or_skip()
+    tab = (ctypes.c_uint32 * 8)(0b1110, 0, 0, 0, 0, 0, 0, 0)
+    rows = 1 << 16
+    ws32 = lib.sx_bool_workspace_bytes(rows // 32)  # enough for 32-row tiles only
+    for kernel, tile_rows in ((5, 1), (6, 3), (4, 16)):
+        tun = _lib.SxTuning(kernel, 0, 0, 0, tile_rows, 0, 0)
+        rc = lib.sx_bool_eval(_one_leaf(), 1, rows, tab, _lib.MODE_TABLE, 16, 16, 16, 100, 16, 16, ws32,
+                              ctypes.byref(tun), None)
+        assert rc == _lib.SX_ERR_WORKSPACE, (kernel, tile_rows)
+        assert f"{tile_rows}-row tiles" in _lib.last_error()
 
 
 def test_workspace_for_small_tiles_covers_32_row_tiles():
