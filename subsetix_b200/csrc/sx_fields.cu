@@ -615,6 +615,11 @@ __global__ void __launch_bounds__(256) sx_sum_pairs_kernel(const double* __restr
 // chunk (fewer than 128: they are disjoint and non-empty).
 // ---------------------------------------------------------------------------
 #define SX_CHUNK 128
+// Blocks of 256 threads the chunked stencil asks to keep resident per SM
+// (a register cap for the compiler); a build-time tuning knob.
+#ifndef SX_UPWIND_MIN_BLOCKS
+#define SX_UPWIND_MIN_BLOCKS 1
+#endif
 #define SX_CHUNK_SUB (SX_CHUNK / 32)
 
 __global__ void sx_chunk_count_kernel(const int* __restrict__ b, const int* __restrict__ e, int n,
@@ -685,6 +690,68 @@ __device__ __forceinline__ int sx_row_index(SxRowReader& r, int x, int width, co
     return r.cc + (x - r.cb);
 }
 
+// Value indices of the neighbour-row cells under a chunk's active cells, for
+// all its sub-rounds at once (the whole warp calls it with the same plan
+// entry).  When the plan's first interval reaches past the chunk, no load is
+// needed.  Otherwise the warp loads the row's next 32 intervals with one
+// coalesced load per array and every lane finds the interval under each of
+// its columns by a binary search over the lanes' interval ends (shuffles):
+// one memory round trip per 32 intervals instead of one per interval
+// stepped over.  idx[q] = -1 where the cell has no neighbour in the set or
+// lies outside [0, width).
+template <int SUB>
+__device__ __forceinline__ void sx_row_indices(const SxRowReader& r0, int x0, int nq, int ie, int width,
+                                               const int* __restrict__ b, const int* __restrict__ e,
+                                               const int* __restrict__ coff, int lane, int (&idx)[SUB])
+{
+    bool done[SUB];
+#pragma unroll
+    for (int q = 0; q < SUB; ++q) {
+        idx[q] = -1;
+        done[q] = !(q < nq && x0 + 32 * q + lane < ie);
+    }
+    if (r0.j >= r0.je) return;
+    const int xlast = min(ie, x0 + 32 * nq) - 1;
+    if (r0.ce > xlast) {  // one interval reaches past the chunk
+#pragma unroll
+        for (int q = 0; q < SUB; ++q) {
+            const int x = x0 + 32 * q + lane;
+            if (!done[q] && x >= r0.cb && x >= 0 && x < width) idx[q] = r0.cc + (x - r0.cb);
+        }
+        return;
+    }
+    for (int k0 = r0.j; k0 < r0.je; k0 += 32) {
+        const int k = k0 + lane;
+        int bk = INT_MAX, ek = INT_MAX, ck = 0;
+        if (k < r0.je) {
+            bk = b[k];
+            ek = e[k];
+            ck = coff[k];
+        }
+#pragma unroll
+        for (int q = 0; q < SUB; ++q) {
+            if (q >= nq) break;
+            const int x = x0 + 32 * q + lane;
+            // first lane m whose interval ends after x (ends rise across the lanes)
+            int m = 0;
+#pragma unroll
+            for (int step = 16; step >= 1; step >>= 1) {
+                const int em = __shfl_sync(0xFFFFFFFFu, ek, m + step - 1);
+                if (em <= x) m += step;
+            }
+            const int em = __shfl_sync(0xFFFFFFFFu, ek, m);
+            const int bm = __shfl_sync(0xFFFFFFFFu, bk, m);
+            const int cm = __shfl_sync(0xFFFFFFFFu, ck, m);
+            if (!done[q] && em > x) {
+                done[q] = true;
+                if (bm <= x && x >= 0 && x < width) idx[q] = cm + (x - bm);
+            }
+        }
+        const int elast = __shfl_sync(0xFFFFFFFFu, ek, 31);
+        if (elast > xlast) break;  // every column is resolved (or the row has ended)
+    }
+}
+
 template <typename T>
 __device__ __forceinline__ T sx_row_take(SxRowReader& r, int x, int width, const int* __restrict__ b,
                                          const int* __restrict__ e, const int* __restrict__ coff,
@@ -752,7 +819,7 @@ __global__ void sx_chunk_info_kernel(const int* __restrict__ rows, const int* __
 // exact reciprocals), dt, and 1 when the reciprocals are given.  Chunks of a
 // row whose band index is outside [0, nbands) are left unwritten.
 template <typename T, bool BANDS>
-__global__ void __launch_bounds__(256) sx_upwind_chunk_kernel(const int* __restrict__ off,
+__global__ void __launch_bounds__(256, SX_UPWIND_MIN_BLOCKS) sx_upwind_chunk_kernel(const int* __restrict__ off,
                                                               const int* __restrict__ b, const int* __restrict__ e,
                                                               const int* __restrict__ coff,
                                                               const int* __restrict__ info, long long chunks,
@@ -788,20 +855,13 @@ __global__ void __launch_bounds__(256) sx_upwind_chunk_kernel(const int* __restr
             const int x = x0 + 32 * q + lane;
             cen[q] = (q < nq && x < ie) ? v[c0 + 32 * q + lane] : (T)0;
         }
-        SxRowReader dn{p1.x, p1.y, p1.z, p1.w, p2.x};
-        SxRowReader upc{p2.y, p2.z, p2.w, p3.x, p3.y};
+        const SxRowReader dn{p1.x, p1.y, p1.z, p1.w, p2.x};
+        const SxRowReader upc{p2.y, p2.z, p2.w, p3.x, p3.y};
         // neighbour-row value indices of all four sub-rounds first, then all
         // their loads at once, so the chunk waits for one round trip
         int idn[SX_CHUNK_SUB], iup[SX_CHUNK_SUB];
-#pragma unroll
-        for (int q = 0; q < SX_CHUNK_SUB; ++q) {
-            idn[q] = iup[q] = -1;
-            if (q < nq) {
-                const int x = x0 + 32 * q + lane;
-                idn[q] = sx_row_index(dn, x, width, b, e, coff, x < ie);
-                iup[q] = sx_row_index(upc, x, width, b, e, coff, x < ie);
-            }
-        }
+        sx_row_indices<SX_CHUNK_SUB>(dn, x0, nq, ie, width, b, e, coff, lane, idn);
+        sx_row_indices<SX_CHUNK_SUB>(upc, x0, nq, ie, width, b, e, coff, lane, iup);
         T vdn[SX_CHUNK_SUB], vup[SX_CHUNK_SUB];
 #pragma unroll
         for (int q = 0; q < SX_CHUNK_SUB; ++q) {
