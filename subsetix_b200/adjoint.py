@@ -226,6 +226,7 @@ class Hierarchy:
         self.inner_cells: List[int] = []
         self.ghost: List[Optional[tuple]] = []
         self.cover: List[Optional[tuple]] = []
+        self._segments: dict = {}
         for k, s in enumerate(sets):
             W, H = int(width) * r ** k, int(height) * r ** k
             if k == 0:
@@ -362,20 +363,81 @@ def _run_composite(h: Hierarchy, states: List[torch.Tensor], a: float, b: float,
     return cur, inputs
 
 
+class _Segment:
+    """``n`` coupled steps and their transposes as two CUDA graphs on fixed buffers.
+
+    The forward graph runs the steps from ``inp`` and keeps every step's
+    upwind inputs (``inputs``, the recomputation a backward pass needs); the
+    backward graph applies the steps' transposes, last step first, from
+    ``w_in`` to ``w_out`` and adds the velocity gradient into ``grad``.
+    Velocity and time step are baked into the graphs.  Every launch of a
+    segment becomes one graph replay instead of about seven launches per step
+    issued from Python.
+    """
+
+    def __init__(self, h: "Hierarchy", n: int, a: float, b: float, dt: float, dtype: torch.dtype):
+        dev = h.levels[0].device
+        self.inp = [torch.zeros(lvl.cells, dtype=dtype, device=dev) for lvl in h.levels]
+        self.w_in = [torch.zeros(lvl.cells, dtype=dtype, device=dev) for lvl in h.levels]
+        self.grad = torch.zeros(2, dtype=torch.float64, device=dev)
+        side = torch.cuda.Stream(device=dev)
+        side.wait_stream(torch.cuda.current_stream(dev))
+        self.fwd = torch.cuda.CUDAGraph()
+        self.bwd = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(side):
+            with torch.cuda.graph(self.fwd, stream=side):
+                cur, self.inputs = _run_composite(h, list(self.inp), a, b, dt, n, keep=True)
+                self.out = cur
+            with torch.cuda.graph(self.bwd, stream=side):
+                w = list(self.w_in)
+                for j in reversed(range(n)):
+                    w = h.step_adjoint(w, self.inputs[j], a, b, dt, self.grad)
+                self.w_out = w
+        torch.cuda.current_stream(dev).wait_stream(side)
+
+    def forward(self, states: Sequence[torch.Tensor]) -> List[torch.Tensor]:
+        for dst, src in zip(self.inp, states):
+            dst.copy_(src)
+        self.fwd.replay()
+        return self.out
+
+    def backward(self, w: Sequence[torch.Tensor]) -> List[torch.Tensor]:
+        for dst, src in zip(self.w_in, w):
+            dst.copy_(src)
+        self.bwd.replay()
+        return self.w_out
+
+
+def _segment(h: "Hierarchy", n: int, a: float, b: float, dt: float, dtype: torch.dtype) -> _Segment:
+    """Cached segment graphs of ``h`` (the two most recent parameter sets are kept)."""
+    key = (n, a, b, dt, dtype)
+    cache = h._segments
+    seg = cache.pop(key, None)
+    if seg is None:
+        while len(cache) >= 2:
+            cache.pop(next(iter(cache)))
+        seg = _Segment(h, n, a, b, dt, dtype)
+    cache[key] = seg
+    return seg
+
+
 class _AdvectComposite(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, velocity: torch.Tensor, h: Hierarchy, dt: float, steps: int, every: int, *u0):
+    def forward(ctx, velocity: torch.Tensor, h: Hierarchy, dt: float, steps: int, every: int, graphs: bool, *u0):
         a, b = (float(v) for v in velocity.detach().cpu().tolist())
         cur = h.extend([u.detach() for u in u0])
         checkpoints = [[x.clone() for x in cur]]
         done = 0
         while done < steps:
             n = min(every, steps - done)
-            cur, _ = _run_composite(h, cur, a, b, dt, n, keep=False)
+            if graphs:
+                cur = _segment(h, n, a, b, dt, cur[0].dtype).forward(cur)
+            else:
+                cur, _ = _run_composite(h, cur, a, b, dt, n, keep=False)
             done += n
             if done < steps:
                 checkpoints.append([x.clone() for x in cur])
-        ctx.h, ctx.dt, ctx.steps, ctx.every, ctx.ab = h, dt, steps, every, (a, b)
+        ctx.h, ctx.dt, ctx.steps, ctx.every, ctx.ab, ctx.graphs = h, dt, steps, every, (a, b), graphs
         ctx.checkpoints = checkpoints
         ctx.vel = (velocity.dtype, velocity.device)
         return tuple(h.interior(cur))
@@ -388,21 +450,36 @@ class _AdvectComposite(torch.autograd.Function):
         w = h.extend([g if g is not None else z for g, z in zip(grad_out, zeros)])
         grad_ab = torch.zeros(2, dtype=torch.float64, device=h.levels[0].device)
         starts = list(range(0, steps, every))
+        used = []
         for si in reversed(range(len(starts))):
             n = min(every, steps - starts[si])
-            _, inputs = _run_composite(h, [x.clone() for x in ctx.checkpoints[si]], a, b, dt, n, keep=True)
-            for j in reversed(range(n)):
-                w = h.step_adjoint(w, inputs[j], a, b, dt, grad_ab)
+            if ctx.graphs:
+                seg = _segment(h, n, a, b, dt, w[0].dtype)
+                if all(seg is not u for u in used):
+                    seg.grad.zero_()
+                    used.append(seg)
+                seg.forward(ctx.checkpoints[si])
+                w = [x.clone() for x in seg.backward(w)]
+            else:
+                _, inputs = _run_composite(h, [x.clone() for x in ctx.checkpoints[si]], a, b, dt, n, keep=True)
+                for j in reversed(range(n)):
+                    w = h.step_adjoint(w, inputs[j], a, b, dt, grad_ab)
+        for seg in used:
+            grad_ab += seg.grad
         ctx.checkpoints = None
         grads = h.interior(w)
-        return (grad_ab.to(device=ctx.vel[1], dtype=ctx.vel[0]), None, None, None, None, *grads)
+        return (grad_ab.to(device=ctx.vel[1], dtype=ctx.vel[0]), None, None, None, None, None, *grads)
 
 
 def advect_composite(velocity: torch.Tensor, hierarchy: Hierarchy, u0: Sequence[torch.Tensor], *, dt: float,
-                     steps: int, checkpoint_every: int = 10) -> Tuple[torch.Tensor, ...]:
+                     steps: int, checkpoint_every: int = 10, graphs: bool = True) -> Tuple[torch.Tensor, ...]:
     """``steps`` coupled steps of a :class:`Hierarchy`; differentiable in ``velocity`` (2 values) and ``u0``.
 
     ``u0[k]`` holds the cells of level ``k``'s set; so does each returned field.
+    With ``graphs`` every checkpoint segment runs as a CUDA-graph replay (the
+    graphs for a velocity and time step are captured on first use and kept for
+    the two most recent ones); without, the same launches are issued one by
+    one.  Results are the same either way.
     """
     if len(u0) != len(hierarchy.levels):
         raise ValueError("one initial field per level")
@@ -411,7 +488,8 @@ def advect_composite(velocity: torch.Tensor, hierarchy: Hierarchy, u0: Sequence[
             raise ValueError(f"level {k}: expected {n} values, got {int(u.numel())}")
     if steps < 0 or checkpoint_every < 1:
         raise ValueError("steps must be >= 0 and checkpoint_every >= 1")
-    return _AdvectComposite.apply(velocity, hierarchy, float(dt), int(steps), int(checkpoint_every), *u0)
+    return _AdvectComposite.apply(velocity, hierarchy, float(dt), int(steps), int(checkpoint_every), bool(graphs),
+                                  *u0)
 
 
 __all__ = ["Level", "advect", "Hierarchy", "advect_composite"]
