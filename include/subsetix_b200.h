@@ -358,17 +358,33 @@ int sx_upwind(int dtype, const int32_t* rows, const int32_t* row_ids, const int3
  *                        interval bounds, its row, whether its interval
  *                        touches its neighbours in the row, and where the
  *                        rows above and below start to overlap it (lookup
- *                        as for sx_upwind).
- * Each step is then sx_upwind_chunked (values != out). */
+ *                        as for sx_upwind);
+ *   sx_upwind_plan_table optional: neighbours[cells] (2-byte aligned), one
+ *                        16-bit word per cell giving where its neighbours
+ *                        in the rows below (low byte) and above (high byte)
+ *                        sit in `values` (offsets from the chunk's first
+ *                        neighbour cell), 0xFF for none; `cells` is
+ *                        cell_offsets[n].  With cell_offsets the prefix sum
+ *                        of the interval lengths every offset is below 128;
+ *                        with gaps between intervals one may not fit a byte,
+ *                        and then *status (device) becomes nonzero and the
+ *                        table must not be used.
+ * Each step is then sx_upwind_chunked (values != out), with the neighbour
+ * table or NULL (then the rows above and below are searched every step).
+ * The table is the same for every width; it depends on `height` through the
+ * plan. */
 int sx_upwind_plan(const int32_t* begin, const int32_t* end, int64_t n, int32_t* chunk_offsets, int32_t* result,
                    void* workspace, size_t workspace_bytes, void* stream);
 int sx_upwind_plan_fill(const int32_t* rows, const int32_t* row_offsets, int32_t row_count, const int32_t* begin,
                         const int32_t* end, const int32_t* cell_offsets, int64_t n, const int32_t* chunk_offsets,
                         int64_t chunks, const int32_t* lookup, int32_t height, int32_t* chunk_info, void* stream);
+int sx_upwind_plan_table(const int32_t* begin, const int32_t* end, const int32_t* cell_offsets,
+                         const int32_t* chunk_info, int64_t chunks, uint16_t* neighbours, int32_t* status,
+                         void* stream);
 int sx_upwind_chunked(int dtype, const int32_t* row_offsets, const int32_t* begin, const int32_t* end,
                       const int32_t* cell_offsets, const int32_t* chunk_info, int64_t chunks, const int32_t* lookup,
-                      const void* values, void* out, int32_t width, int32_t height, double a, double b, double dt,
-                      double dx, double dy, void* stream);
+                      const uint16_t* neighbours, const void* values, void* out, int32_t width, int32_t height,
+                      double a, double b, double dt, double dx, double dy, void* stream);
 /* Banded form for batches of independent sets laid on row bands (subsetix_b200/batch.py): every row
  * belongs to band row_band[row] (device, `height` entries) with its own spacing and time step, so
  * each set keeps the dx = 1/side and CFL time step of its own step_upwind_interval call
@@ -379,9 +395,9 @@ int sx_upwind_chunked(int dtype, const int32_t* row_offsets, const int32_t* begi
 int sx_upwind_band_table(int dtype, const double* spacing, int32_t nbands, void* table);
 int sx_upwind_chunked_bands(int dtype, const int32_t* row_offsets, const int32_t* begin, const int32_t* end,
                             const int32_t* cell_offsets, const int32_t* chunk_info, int64_t chunks,
-                            const int32_t* lookup, const void* values, void* out, int32_t width, int32_t height,
-                            double a, double b, const int32_t* row_band, const void* band_table, int32_t nbands,
-                            void* stream);
+                            const int32_t* lookup, const uint16_t* neighbours, const void* values, void* out,
+                            int32_t width, int32_t height, double a, double b, const int32_t* row_band,
+                            const void* band_table, int32_t nbands, void* stream);
 int sx_upwind_f32(const int32_t* rows, const int32_t* row_offsets, int32_t row_count, const int32_t* begin,
                   const int32_t* end, const int32_t* cell_offsets, int64_t n, int64_t cells, const int32_t* lookup,
                   const float* values, float* out, int32_t width, int32_t height, float a, float b, float dt, float dx,
@@ -406,14 +422,16 @@ int sx_upwind_adjoint(int dtype, const int32_t* rows, const int32_t* row_offsets
                       double* grad_velocity, void* scratch, size_t scratch_bytes, void* stream);
 
 /* sx_upwind_adjoint on a chunk plan (sx_upwind_plan / sx_upwind_plan_fill;
- * rows sorted and disjoint); same values.  scratch:
+ * rows sorted and disjoint); same values.  neighbours: the plan's neighbour
+ * table (sx_upwind_plan_table) or NULL.  scratch:
  * sx_upwind_adjoint_chunked_scratch_bytes(chunks) bytes. */
 size_t sx_upwind_adjoint_chunked_scratch_bytes(int64_t chunks);
 int sx_upwind_adjoint_chunked(int dtype, const int32_t* row_offsets, const int32_t* begin, const int32_t* end,
                               const int32_t* cell_offsets, const int32_t* chunk_info, int64_t chunks,
-                              const int32_t* lookup, const void* grad_out, const void* values, void* grad_in,
-                              int32_t width, int32_t height, double a, double b, double dt, double dx, double dy,
-                              double* grad_velocity, void* scratch, size_t scratch_bytes, void* stream);
+                              const int32_t* lookup, const uint16_t* neighbours, const void* grad_out,
+                              const void* values, void* grad_in, int32_t width, int32_t height, double a, double b,
+                              double dt, double dx, double dy, double* grad_velocity, void* scratch,
+                              size_t scratch_bytes, void* stream);
 
 /* Threshold run-length encoding of a full width x height float32 grid
  * (subsetix_amr2/regrid.py:20-124 K11/K12, and regrid.py:172-223 K14 when

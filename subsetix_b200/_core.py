@@ -438,12 +438,24 @@ def upwind_plan(rows, offsets, begin, end, cell_offs, lookup, height: int, devic
     return info, chunks
 
 
+def upwind_table(begin, end, cell_offs, chunk_info, chunks: int, cells: int, device):
+    """Neighbour table of a chunk plan (uint16 per cell; one synchronisation)."""
+    lib = _lib.load()
+    table = torch.empty(max(int(cells), 1), dtype=torch.int16, device=device)
+    status = empty_i32(1, device)
+    _lib.check(lib.sx_upwind_plan_table(ptr(begin), ptr(end), ptr(cell_offs), ptr(chunk_info), int(chunks), ptr(table),
+                                        ptr(status), stream_handle(device)), "sx_upwind_plan_table")
+    if int(status.item()):
+        raise _lib.SubsetixError("sx_upwind_plan_table: cell offsets are not the packed prefix sum")
+    return table
+
+
 def upwind_chunked(offsets, begin, end, cell_offs, chunk_info, chunks: int, lookup, values, out, width: int,
-                   height: int, a, b, dt, dx, dy, device):
+                   height: int, a, b, dt, dx, dy, device, table=None):
     lib = _lib.load()
     _lib.check(lib.sx_upwind_chunked(_dtype_code(values), ptr(offsets), ptr(begin), ptr(end), ptr(cell_offs),
-                                     ptr(chunk_info), int(chunks), ptr(lookup), ptr(values), ptr(out), int(width),
-                                     int(height), float(a), float(b), float(dt), float(dx), float(dy),
+                                     ptr(chunk_info), int(chunks), ptr(lookup), ptr(table), ptr(values), ptr(out),
+                                     int(width), int(height), float(a), float(b), float(dt), float(dx), float(dy),
                                      stream_handle(device)), "sx_upwind_chunked")
 
 

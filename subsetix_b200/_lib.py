@@ -103,8 +103,9 @@ _SIGNATURES = {
     "sx_upwind_plan": (ctypes.c_int, [c_vp, c_vp, ctypes.c_int64, c_vp, c_vp, c_vp, ctypes.c_size_t, c_vp]),
     "sx_upwind_plan_fill": (ctypes.c_int, [c_vp, c_vp, ctypes.c_int32, c_vp, c_vp, c_vp, ctypes.c_int64, c_vp,
                                            ctypes.c_int64, c_vp, ctypes.c_int32, c_vp, c_vp]),
+    "sx_upwind_plan_table": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, ctypes.c_int64, c_vp, c_vp, c_vp]),
     "sx_upwind_chunked": (ctypes.c_int, [ctypes.c_int, c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.c_int64, c_vp, c_vp, c_vp,
-                                         ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
+                                         c_vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
                                          ctypes.c_double, ctypes.c_double, ctypes.c_double, c_vp]),
     "sx_upwind_f32": (ctypes.c_int, [c_vp, c_vp, ctypes.c_int32, c_vp, c_vp, c_vp, ctypes.c_int64, ctypes.c_int64,
                                      c_vp, c_vp, c_vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_float, ctypes.c_float,
@@ -120,7 +121,7 @@ _SIGNATURES = {
                                          ctypes.c_double, ctypes.c_int, c_vp, c_vp, ctypes.c_size_t, c_vp]),
     "sx_upwind_adjoint_chunked_scratch_bytes": (ctypes.c_size_t, [ctypes.c_int64]),
     "sx_upwind_adjoint_chunked": (ctypes.c_int, [ctypes.c_int, c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.c_int64, c_vp,
-                                                 c_vp, c_vp, c_vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
+                                                 c_vp, c_vp, c_vp, c_vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
                                                  ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                                  c_vp, c_vp, ctypes.c_size_t, c_vp]),
     "sx_threshold_rle": (ctypes.c_int, [c_vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_float, ctypes.c_int, c_vp,
@@ -135,8 +136,8 @@ _SIGNATURES = {
     "sx_gather_i32": (ctypes.c_int, [c_vp, ctypes.c_int32, c_vp, c_vp, c_vp]),
     "sx_upwind_band_table": (ctypes.c_int, [ctypes.c_int, c_vp, ctypes.c_int32, c_vp]),
     "sx_upwind_chunked_bands": (ctypes.c_int, [ctypes.c_int, c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.c_int64, c_vp, c_vp,
-                                               c_vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
-                                               c_vp, c_vp, ctypes.c_int32, c_vp]),
+                                               c_vp, c_vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
+                                               ctypes.c_double, c_vp, c_vp, ctypes.c_int32, c_vp]),
     "sx_cell_quads": (ctypes.c_int, [ctypes.c_int, c_vp, c_vp, ctypes.c_int32, c_vp, c_vp, c_vp, ctypes.c_int32, c_vp,
                                      ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, c_vp, c_vp, c_vp]),
     "sx_index_copy": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, c_vp, c_vp, c_vp, c_vp, c_vp]),

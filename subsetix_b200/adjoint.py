@@ -62,6 +62,8 @@ class Level:
         self.direct = not (_core.check_rows(self.begin, self.end, self.off, device) & _ROWS_UNSAFE)
         self.chunk_off, self.chunks = (_core.upwind_plan(self.rows, self.off, self.begin, self.end, self.cell_off,
                                                          self.lookup, self.height, device) if self.direct else (None, 0))
+        self.table = (_core.upwind_table(self.begin, self.end, self.cell_off, self.chunk_off, self.chunks, self.cells,
+                                         device) if self.direct else None)
         self.device = device
         lib = _lib.load()
         nbytes = max(int(lib.sx_upwind_adjoint_scratch_bytes(self.cells)),
@@ -71,7 +73,8 @@ class Level:
     def step(self, u: torch.Tensor, out: torch.Tensor, a: float, b: float, dt: float) -> torch.Tensor:
         if self.chunk_off is not None:
             _core.upwind_chunked(self.off, self.begin, self.end, self.cell_off, self.chunk_off, self.chunks,
-                                 self.lookup, u, out, self.width, self.height, a, b, dt, self.dx, self.dy, self.device)
+                                 self.lookup, u, out, self.width, self.height, a, b, dt, self.dx, self.dy, self.device,
+                                 table=self.table)
         else:
             _core.upwind(self.rows, self.off, self.begin, self.end, self.cell_off, self.cells, self.lookup, u, out,
                          self.width, self.height, a, b, dt, self.dx, self.dy, self.direct, self.device)
@@ -87,7 +90,8 @@ class Level:
         if self.chunk_off is not None:
             _lib.check(lib.sx_upwind_adjoint_chunked(code, ptr(self.off), ptr(self.begin), ptr(self.end),
                                                      ptr(self.cell_off), ptr(self.chunk_off), self.chunks,
-                                                     ptr(self.lookup), ptr(w), ptr(u), ptr(ubar), self.width,
+                                                     ptr(self.lookup), ptr(self.table), ptr(w), ptr(u), ptr(ubar),
+                                                     self.width,
                                                      self.height, a, b, dt, self.dx, self.dy, ptr(g),
                                                      ptr(self.scratch), int(self.scratch.numel()),
                                                      stream_handle(self.device)), "sx_upwind_adjoint_chunked")
@@ -369,7 +373,8 @@ class _Segment:
     The forward graph runs the steps from ``inp`` and keeps every step's
     upwind inputs (``inputs``, the recomputation a backward pass needs); the
     backward graph applies the steps' transposes, last step first, from
-    ``w_in`` to ``w_out`` and adds the velocity gradient into ``grad``.
+    ``w_in`` to ``w_out`` and adds each step's velocity gradient onto
+    ``grad`` (which the caller loads with the running sum).
     Velocity and time step are baked into the graphs.  Every launch of a
     segment becomes one graph replay instead of about seven launches per step
     issued from Python.
@@ -450,22 +455,19 @@ class _AdvectComposite(torch.autograd.Function):
         w = h.extend([g if g is not None else z for g, z in zip(grad_out, zeros)])
         grad_ab = torch.zeros(2, dtype=torch.float64, device=h.levels[0].device)
         starts = list(range(0, steps, every))
-        used = []
         for si in reversed(range(len(starts))):
             n = min(every, steps - starts[si])
             if ctx.graphs:
+                # the graph adds every step's velocity gradient onto the running sum, in the eager order
                 seg = _segment(h, n, a, b, dt, w[0].dtype)
-                if all(seg is not u for u in used):
-                    seg.grad.zero_()
-                    used.append(seg)
+                seg.grad.copy_(grad_ab)
                 seg.forward(ctx.checkpoints[si])
                 w = [x.clone() for x in seg.backward(w)]
+                grad_ab.copy_(seg.grad)
             else:
                 _, inputs = _run_composite(h, [x.clone() for x in ctx.checkpoints[si]], a, b, dt, n, keep=True)
                 for j in reversed(range(n)):
                     w = h.step_adjoint(w, inputs[j], a, b, dt, grad_ab)
-        for seg in used:
-            grad_ab += seg.grad
         ctx.checkpoints = None
         grads = h.interior(w)
         return (grad_ab.to(device=ctx.vel[1], dtype=ctx.vel[0]), None, None, None, None, None, *grads)

@@ -51,6 +51,7 @@ class _StencilPlan:
     chunk_off: Optional[torch.Tensor]
     chunks: int
     row_band: torch.Tensor
+    table: Optional[torch.Tensor] = None
 
 
 @dataclass
@@ -129,10 +130,11 @@ class SetBatch:
                 raise ValueError("batch rows outside the band layout")
             direct = not (_core.check_rows(b, e, off, dev) & _ROWS_UNSAFE)
             chunk_off, chunks = (_core.upwind_plan(rows, off, b, e, cell_off, lookup, H, dev) if direct else (None, 0))
+            table = _core.upwind_table(b, e, cell_off, chunk_off, chunks, cells, dev) if direct else None
             band = torch.full((H,), -1, dtype=I32, device=dev)
             for i, (base, h) in enumerate(zip(self.bases, self.heights)):
                 band[base:base + h] = i
-            self._plan = _StencilPlan(cell_off, cells, lookup, H, chunk_off, chunks, band)
+            self._plan = _StencilPlan(cell_off, cells, lookup, H, chunk_off, chunks, band, table)
         return self._plan
 
     def band_table(self, dtype: torch.dtype, spacing: Sequence[Tuple[float, float, float]]) -> torch.Tensor:
@@ -203,7 +205,8 @@ def _upwind_bands(batch: SetBatch, plan: _StencilPlan, table: torch.Tensor, vals
     code = _lib.SX_F64 if vals.dtype == torch.float64 else _lib.SX_F32
     _lib.check(lib.sx_upwind_chunked_bands(code, ptr(_t(s.row_offsets)), ptr(_t(s.begin)), ptr(_t(s.end)),
                                            ptr(plan.cell_off), ptr(plan.chunk_off), int(plan.chunks),
-                                           ptr(plan.lookup), ptr(vals), ptr(out), int(width), int(plan.height),
+                                           ptr(plan.lookup), ptr(plan.table), ptr(vals), ptr(out), int(width),
+                                           int(plan.height),
                                            float(a), float(b), ptr(plan.row_band), ptr(table), len(batch.bases),
                                            stream_handle(vals.device)), "sx_upwind_chunked_bands")
 

@@ -519,10 +519,26 @@ int sx_upwind_plan_fill(const int32_t* rows, const int32_t* row_offsets, int32_t
     return SX_OK;
 }
 
+int sx_upwind_plan_table(const int32_t* begin, const int32_t* end, const int32_t* cell_offsets,
+                         const int32_t* chunk_info, int64_t chunks, uint16_t* neighbours, int32_t* status,
+                         void* stream)
+{
+    if (chunks < 0) return fail(SX_ERR_INVALID, "sx_upwind_plan_table: bad size");
+    if (!status) return fail(SX_ERR_INVALID, "sx_upwind_plan_table: null status");
+    if (chunks > 0 && (!begin || !end || !cell_offsets || !chunk_info || !neighbours))
+        return fail(SX_ERR_INVALID, "sx_upwind_plan_table: null argument");
+    if (((uintptr_t)chunk_info & 15u) != 0 || ((uintptr_t)neighbours & 1u) != 0)
+        return fail(SX_ERR_INVALID, "sx_upwind_plan_table: chunk_info must be 16-byte and neighbours 2-byte aligned");
+    cudaError_t err = sx_upwind_table_launch(begin, end, cell_offsets, chunk_info, chunks, neighbours, status,
+                                             (cudaStream_t)stream);
+    if (err != cudaSuccess) return cuda_fail(err, "sx_upwind_plan_table");
+    return SX_OK;
+}
+
 int sx_upwind_chunked(int dtype, const int32_t* row_offsets, const int32_t* begin, const int32_t* end,
                       const int32_t* cell_offsets, const int32_t* chunk_info, int64_t chunks, const int32_t* lookup,
-                      const void* values, void* out, int32_t width, int32_t height, double a, double b, double dt,
-                      double dx, double dy, void* stream)
+                      const uint16_t* neighbours, const void* values, void* out, int32_t width, int32_t height,
+                      double a, double b, double dt, double dx, double dy, void* stream)
 {
     if (dtype != SX_F32 && dtype != SX_F64) return fail(SX_ERR_INVALID, "sx_upwind_chunked: dtype %d", dtype);
     if (width <= 0 || height <= 0) return fail(SX_ERR_INVALID, "sx_upwind_chunked: width and height must be positive");
@@ -532,8 +548,10 @@ int sx_upwind_chunked(int dtype, const int32_t* row_offsets, const int32_t* begi
         return fail(SX_ERR_INVALID, "sx_upwind_chunked: null argument");
     if (((uintptr_t)chunk_info & 15u) != 0) return fail(SX_ERR_INVALID, "sx_upwind_chunked: chunk_info must be 16-byte aligned");
     if (values == out) return fail(SX_ERR_INVALID, "sx_upwind_chunked: out must not alias values");
-    cudaError_t err = sx_upwind_chunk_launch(row_offsets, begin, end, cell_offsets, chunk_info, chunks, lookup, values,
-                                             out, width, height, a, b, dt, dx, dy, dtype == SX_F64, (cudaStream_t)stream);
+    if (((uintptr_t)neighbours & 1u) != 0) return fail(SX_ERR_INVALID, "sx_upwind_chunked: neighbours must be 2-byte aligned");
+    cudaError_t err = sx_upwind_chunk_launch(row_offsets, begin, end, cell_offsets, chunk_info, chunks, lookup,
+                                             neighbours, values, out, width, height, a, b, dt, dx, dy,
+                                             dtype == SX_F64, (cudaStream_t)stream);
     if (err != cudaSuccess) return cuda_fail(err, "sx_upwind_chunked");
     return SX_OK;
 }
@@ -553,9 +571,9 @@ int sx_upwind_band_table(int dtype, const double* spacing, int32_t nbands, void*
 
 int sx_upwind_chunked_bands(int dtype, const int32_t* row_offsets, const int32_t* begin, const int32_t* end,
                             const int32_t* cell_offsets, const int32_t* chunk_info, int64_t chunks,
-                            const int32_t* lookup, const void* values, void* out, int32_t width, int32_t height,
-                            double a, double b, const int32_t* row_band, const void* band_table, int32_t nbands,
-                            void* stream)
+                            const int32_t* lookup, const uint16_t* neighbours, const void* values, void* out,
+                            int32_t width, int32_t height, double a, double b, const int32_t* row_band,
+                            const void* band_table, int32_t nbands, void* stream)
 {
     if (dtype != SX_F32 && dtype != SX_F64) return fail(SX_ERR_INVALID, "sx_upwind_chunked_bands: dtype %d", dtype);
     if (width <= 0 || height <= 0)
@@ -568,9 +586,11 @@ int sx_upwind_chunked_bands(int dtype, const int32_t* row_offsets, const int32_t
     if (((uintptr_t)chunk_info & 15u) != 0)
         return fail(SX_ERR_INVALID, "sx_upwind_chunked_bands: chunk_info must be 16-byte aligned");
     if (values == out) return fail(SX_ERR_INVALID, "sx_upwind_chunked_bands: out must not alias values");
+    if (((uintptr_t)neighbours & 1u) != 0)
+        return fail(SX_ERR_INVALID, "sx_upwind_chunked_bands: neighbours must be 2-byte aligned");
     cudaError_t err = sx_upwind_chunk_bands_launch(row_offsets, begin, end, cell_offsets, chunk_info, chunks, lookup,
-                                                   values, out, width, height, a, b, row_band, band_table, nbands,
-                                                   dtype == SX_F64, (cudaStream_t)stream);
+                                                   neighbours, values, out, width, height, a, b, row_band, band_table,
+                                                   nbands, dtype == SX_F64, (cudaStream_t)stream);
     if (err != cudaSuccess) return cuda_fail(err, "sx_upwind_chunked_bands");
     return SX_OK;
 }
@@ -632,9 +652,10 @@ size_t sx_upwind_adjoint_chunked_scratch_bytes(int64_t chunks)
 
 int sx_upwind_adjoint_chunked(int dtype, const int32_t* row_offsets, const int32_t* begin, const int32_t* end,
                               const int32_t* cell_offsets, const int32_t* chunk_info, int64_t chunks,
-                              const int32_t* lookup, const void* grad_out, const void* values, void* grad_in,
-                              int32_t width, int32_t height, double a, double b, double dt, double dx, double dy,
-                              double* grad_velocity, void* scratch, size_t scratch_bytes, void* stream)
+                              const int32_t* lookup, const uint16_t* neighbours, const void* grad_out,
+                              const void* values, void* grad_in, int32_t width, int32_t height, double a, double b,
+                              double dt, double dx, double dy, double* grad_velocity, void* scratch,
+                              size_t scratch_bytes, void* stream)
 {
     if (dtype != SX_F32 && dtype != SX_F64) return fail(SX_ERR_INVALID, "sx_upwind_adjoint_chunked: dtype %d", dtype);
     if (width <= 0 || height <= 0) return fail(SX_ERR_INVALID, "sx_upwind_adjoint_chunked: width and height must be positive");
@@ -651,8 +672,11 @@ int sx_upwind_adjoint_chunked(int dtype, const int32_t* row_offsets, const int32
     if (!scratch || scratch_bytes < sx_upwind_adjoint_chunked_scratch_bytes(chunks))
         return fail(SX_ERR_WORKSPACE, "sx_upwind_adjoint_chunked: scratch needs %zu bytes",
                     sx_upwind_adjoint_chunked_scratch_bytes(chunks));
+    if (((uintptr_t)neighbours & 1u) != 0)
+        return fail(SX_ERR_INVALID, "sx_upwind_adjoint_chunked: neighbours must be 2-byte aligned");
     cudaError_t err = sx_upwind_adjoint_chunk_launch(row_offsets, begin, end, cell_offsets, chunk_info, chunks, lookup,
-                                                     grad_out, values, grad_in, width, height, a, b, dt, dx, dy,
+                                                     neighbours, grad_out, values, grad_in, width, height, a, b, dt,
+                                                     dx, dy,
                                                      dtype == SX_F64, (double*)scratch, grad_velocity,
                                                      (cudaStream_t)stream);
     if (err != cudaSuccess) return cuda_fail(err, "sx_upwind_adjoint_chunked");

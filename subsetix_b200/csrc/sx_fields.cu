@@ -620,6 +620,13 @@ __global__ void __launch_bounds__(256) sx_sum_pairs_kernel(const double* __restr
 #ifndef SX_UPWIND_MIN_BLOCKS
 #define SX_UPWIND_MIN_BLOCKS 1
 #endif
+// The same for the table-driven form, which holds fewer values per lane: six
+// blocks (48 warps per SM, 40 registers) hide the two dependent loads of a
+// chunk best (config-4 batch on a B200: 1.79 ms at 1 block, 1.42 ms at 6,
+// 1.45 ms at 8).
+#ifndef SX_UPWIND_TABLE_MIN_BLOCKS
+#define SX_UPWIND_TABLE_MIN_BLOCKS 6
+#endif
 #define SX_CHUNK_SUB (SX_CHUNK / 32)
 
 __global__ void sx_chunk_count_kernel(const int* __restrict__ b, const int* __restrict__ e, int n,
@@ -698,8 +705,8 @@ __device__ __forceinline__ int sx_row_index(SxRowReader& r, int x, int width, co
 // its columns by a binary search over the lanes' interval ends (shuffles):
 // one memory round trip per 32 intervals instead of one per interval
 // stepped over.  idx[q] = -1 where the cell has no neighbour in the set or
-// lies outside [0, width).
-template <int SUB>
+// lies outside [0, width) (the column test only with XDOM).
+template <int SUB, bool XDOM = true>
 __device__ __forceinline__ void sx_row_indices(const SxRowReader& r0, int x0, int nq, int ie, int width,
                                                const int* __restrict__ b, const int* __restrict__ e,
                                                const int* __restrict__ coff, int lane, int (&idx)[SUB])
@@ -716,7 +723,7 @@ __device__ __forceinline__ void sx_row_indices(const SxRowReader& r0, int x0, in
 #pragma unroll
         for (int q = 0; q < SUB; ++q) {
             const int x = x0 + 32 * q + lane;
-            if (!done[q] && x >= r0.cb && x >= 0 && x < width) idx[q] = r0.cc + (x - r0.cb);
+            if (!done[q] && x >= r0.cb && (!XDOM || (x >= 0 && x < width))) idx[q] = r0.cc + (x - r0.cb);
         }
         return;
     }
@@ -744,7 +751,7 @@ __device__ __forceinline__ void sx_row_indices(const SxRowReader& r0, int x0, in
             const int cm = __shfl_sync(0xFFFFFFFFu, ck, m);
             if (!done[q] && em > x) {
                 done[q] = true;
-                if (bm <= x && x >= 0 && x < width) idx[q] = cm + (x - bm);
+                if (bm <= x && (!XDOM || (x >= 0 && x < width))) idx[q] = cm + (x - bm);
             }
         }
         const int elast = __shfl_sync(0xFFFFFFFFu, ek, 31);
@@ -814,20 +821,73 @@ __global__ void sx_chunk_info_kernel(const int* __restrict__ rows, const int* __
     }
 }
 
+// Neighbour table of a chunk plan, one 16-bit word per cell: the low byte
+// is the offset of the cell below from the chunk's base in that row, the
+// high byte the same for the row above, 0xFF where the neighbour is not in
+// the set (the column test against the domain stays with the step).  The
+// base of a neighbour row is the value index of its first cell at or right
+// of the chunk's first column; with values packed in interval order the
+// row's cells under the chunk are consecutive from there, so an offset is
+// below 128.  An offset that does not fit (values not packed) sets *status.
+__device__ __forceinline__ int sx_chunk_base(const SxRowReader& r, int x0)
+{
+    return r.j < r.je ? r.cc + max(0, x0 - r.cb) : 0;
+}
+
+__global__ void __launch_bounds__(256) sx_chunk_table_kernel(const int* __restrict__ b, const int* __restrict__ e,
+                                                             const int* __restrict__ coff,
+                                                             const int* __restrict__ info, long long chunks,
+                                                             unsigned short* __restrict__ nbr, int* __restrict__ status)
+{
+    const int lane = threadIdx.x & 31;
+    const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+    bool bad = false;
+    for (long long u = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); u < chunks; u += warps) {
+        const int4* pl = (const int4*)(info + (long long)SX_PLAN_INTS * u);
+        const int4 p0 = __ldg(pl), p1 = __ldg(pl + 1), p2 = __ldg(pl + 2), p3 = __ldg(pl + 3);
+        const int x0 = p0.x, ie = p0.y;
+        const long long c0 = p0.z;
+        const int nq = min(SX_CHUNK_SUB, (ie - x0 + 31) >> 5);
+        const SxRowReader dn{p1.x, p1.y, p1.z, p1.w, p2.x};
+        const SxRowReader upc{p2.y, p2.z, p2.w, p3.x, p3.y};
+        int idn[SX_CHUNK_SUB], iup[SX_CHUNK_SUB];
+        sx_row_indices<SX_CHUNK_SUB, false>(dn, x0, nq, ie, 0, b, e, coff, lane, idn);
+        sx_row_indices<SX_CHUNK_SUB, false>(upc, x0, nq, ie, 0, b, e, coff, lane, iup);
+        const int bdn = sx_chunk_base(dn, x0), bup = sx_chunk_base(upc, x0);
+#pragma unroll
+        for (int q = 0; q < SX_CHUNK_SUB; ++q) {
+            if (q >= nq) break;
+            if (x0 + 32 * q + lane >= ie) continue;
+            unsigned lo = 0xFFu, hi = 0xFFu;
+            if (idn[q] >= 0) {
+                const int d = idn[q] - bdn;
+                if (d >= 0 && d < 0xFF) lo = (unsigned)d; else bad = true;
+            }
+            if (iup[q] >= 0) {
+                const int d = iup[q] - bup;
+                if (d >= 0 && d < 0xFF) hi = (unsigned)d; else bad = true;
+            }
+            nbr[c0 + 32 * q + lane] = (unsigned short)(lo | (hi << 8));
+        }
+    }
+    if (bad) atomicOr(status, 1);
+}
+
 // With BANDS, every row belongs to a band (row_band[row]) with its own
 // spacing and time step: band_table[4 q .. 4 q + 3] = dx, dy (or their
 // exact reciprocals), dt, and 1 when the reciprocals are given.  Chunks of a
-// row whose band index is outside [0, nbands) are left unwritten.
-template <typename T, bool BANDS>
-__global__ void __launch_bounds__(256, SX_UPWIND_MIN_BLOCKS) sx_upwind_chunk_kernel(const int* __restrict__ off,
-                                                              const int* __restrict__ b, const int* __restrict__ e,
-                                                              const int* __restrict__ coff,
-                                                              const int* __restrict__ info, long long chunks,
-                                                              const int* __restrict__ lookup,
-                                                              const T* __restrict__ v, T* __restrict__ out, int width,
-                                                              int height, T a, T bb, T dt_all, T dx_all, T dy_all,
-                                                              int pow2_all, const int* __restrict__ row_band,
-                                                              const T* __restrict__ band_table, int nbands)
+// row whose band index is outside [0, nbands) are left unwritten.  With
+// TABLE the neighbour-row indices come from the plan's neighbour table
+// (sx_chunk_table_kernel) instead of a search: one coalesced 16-bit load per
+// cell, issued together with the cell's own value.
+template <typename T, bool BANDS, bool TABLE>
+__global__ void __launch_bounds__(256, TABLE ? SX_UPWIND_TABLE_MIN_BLOCKS : SX_UPWIND_MIN_BLOCKS)
+    sx_upwind_chunk_kernel(const int* __restrict__ off, const int* __restrict__ b, const int* __restrict__ e,
+                           const int* __restrict__ coff, const int* __restrict__ info, long long chunks,
+                           const int* __restrict__ lookup, const T* __restrict__ v, T* __restrict__ out, int width,
+                           int height, T a, T bb, T dt_all, T dx_all, T dy_all, int pow2_all,
+                           const int* __restrict__ row_band, const T* __restrict__ band_table, int nbands,
+                           const unsigned short* __restrict__ nbr)
 {
     const int lane = threadIdx.x & 31;
     const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
@@ -850,18 +910,38 @@ __global__ void __launch_bounds__(256, SX_UPWIND_MIN_BLOCKS) sx_upwind_chunk_ker
         // short intervals skip the empty ones instead of issuing them masked
         const int nq = min(SX_CHUNK_SUB, (ie - x0 + 31) >> 5);
         T cen[SX_CHUNK_SUB];
-#pragma unroll
-        for (int q = 0; q < SX_CHUNK_SUB; ++q) {
-            const int x = x0 + 32 * q + lane;
-            cen[q] = (q < nq && x < ie) ? v[c0 + 32 * q + lane] : (T)0;
-        }
+        int idn[SX_CHUNK_SUB], iup[SX_CHUNK_SUB];
         const SxRowReader dn{p1.x, p1.y, p1.z, p1.w, p2.x};
         const SxRowReader upc{p2.y, p2.z, p2.w, p3.x, p3.y};
-        // neighbour-row value indices of all four sub-rounds first, then all
-        // their loads at once, so the chunk waits for one round trip
-        int idn[SX_CHUNK_SUB], iup[SX_CHUNK_SUB];
-        sx_row_indices<SX_CHUNK_SUB>(dn, x0, nq, ie, width, b, e, coff, lane, idn);
-        sx_row_indices<SX_CHUNK_SUB>(upc, x0, nq, ie, width, b, e, coff, lane, iup);
+        if (TABLE) {
+            const int bdn = sx_chunk_base(dn, x0), bup = sx_chunk_base(upc, x0);
+            unsigned nb[SX_CHUNK_SUB];
+#pragma unroll
+            for (int q = 0; q < SX_CHUNK_SUB; ++q) {
+                const int x = x0 + 32 * q + lane;
+                const bool act = q < nq && x < ie;
+                cen[q] = act ? v[c0 + 32 * q + lane] : (T)0;
+                nb[q] = act ? (unsigned)__ldg(nbr + c0 + 32 * q + lane) : 0xFFFFu;
+            }
+#pragma unroll
+            for (int q = 0; q < SX_CHUNK_SUB; ++q) {
+                const int x = x0 + 32 * q + lane;
+                const bool xin = x >= 0 && x < width;
+                const unsigned lo = nb[q] & 0xFFu, hi = nb[q] >> 8;
+                idn[q] = (xin && lo != 0xFFu) ? bdn + (int)lo : -1;
+                iup[q] = (xin && hi != 0xFFu) ? bup + (int)hi : -1;
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < SX_CHUNK_SUB; ++q) {
+                const int x = x0 + 32 * q + lane;
+                cen[q] = (q < nq && x < ie) ? v[c0 + 32 * q + lane] : (T)0;
+            }
+            // neighbour-row value indices of all four sub-rounds first, then all
+            // their loads at once, so the chunk waits for one round trip
+            sx_row_indices<SX_CHUNK_SUB>(dn, x0, nq, ie, width, b, e, coff, lane, idn);
+            sx_row_indices<SX_CHUNK_SUB>(upc, x0, nq, ie, width, b, e, coff, lane, iup);
+        }
         T vdn[SX_CHUNK_SUB], vup[SX_CHUNK_SUB];
 #pragma unroll
         for (int q = 0; q < SX_CHUNK_SUB; ++q) {
@@ -904,13 +984,14 @@ __global__ void __launch_bounds__(256, SX_UPWIND_MIN_BLOCKS) sx_upwind_chunk_ker
 // same values as sx_upwind_adjoint_kernel.  One row reader per direction
 // serves both arrays (w and u share the geometry).  Per-block float64
 // partial sums of dL/da, dL/db go to partial[2 * block].
-template <typename T>
+template <typename T, bool TABLE>
 __global__ void __launch_bounds__(256) sx_upwind_adjoint_chunk_kernel(const int* __restrict__ off,
                                                                       const int* __restrict__ b,
                                                                       const int* __restrict__ e,
                                                                       const int* __restrict__ coff,
                                                                       const int* __restrict__ info, long long chunks,
                                                                       const int* __restrict__ lookup,
+                                                                      const unsigned short* __restrict__ nbr,
                                                                       const T* __restrict__ w, const T* __restrict__ u,
                                                                       T* __restrict__ ubar, int width, int height, T a,
                                                                       T bb, T dt, T dx, T dy, int pow2,
@@ -939,11 +1020,23 @@ __global__ void __launch_bounds__(256) sx_upwind_adjoint_chunk_kernel(const int*
         // the index), w reads need this cell's domain as well (jdom).
         const bool rdom = row >= 0 && row < height;
         int idn[SX_CHUNK_SUB], iup[SX_CHUNK_SUB];
+        if (TABLE) {  // the plan's neighbour table, as in the forward step
+            const int bdn = sx_chunk_base(dn, x0), bup = sx_chunk_base(upr, x0);
 #pragma unroll
-        for (int q = 0; q < SX_CHUNK_SUB; ++q) {
-            const int x = x0 + 32 * q + lane;
-            idn[q] = sx_row_index(dn, x, width, b, e, coff, x < ie);
-            iup[q] = sx_row_index(upr, x, width, b, e, coff, x < ie);
+            for (int q = 0; q < SX_CHUNK_SUB; ++q) {
+                const int x = x0 + 32 * q + lane;
+                const unsigned nb = x < ie ? (unsigned)__ldg(nbr + c0 + 32 * q + lane) : 0xFFFFu;
+                const bool xin = x >= 0 && x < width;
+                idn[q] = (xin && (nb & 0xFFu) != 0xFFu) ? bdn + (int)(nb & 0xFFu) : -1;
+                iup[q] = (xin && (nb >> 8) != 0xFFu) ? bup + (int)(nb >> 8) : -1;
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < SX_CHUNK_SUB; ++q) {
+                const int x = x0 + 32 * q + lane;
+                idn[q] = sx_row_index(dn, x, width, b, e, coff, x < ie);
+                iup[q] = sx_row_index(upr, x, width, b, e, coff, x < ie);
+            }
         }
         T wdn[SX_CHUNK_SUB], wup[SX_CHUNK_SUB], udn[SX_CHUNK_SUB], uup[SX_CHUNK_SUB];
 #pragma unroll
@@ -1576,45 +1669,77 @@ cudaError_t sx_upwind_plan_fill_launch(const int* rows, const int* off, int row_
     return cudaGetLastError();
 }
 
-cudaError_t sx_upwind_chunk_launch(const int* off, const int* b, const int* e, const int* coff, const int* info,
-                                   long long chunks, const int* lookup, const void* v, void* out, int width, int height,
-                                   double a, double bb, double dt, double dx, double dy, int dbl, cudaStream_t stream)
+cudaError_t sx_upwind_table_launch(const int* b, const int* e, const int* coff, const int* info, long long chunks,
+                                   unsigned short* nbr, int* status, cudaStream_t stream)
 {
-    if (chunks <= 0) return cudaSuccess;
+    cudaError_t err = cudaMemsetAsync(status, 0, sizeof(int), stream);
+    if (err != cudaSuccess || chunks <= 0) return err;
     long long blocks = (chunks + 7) / 8;
     if (blocks > 148 * 64) blocks = 148 * 64;
+    sx_chunk_table_kernel<<<(int)blocks, 256, 0, stream>>>(b, e, coff, info, chunks, nbr, status);
+    return cudaGetLastError();
+}
+
+template <typename T, bool BANDS>
+static void sx_upwind_chunk_go(int blocks, const int* off, const int* b, const int* e, const int* coff,
+                               const int* info, long long chunks, const int* lookup, const T* v, T* out, int width,
+                               int height, T a, T bb, T dt, T dx, T dy, int p, const int* row_band, const T* band_table,
+                               int nbands, const unsigned short* nbr, cudaStream_t stream)
+{
+    if (nbr)
+        sx_upwind_chunk_kernel<T, BANDS, true><<<blocks, 256, 0, stream>>>(off, b, e, coff, info, chunks, lookup, v,
+                                                                          out, width, height, a, bb, dt, dx, dy, p,
+                                                                          row_band, band_table, nbands, nbr);
+    else
+        sx_upwind_chunk_kernel<T, BANDS, false><<<blocks, 256, 0, stream>>>(off, b, e, coff, info, chunks, lookup, v,
+                                                                           out, width, height, a, bb, dt, dx, dy, p,
+                                                                           row_band, band_table, nbands, nullptr);
+}
+
+static int sx_chunk_blocks(long long chunks)
+{
+    long long blocks = (chunks + 7) / 8;
+    return (int)(blocks > 148 * 64 ? 148 * 64 : blocks);
+}
+
+cudaError_t sx_upwind_chunk_launch(const int* off, const int* b, const int* e, const int* coff, const int* info,
+                                   long long chunks, const int* lookup, const unsigned short* nbr, const void* v,
+                                   void* out, int width, int height, double a, double bb, double dt, double dx,
+                                   double dy, int dbl, cudaStream_t stream)
+{
+    if (chunks <= 0) return cudaSuccess;
+    const int blocks = sx_chunk_blocks(chunks);
     if (dbl) {
         double ddx = dx, ddy = dy;
         const int p = sx_pow2_pair(ddx, ddy);
-        sx_upwind_chunk_kernel<double, false><<<(int)blocks, 256, 0, stream>>>(
-            off, b, e, coff, info, chunks, lookup, (const double*)v, (double*)out, width, height, a, bb, dt, ddx, ddy,
-            p, nullptr, nullptr, 0);
+        sx_upwind_chunk_go<double, false>(blocks, off, b, e, coff, info, chunks, lookup, (const double*)v,
+                                          (double*)out, width, height, a, bb, dt, ddx, ddy, p, nullptr, nullptr, 0, nbr,
+                                          stream);
     } else {
         float fdx = (float)dx, fdy = (float)dy;
         const int p = sx_pow2_pair(fdx, fdy);
-        sx_upwind_chunk_kernel<float, false><<<(int)blocks, 256, 0, stream>>>(
-            off, b, e, coff, info, chunks, lookup, (const float*)v, (float*)out, width, height, (float)a, (float)bb,
-            (float)dt, fdx, fdy, p, nullptr, nullptr, 0);
+        sx_upwind_chunk_go<float, false>(blocks, off, b, e, coff, info, chunks, lookup, (const float*)v, (float*)out,
+                                         width, height, (float)a, (float)bb, (float)dt, fdx, fdy, p, nullptr, nullptr,
+                                         0, nbr, stream);
     }
     return cudaGetLastError();
 }
 
 cudaError_t sx_upwind_chunk_bands_launch(const int* off, const int* b, const int* e, const int* coff, const int* info,
-                                         long long chunks, const int* lookup, const void* v, void* out, int width,
-                                         int height, double a, double bb, const int* row_band, const void* band_table,
-                                         int nbands, int dbl, cudaStream_t stream)
+                                         long long chunks, const int* lookup, const unsigned short* nbr, const void* v,
+                                         void* out, int width, int height, double a, double bb, const int* row_band,
+                                         const void* band_table, int nbands, int dbl, cudaStream_t stream)
 {
     if (chunks <= 0) return cudaSuccess;
-    long long blocks = (chunks + 7) / 8;
-    if (blocks > 148 * 64) blocks = 148 * 64;
+    const int blocks = sx_chunk_blocks(chunks);
     if (dbl)
-        sx_upwind_chunk_kernel<double, true><<<(int)blocks, 256, 0, stream>>>(
-            off, b, e, coff, info, chunks, lookup, (const double*)v, (double*)out, width, height, a, bb, 0.0, 1.0, 1.0,
-            0, row_band, (const double*)band_table, nbands);
+        sx_upwind_chunk_go<double, true>(blocks, off, b, e, coff, info, chunks, lookup, (const double*)v, (double*)out,
+                                         width, height, a, bb, 0.0, 1.0, 1.0, 0, row_band, (const double*)band_table,
+                                         nbands, nbr, stream);
     else
-        sx_upwind_chunk_kernel<float, true><<<(int)blocks, 256, 0, stream>>>(
-            off, b, e, coff, info, chunks, lookup, (const float*)v, (float*)out, width, height, (float)a, (float)bb,
-            0.0f, 1.0f, 1.0f, 0, row_band, (const float*)band_table, nbands);
+        sx_upwind_chunk_go<float, true>(blocks, off, b, e, coff, info, chunks, lookup, (const float*)v, (float*)out,
+                                        width, height, (float)a, (float)bb, 0.0f, 1.0f, 1.0f, 0, row_band,
+                                        (const float*)band_table, nbands, nbr, stream);
     return cudaGetLastError();
 }
 
@@ -1646,27 +1771,41 @@ int sx_upwind_adjoint_chunk_parts(long long chunks)
     return (int)blocks;
 }
 
+template <typename T>
+static void sx_upwind_adjoint_chunk_go(int blocks, const int* off, const int* b, const int* e, const int* coff,
+                                       const int* info, long long chunks, const int* lookup, const unsigned short* nbr,
+                                       const T* w, const T* u, T* ubar, int width, int height, T a, T bb, T dt, T dx,
+                                       T dy, int p, double* partial, cudaStream_t stream)
+{
+    if (nbr)
+        sx_upwind_adjoint_chunk_kernel<T, true><<<blocks, 256, 0, stream>>>(off, b, e, coff, info, chunks, lookup, nbr,
+                                                                            w, u, ubar, width, height, a, bb, dt, dx,
+                                                                            dy, p, partial);
+    else
+        sx_upwind_adjoint_chunk_kernel<T, false><<<blocks, 256, 0, stream>>>(off, b, e, coff, info, chunks, lookup,
+                                                                             nullptr, w, u, ubar, width, height, a, bb,
+                                                                             dt, dx, dy, p, partial);
+}
+
 cudaError_t sx_upwind_adjoint_chunk_launch(const int* off, const int* b, const int* e, const int* coff, const int* info,
-                                           long long chunks, const int* lookup, const void* w, const void* u,
-                                           void* ubar, int width, int height, double a, double bb, double dt,
-                                           double dx, double dy, int dbl, double* partial, double* grads,
-                                           cudaStream_t stream)
+                                           long long chunks, const int* lookup, const unsigned short* nbr,
+                                           const void* w, const void* u, void* ubar, int width, int height, double a,
+                                           double bb, double dt, double dx, double dy, int dbl, double* partial,
+                                           double* grads, cudaStream_t stream)
 {
     const int blocks = sx_upwind_adjoint_chunk_parts(chunks);
     if (dbl) {
         double ddx = dx, ddy = dy;
         const int p = sx_pow2_pair(ddx, ddy);
-        sx_upwind_adjoint_chunk_kernel<double><<<blocks, 256, 0, stream>>>(off, b, e, coff, info, chunks, lookup,
-                                                                           (const double*)w, (const double*)u,
-                                                                           (double*)ubar, width, height, a, bb, dt,
-                                                                           ddx, ddy, p, partial);
+        sx_upwind_adjoint_chunk_go<double>(blocks, off, b, e, coff, info, chunks, lookup, nbr, (const double*)w,
+                                           (const double*)u, (double*)ubar, width, height, a, bb, dt, ddx, ddy, p,
+                                           partial, stream);
     } else {
         float fdx = (float)dx, fdy = (float)dy;
         const int p = sx_pow2_pair(fdx, fdy);
-        sx_upwind_adjoint_chunk_kernel<float><<<blocks, 256, 0, stream>>>(off, b, e, coff, info, chunks, lookup,
-                                                                          (const float*)w, (const float*)u,
-                                                                          (float*)ubar, width, height, (float)a,
-                                                                          (float)bb, (float)dt, fdx, fdy, p, partial);
+        sx_upwind_adjoint_chunk_go<float>(blocks, off, b, e, coff, info, chunks, lookup, nbr, (const float*)w,
+                                          (const float*)u, (float*)ubar, width, height, (float)a, (float)bb, (float)dt,
+                                          fdx, fdy, p, partial, stream);
     }
     sx_sum_pairs_kernel<<<1, 256, 0, stream>>>(partial, blocks, grads);
     return cudaGetLastError();

@@ -146,20 +146,24 @@ cudaError_t sx_upwind_plan_launch(const int* b, const int* e, int n, int* chunk_
 cudaError_t sx_upwind_plan_fill_launch(const int* rows, const int* off, int row_count, const int* b, const int* e,
                                        const int* coff, int n, const int* chunk_off, long long chunks,
                                        const int* lookup, int height, int* info, cudaStream_t stream);
+// nbr: the plan's neighbour table (sx_upwind_table_launch), or null to search the neighbour rows.
+cudaError_t sx_upwind_table_launch(const int* b, const int* e, const int* coff, const int* info, long long chunks,
+                                   unsigned short* nbr, int* status, cudaStream_t stream);
 cudaError_t sx_upwind_chunk_launch(const int* off, const int* b, const int* e, const int* coff, const int* info,
-                                   long long chunks, const int* lookup, const void* v, void* out, int width, int height,
-                                   double a, double bb, double dt, double dx, double dy, int dbl, cudaStream_t stream);
+                                   long long chunks, const int* lookup, const unsigned short* nbr, const void* v,
+                                   void* out, int width, int height, double a, double bb, double dt, double dx,
+                                   double dy, int dbl, cudaStream_t stream);
 cudaError_t sx_upwind_chunk_bands_launch(const int* off, const int* b, const int* e, const int* coff, const int* info,
-                                         long long chunks, const int* lookup, const void* v, void* out, int width,
-                                         int height, double a, double bb, const int* row_band, const void* band_table,
-                                         int nbands, int dbl, cudaStream_t stream);
+                                         long long chunks, const int* lookup, const unsigned short* nbr, const void* v,
+                                         void* out, int width, int height, double a, double bb, const int* row_band,
+                                         const void* band_table, int nbands, int dbl, cudaStream_t stream);
 void sx_upwind_band_table_fill(int dbl, const double* spacing, int nbands, void* table);
 int sx_upwind_adjoint_chunk_parts(long long chunks);
 cudaError_t sx_upwind_adjoint_chunk_launch(const int* off, const int* b, const int* e, const int* coff, const int* info,
-                                           long long chunks, const int* lookup, const void* w, const void* u,
-                                           void* ubar, int width, int height, double a, double bb, double dt,
-                                           double dx, double dy, int dbl, double* partial, double* grads,
-                                           cudaStream_t stream);
+                                           long long chunks, const int* lookup, const unsigned short* nbr,
+                                           const void* w, const void* u, void* ubar, int width, int height, double a,
+                                           double bb, double dt, double dx, double dy, int dbl, double* partial,
+                                           double* grads, cudaStream_t stream);
 // Level coupling by index tables (sx_coupling.cu)
 cudaError_t sx_index_copy_launch(int dtype, long long n, const int* dst_idx, const int* src_idx, const void* src,
                                  void* dst, cudaStream_t stream);

@@ -4,8 +4,8 @@ Arguments, checks and results follow ``subsetix_cupy/interval_stencil.py``
 of the reference.  On geometry whose rows are sorted and disjoint (the
 usual case, checked once per set) the chunked kernel ``sx_upwind_chunked``
 runs: warps take chunks of 128 cells of one interval in four coalesced
-sub-rounds, exchange left/right neighbours by shuffles and read the rows
-above and below with coalesced loads.  Other geometry takes ``sx_upwind``, which assigns 256 consecutive
+sub-rounds, exchange left/right neighbours by shuffles and find the cells
+above and below through a per-cell neighbour table built with the plan.  Other geometry takes ``sx_upwind``, which assigns 256 consecutive
 cells to each block and searches every neighbour.  Both give the same
 values.  Float32 is the
 reference's arithmetic.  Float64 values run the same formula in double
@@ -34,16 +34,17 @@ class _Geometry:
     lookup (and its synchronising range check) once.
     """
 
-    __slots__ = ("height", "lookup", "direct", "chunk_off", "chunks", "cell_off", "_seen")
+    __slots__ = ("height", "lookup", "direct", "chunk_off", "chunks", "cell_off", "table", "_seen")
 
     def __init__(self, height: int, lookup: torch.Tensor, direct: bool, chunk_off=None, chunks: int = 0,
-                 cell_off=None):
+                 cell_off=None, table=None):
         self.height = height
         self.lookup = lookup
         self.direct = direct
         self.chunk_off = chunk_off
         self.chunks = chunks
         self.cell_off = cell_off
+        self.table = table
         self._seen = None
 
     def canonical(self, cell_off: torch.Tensor) -> bool:
@@ -77,12 +78,13 @@ def _geometry(interval_set, height: int) -> _Geometry:
         raise ValueError("interval_set rows exceed provided height")
     flags = _core.check_rows(_t(interval_set.begin), _t(interval_set.end), _t(interval_set.row_offsets), device)
     direct = not (flags & (_lib.ROWS_UNSORTED_BEGIN | _lib.ROWS_OVERLAP | _lib.ROWS_EMPTY))
-    chunk_off, chunks, coff = (None, 0, None)
+    chunk_off, chunks, coff, table = (None, 0, None, None)
     if direct:
         b, e = _t(interval_set.begin), _t(interval_set.end)
-        coff, _ = _core.cell_offsets(b, e, device)
+        coff, cells = _core.cell_offsets(b, e, device)
         chunk_off, chunks = _core.upwind_plan(rows, _t(interval_set.row_offsets), b, e, coff, lookup, height, device)
-    geo = _Geometry(height, lookup, direct, chunk_off, chunks, coff)
+        table = _core.upwind_table(b, e, coff, chunk_off, chunks, cells, device)
+    geo = _Geometry(height, lookup, direct, chunk_off, chunks, coff, table)
     try:
         object.__setattr__(interval_set, "_sx_stencil", geo)
     except Exception:  # pragma: no cover - sets that refuse attributes
@@ -139,7 +141,7 @@ def step_upwind_interval(field: IntervalField, *, width: int, height: int, a: fl
             and geo.canonical(cell_off)):
         # fixed geometry with sorted, disjoint rows and packed values: the chunked kernel (same results)
         _core.upwind_chunked(_t(s.row_offsets), begin, _t(s.end), cell_off, geo.chunk_off, geo.chunks, geo.lookup, vals,
-                             out_t, width, height, a, b, dt, dx, dy, device)
+                             out_t, width, height, a, b, dt, dx, dy, device, table=geo.table)
     else:
         _core.upwind(_t(s.rows), _t(s.row_offsets), begin, _t(s.end), cell_off, int(vals.numel()), geo.lookup, vals,
                      out_t, width, height, a, b, dt, dx, dy, geo.direct and rid is None, device, row_ids=rid)

@@ -135,13 +135,16 @@ def test_checkpoint_spacing_and_fp32(cuda_device):
 
 
 @pytest.mark.parametrize("a,b", [(0.7, 0.4), (-0.5, -0.9)])
-def test_chunked_adjoint_equals_generic(cuda_device, a, b):
+@pytest.mark.parametrize("table", [True, False])
+def test_chunked_adjoint_equals_generic(cuda_device, a, b, table):
     from subsetix_b200 import _lib
     from subsetix_b200._runtime import ptr, stream_handle
 
     h = rand_set(400, 12.0, seed=8, row_stride=1, max_col=350, touching=True, row0=0)
     lvl = _level(h, 330, 400)      # some cells lie beyond the width
-    assert lvl.chunk_off is not None
+    assert lvl.chunk_off is not None and lvl.table is not None
+    if not table:
+        lvl.table = None           # neighbour rows searched instead of read from the plan's table
     rng = np.random.default_rng(3)
     w = torch.as_tensor(rng.standard_normal(lvl.cells), device="cuda")
     u = torch.as_tensor(rng.standard_normal(lvl.cells), device="cuda")

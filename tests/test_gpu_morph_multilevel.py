@@ -287,6 +287,8 @@ def test_upwind_chunked_equals_generic(cuda_device, dtype):
              rand_set(300, 1.0, seed=32, row_stride=2, row0=1),                   # sparse rows, gaps between rows
              (np.zeros(64, np.int32), np.full(64, 5000, np.int32), np.arange(65, dtype=np.int32),
               np.arange(64, dtype=np.int32))]                                     # long single intervals
+    shifted = rand_set(400, 12.0, seed=33, row_stride=1, touching=True, row0=0)
+    cases.append((shifted[0] - 150, shifted[1] - 150, shifted[2], shifted[3]))    # columns on both sides of 0
     for h in cases:
         S = dev_set(h)
         H = int(h[3].max()) + 2
@@ -296,14 +298,16 @@ def test_upwind_chunked_equals_generic(cuda_device, dtype):
         lookup, bad = _core.row_lookup(rows, H, dev)
         assert not bad
         chunk_off, chunks = _core.upwind_plan(rows, off, b, e, coff, lookup, H, dev)
+        table = _core.upwind_table(b, e, coff, chunk_off, chunks, cells, dev)
         v = torch.as_tensor(rng.standard_normal(cells), device=dev).to(dtype)
         for a_, b_ in ((0.6, 0.3), (-0.4, -0.9)):
             ref = torch.empty_like(v)
-            got = torch.empty_like(v)
             _core.upwind(rows, off, b, e, coff, cells, lookup, v, ref, W, H, a_, b_, 1e-3, 1e-2, 1e-2, False, dev)
-            _core.upwind_chunked(off, b, e, coff, chunk_off, chunks, lookup, v, got, W, H, a_, b_, 1e-3, 1e-2, 1e-2,
-                                 dev)
-            assert torch.equal(got, ref)
+            for tab in (None, table):  # neighbour rows searched, then read from the plan's table
+                got = torch.full_like(v, float("nan"))
+                _core.upwind_chunked(off, b, e, coff, chunk_off, chunks, lookup, v, got, W, H, a_, b_, 1e-3, 1e-2,
+                                     1e-2, dev, table=tab)
+                assert torch.equal(got, ref), tab is None
 
 
 def test_upwind_padded_cell_offsets(cuda_device):
@@ -329,6 +333,37 @@ def test_upwind_padded_cell_offsets(cuda_device):
     got = sc.step_upwind_interval(fp, **kw).cpu().numpy()
     for i in range(lens.size):
         assert np.array_equal(got[padded[i]:padded[i] + lens[i]], ref[packed[i]:packed[i + 1]])
+
+
+def test_neighbour_table_with_gapped_offsets(cuda_device):
+    """The table is exact wherever its byte offsets fit; gaps too wide for a byte are reported, not stored."""
+    from subsetix_b200 import _core, _lib
+
+    dev = torch.device("cuda", 0)
+    h = rand_set(120, 6.0, seed=42, row_stride=1, touching=True, row0=0)
+    b, e, off, rows = (torch.as_tensor(a, device=dev) for a in h)
+    lens = (e - b).long()
+    H, W = int(h[3].max()) + 2, 200
+    lookup, bad = _core.row_lookup(rows, H, dev)
+    assert not bad
+    rng = np.random.default_rng(6)
+    for gap, fits in ((2, True), (400, False)):
+        coff = torch.zeros(lens.numel() + 1, dtype=torch.int32, device=dev)
+        coff[1:] = torch.cumsum(lens + gap, 0).to(torch.int32)
+        cells = int(coff[-1])
+        chunk_off, chunks = _core.upwind_plan(rows, off, b, e, coff, lookup, H, dev)
+        v = torch.as_tensor(rng.standard_normal(cells).astype(np.float32), device=dev)
+        if not fits:
+            with pytest.raises(_lib.SubsetixError, match="prefix sum"):
+                _core.upwind_table(b, e, coff, chunk_off, chunks, cells, dev)
+            continue
+        table = _core.upwind_table(b, e, coff, chunk_off, chunks, cells, dev)
+        ref = torch.zeros_like(v)
+        got = torch.zeros_like(v)
+        _core.upwind_chunked(off, b, e, coff, chunk_off, chunks, lookup, v, ref, W, H, 0.5, 0.5, 1e-3, 1e-2, 1e-2, dev)
+        _core.upwind_chunked(off, b, e, coff, chunk_off, chunks, lookup, v, got, W, H, 0.5, 0.5, 1e-3, 1e-2, 1e-2, dev,
+                             table=table)
+        assert torch.equal(got, ref)
 
 
 # ------------------------------------------------ percentile tagging and level helpers (reference fixtures)
