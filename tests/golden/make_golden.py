@@ -147,12 +147,12 @@ def main():
     rec = Recorder()
     a_host = synth.random_rows_set(0)
     b_host = synth.random_rows_set(1)
-    put_host(rec, "cfg1/A", a_host)
-    put_host(rec, "cfg1/B", b_host)
+    put_host(rec, "rows256/A", a_host)
+    put_host(rec, "rows256/B", b_host)
     A, B = mk(a_host), mk(b_host)
     for name, fn in binops.items():
-        rec.put_set(f"cfg1/{name}", sc.evaluate(fn(sc.make_input(A), sc.make_input(B))))
-    rec.put_set("cfg1/dilate11", sx_morph.dilate_interval_set(A, halo_x=1, halo_y=1))
+        rec.put_set(f"rows256/{name}", sc.evaluate(fn(sc.make_input(A), sc.make_input(B))))
+    rec.put_set("rows256/dilate11", sx_morph.dilate_interval_set(A, halo_x=1, halo_y=1))
 
     rng = np.random.default_rng(1234)
     kinds = ["canonical", "touching", "empties"]
@@ -225,11 +225,11 @@ def main():
                 rec.put_set(f"m{mcase}/ghost_{w}_{h}", sx_morph.ghost_zones(S, halo_x=1, halo_y=1, width=w, height=h))
             mcase += 1
     rec.put("morph_count", np.array(mcase))
-    # config-1 morphology
+    # morphology of the 256 x 256 random-rows set
     for hx, hy in [(1, 1), (2, 2), (4, 4), (3, 0)]:
-        rec.put_set(f"cfg1/dilate_{hx}_{hy}", sx_morph.dilate_interval_set(A, halo_x=hx, halo_y=hy))
-        rec.put_set(f"cfg1/erode_{hx}_{hy}", sx_morph.erode_interval_set(A, halo_x=hx, halo_y=hy, width=256, height=256))
-    put_host(rec, "cfg1/A", a_host)
+        rec.put_set(f"rows256/dilate_{hx}_{hy}", sx_morph.dilate_interval_set(A, halo_x=hx, halo_y=hy))
+        rec.put_set(f"rows256/erode_{hx}_{hy}", sx_morph.erode_interval_set(A, halo_x=hx, halo_y=hy, width=256, height=256))
+    put_host(rec, "rows256/A", a_host)
     if "morph" in only:
         rec.save("morph.npz")
 

@@ -277,7 +277,7 @@ def test_vtk_quads_device_equal_host(cuda_device, tmp_path):
 
 
 def test_amr2_simulation_128_physical_threshold(cuda_device):
-    """Config 3's loop at 128^2 with the physical threshold 0.05 dx (12 % of the cells refined), 40 steps,
+    """The two-level AMR loop at 128^2 with the physical threshold 0.05 dx (12 % of the cells refined), 40 steps,
     regrid every 10: the drop-in AMR2Simulation and the fused engine against the reference's own run."""
     from subsetix_b200.subsetix_amr2.fused import FusedTwoLevelAMR
 

@@ -176,7 +176,7 @@ def test_fused_step_any_width(cuda_device, res, dtype):
 
 
 def test_batched_upwind_per_set_spacing_and_graph_step(cuda_device):
-    """Config 4's form: every set with dx = 1/side and its own CFL time step, against the oracle per set;
+    """Uneven batched sets, every set with dx = 1/side and its own CFL time step, against the oracle per set;
     the graph-captured BatchStep equals the direct calls."""
     from subsetix_b200 import synth
     from subsetix_b200.batch import BatchStep, SetBatch, batched_binary, batched_upwind

@@ -51,13 +51,13 @@ def test_morphology_fixtures(cuda_device):
     assert checked >= 60 * 15
 
 
-def test_morphology_config1(cuda_device):
+def test_morphology_random_rows_256(cuda_device):
     data = load(MORPH)
-    A = dev_set(get_set(data, "cfg1/A"))
+    A = dev_set(get_set(data, "rows256/A"))
     for hx, hy in [(1, 1), (2, 2), (4, 4), (3, 0)]:
-        assert_same(sc.dilate_interval_set(A, halo_x=hx, halo_y=hy), get_set(data, f"cfg1/dilate_{hx}_{hy}"))
+        assert_same(sc.dilate_interval_set(A, halo_x=hx, halo_y=hy), get_set(data, f"rows256/dilate_{hx}_{hy}"))
         assert_same(sc.erode_interval_set(A, halo_x=hx, halo_y=hy, width=256, height=256),
-                    get_set(data, f"cfg1/erode_{hx}_{hy}"))
+                    get_set(data, f"rows256/erode_{hx}_{hy}"))
 
 
 @pytest.mark.parametrize("hx,hy", [(1, 1), (2, 4), (0, 6), (3, 9), (5, 0)])

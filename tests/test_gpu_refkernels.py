@@ -73,7 +73,7 @@ def _gauss(n, sigma=0.05):
     return np.exp(-((X - 0.5) ** 2 + (Y - 0.5) ** 2) / (2 * sigma ** 2)).astype(np.float32)
 
 
-_VELOCITIES = [(1.0, 0.5, 0.5 / (1.5 * 2048), 1 / 2048, 1 / 2048),  # config 3's fine level
+_VELOCITIES = [(1.0, 0.5, 0.5 / (1.5 * 2048), 1 / 2048, 1 / 2048),  # the fine level of the 1024^2 AMR run
                (1.0, 0.5, 0.5 / (1.5 * 2048), 1 / 1024, 1 / 1024),  # and its coarse level
                (0.7, -0.3, 0.37, 0.9, 1.1), (-1.3, 0.9, 0.05, 0.3, 0.7), (0.3, 0.123, 0.77, 1.0, 1.0),
                (1.7, -2.1, 0.013, 0.1, 0.1)]

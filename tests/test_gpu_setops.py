@@ -132,11 +132,11 @@ def _binop(name, a, b):
     return sc.evaluate(_ops()[name](sc.make_input(a), sc.make_input(b)))
 
 
-def test_config1_setops(cuda_device):
+def test_random_rows_256_setops(cuda_device):
     g = load("setops.npz")
-    A, B = dev_set(get_set(g, "cfg1/A")), dev_set(get_set(g, "cfg1/B"))
+    A, B = dev_set(get_set(g, "rows256/A")), dev_set(get_set(g, "rows256/B"))
     for op in BIN:
-        assert_same(_binop(op, A, B), get_set(g, f"cfg1/{op}"), op)
+        assert_same(_binop(op, A, B), get_set(g, f"rows256/{op}"), op)
 
 
 def test_fixture_binary_cases(cuda_device):

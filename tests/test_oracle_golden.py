@@ -36,12 +36,12 @@ def ulp_diff32(a, b):
 BIN = ["union", "intersection", "difference", "symmetric_difference", "complement"]
 
 
-def test_config1_setops():
+def test_random_rows_256_setops():
     g = load("setops.npz")
-    A, B = iset(get_set(g, "cfg1/A")), iset(get_set(g, "cfg1/B"))
+    A, B = iset(get_set(g, "rows256/A")), iset(get_set(g, "rows256/B"))
     for op in BIN:
-        assert_set_equal(O.BINARY[op](A, B), get_set(g, f"cfg1/{op}"), op)
-    assert_set_equal(O.dilate(A, 1, 1), get_set(g, "cfg1/dilate11"), "dilate")
+        assert_set_equal(O.BINARY[op](A, B), get_set(g, f"rows256/{op}"), op)
+    assert_set_equal(O.dilate(A, 1, 1), get_set(g, "rows256/dilate11"), "dilate")
 
 
 def test_random_binary_cases():
@@ -80,10 +80,10 @@ def test_morphology_cases():
             assert_set_equal(O.clip(S, w, h), get_set(g, f"m{c}/clip_{w}_{h}"), f"m{c} clip")
             assert_set_equal(O.erode(S, 1, 1, width=w, height=h), get_set(g, f"m{c}/erode_{w}_{h}"), f"m{c} erode")
             assert_set_equal(O.ghost_zones(S, 1, 1, width=w, height=h), get_set(g, f"m{c}/ghost_{w}_{h}"), f"m{c} ghost")
-    A = iset(get_set(g, "cfg1/A"))
+    A = iset(get_set(g, "rows256/A"))
     for hx, hy in [(1, 1), (2, 2), (4, 4), (3, 0)]:
-        assert_set_equal(O.dilate(A, hx, hy), get_set(g, f"cfg1/dilate_{hx}_{hy}"))
-        assert_set_equal(O.erode(A, hx, hy, width=256, height=256), get_set(g, f"cfg1/erode_{hx}_{hy}"))
+        assert_set_equal(O.dilate(A, hx, hy), get_set(g, f"rows256/dilate_{hx}_{hy}"))
+        assert_set_equal(O.erode(A, hx, hy, width=256, height=256), get_set(g, f"rows256/erode_{hx}_{hy}"))
 
 
 def test_multilevel_sets():
@@ -193,7 +193,7 @@ def test_level_helpers():
 
 
 def test_amr_simulation_128_physical_threshold():
-    """Config 3's loop at 128^2 with the physical threshold 0.05 dx (12 % refined), 40 steps."""
+    """The two-level AMR loop at 128^2 with the physical threshold 0.05 dx (12 % refined), 40 steps."""
     g = load("amr_large.npz")
     res, steps, every, va, vb, dt, thr = g["g128/params"].tolist()
     sim = O.AMR2(int(res), (va, vb), cfl=0.5, threshold=thr, grading_pad=1)
