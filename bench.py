@@ -302,7 +302,9 @@ def amr_section(device, steps: int = 200, every: int = 10, res: int = 1024, thre
                        f"CFL 0.5, {steps} steps, regrid+grading every {every}, refine threshold {threshold:g} "
                        "(reference gradient: half the central difference)",
            "cells_per_step": cells, "steps": steps, "refine_threshold": threshold,
-           "refined_fraction_final": float((ref.actions != 0).float().mean())}
+           "refined_fraction_final": float((ref.actions != 0).float().mean()),
+           "residency": f"the step's two value buffers ({2 * cells * 4 / 1e6:.0f} MB in FP32) stay in the 126 MB L2, "
+                        "so the algorithmic GB/s below are not HBM traffic (ncu sees about half of them at DRAM)"}
     peak, _ = peak_hbm()
     for name, (eng, ms, m0) in runs.items():
         es = 8 if eng.dtype == torch.float64 else 4
@@ -311,7 +313,8 @@ def amr_section(device, steps: int = 200, every: int = 10, res: int = 1024, thre
         # and writes tag and action bytes once per period
         algo = res * res * (10 * es + 1) + res * res * (es + 3) / every
         out[name] = {"ms_per_step": ms / steps, "gcell_updates_per_s": cells * steps / (ms / 1e3) / 1e9,
-                     "hbm_gbs": algo / (ms / steps / 1e3) / 1e9, "hbm_frac": algo / (ms / steps / 1e3) / 1e9 / peak,
+                     "algorithmic_gbs": algo / (ms / steps / 1e3) / 1e9,
+                     "algorithmic_frac_of_hbm_peak": algo / (ms / steps / 1e3) / 1e9 / peak,
                      "mass_final": float(eng.mass()[0]), "mass_initial": m0,
                      "restriction_defect": float(eng.restriction_defect()[0])}
     for lvl in ("coarse_values", "fine_values"):
