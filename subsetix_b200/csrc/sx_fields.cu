@@ -624,6 +624,12 @@ __global__ void __launch_bounds__(256) sx_sum_pairs_kernel(const double* __restr
 // blocks (48 warps per SM, 40 registers) hide the two dependent loads of a
 // chunk best (config-4 batch on a B200: 1.79 ms at 1 block, 1.42 ms at 6,
 // 1.45 ms at 8).
+// The same for the adjoint chunk kernel: four blocks (64 registers, no
+// spills) took the three-level backward pass from 16.7 to 15.5 ms on a B200;
+// five and six spill and are slower.
+#ifndef SX_UPWIND_ADJOINT_MIN_BLOCKS
+#define SX_UPWIND_ADJOINT_MIN_BLOCKS 4
+#endif
 #ifndef SX_UPWIND_TABLE_MIN_BLOCKS
 #define SX_UPWIND_TABLE_MIN_BLOCKS 6
 #endif
@@ -985,7 +991,7 @@ __global__ void __launch_bounds__(256, TABLE ? SX_UPWIND_TABLE_MIN_BLOCKS : SX_U
 // serves both arrays (w and u share the geometry).  Per-block float64
 // partial sums of dL/da, dL/db go to partial[2 * block].
 template <typename T, bool TABLE>
-__global__ void __launch_bounds__(256) sx_upwind_adjoint_chunk_kernel(const int* __restrict__ off,
+__global__ void __launch_bounds__(256, SX_UPWIND_ADJOINT_MIN_BLOCKS) sx_upwind_adjoint_chunk_kernel(const int* __restrict__ off,
                                                                       const int* __restrict__ b,
                                                                       const int* __restrict__ e,
                                                                       const int* __restrict__ coff,
