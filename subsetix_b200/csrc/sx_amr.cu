@@ -142,8 +142,22 @@ __global__ void __launch_bounds__(256) sx_amr_step_full_kernel(const T* __restri
     const T cd = y > 0 ? C[ci - W] : (T)0;
     const T cu = y + 1 < H ? C[ci + W] : (T)0;
     const T cn = sxa_upwind_cell(c, cl, cr, cd, cu, a, b, dt, dxc, dyc, pow2c);
-    // fine block: rows 2y-1 .. 2y+2, columns 2x-1 .. 2x+2
     const int fx = 2 * x, fy = 2 * y;
+    T* CO = cout + plane * blockIdx.z;
+    T* FO = fout + 4 * plane * blockIdx.z;
+    if (actions[plane * blockIdx.z + ci] != 1) {
+        // not refined: the synchronisation overwrites the fine block with the
+        // new coarse value, so its own upwind update is never needed
+        CO[ci] = cn;
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            T* row = FO + (long long)(fy + j) * FW + fx;
+            row[0] = cn;
+            row[1] = cn;
+        }
+        return;
+    }
+    // refined: fine block, rows 2y-1 .. 2y+2, columns 2x-1 .. 2x+2
     T v[4][4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
@@ -162,15 +176,8 @@ __global__ void __launch_bounds__(256) sx_amr_step_full_kernel(const T* __restri
         for (int i = 0; i < 2; ++i)
             fn[j][i] = sxa_upwind_cell(v[j + 1][i + 1], v[j + 1][i], v[j + 1][i + 2], v[j][i + 1], v[j + 2][i + 1], a, b,
                                        dt, dxf, dyf, pow2f);
-    T* CO = cout + plane * blockIdx.z;
-    T* FO = fout + 4 * plane * blockIdx.z;
-    if (actions[plane * blockIdx.z + ci] == 1) {
-        T acc = sxa_add(sxa_add(sxa_add(sxa_add((T)0, fn[0][0]), fn[0][1]), fn[1][0]), fn[1][1]);
-        CO[ci] = sxa_mul(acc, norm);
-    } else {
-        CO[ci] = cn;
-        fn[0][0] = fn[0][1] = fn[1][0] = fn[1][1] = cn;
-    }
+    T acc = sxa_add(sxa_add(sxa_add(sxa_add((T)0, fn[0][0]), fn[0][1]), fn[1][0]), fn[1][1]);
+    CO[ci] = sxa_mul(acc, norm);
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
         T* row = FO + (long long)(fy + j) * FW + fx;
