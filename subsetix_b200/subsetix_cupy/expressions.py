@@ -381,7 +381,9 @@ def _same_rows(sets: Sequence[IntervalSet]) -> bool:
     others = [_t(s.rows) for s in sets[1:] if _t(s.rows).data_ptr() != r0.data_ptr() or n0 == 0]
     if not others or n0 == 0:
         return True
-    return all(torch.equal(r0, o) for o in others)
+    # one device comparison and one read-back for all the sets
+    same = torch.stack([torch.eq(r0, o).all() for o in others])
+    return bool(same.all())
 
 
 def _row_bounds(sets: Sequence[IntervalSet]) -> Tuple[int, int]:
