@@ -886,6 +886,91 @@ __global__ void __launch_bounds__(256) sx_chunk_table_kernel(const int* __restri
 // TABLE the neighbour-row indices come from the plan's neighbour table
 // (sx_chunk_table_kernel) instead of a search: one coalesced 16-bit load per
 // cell, issued together with the cell's own value.
+// One chunk's update (the body of sx_upwind_chunk_kernel).  With EDGE false
+// the chunk's cells and their left and right neighbours all lie in
+// [0, width), so the domain tests are known to pass and are left out.
+template <typename T, bool TABLE, bool EDGE>
+__device__ __forceinline__ void sx_chunk_upwind(const int4 p0, const int4 p1, const int4 p2, const int4 p3, int lane,
+                                                const int* __restrict__ b, const int* __restrict__ e,
+                                                const int* __restrict__ coff, const unsigned short* __restrict__ nbr,
+                                                const T* __restrict__ v, T* __restrict__ out, int width, T a, T bb,
+                                                T dt, T dx, T dy, int pow2)
+{
+    const int x0 = p0.x, ie = p0.y, touch = p0.w, ib = p3.w;
+    const long long c0 = p0.z;
+    // sub-rounds that hold cells (the same for the whole warp): chunks of
+    // short intervals skip the empty ones instead of issuing them masked
+    const int nq = min(SX_CHUNK_SUB, (ie - x0 + 31) >> 5);
+    T cen[SX_CHUNK_SUB];
+    int idn[SX_CHUNK_SUB], iup[SX_CHUNK_SUB];
+    const SxRowReader dn{p1.x, p1.y, p1.z, p1.w, p2.x};
+    const SxRowReader upc{p2.y, p2.z, p2.w, p3.x, p3.y};
+    if (TABLE) {
+        const int bdn = sx_chunk_base(dn, x0), bup = sx_chunk_base(upc, x0);
+        unsigned nb[SX_CHUNK_SUB];
+#pragma unroll
+        for (int q = 0; q < SX_CHUNK_SUB; ++q) {
+            const int x = x0 + 32 * q + lane;
+            const bool act = q < nq && x < ie;
+            cen[q] = act ? v[c0 + 32 * q + lane] : (T)0;
+            nb[q] = act ? (unsigned)__ldg(nbr + c0 + 32 * q + lane) : 0xFFFFu;
+        }
+#pragma unroll
+        for (int q = 0; q < SX_CHUNK_SUB; ++q) {
+            const int x = x0 + 32 * q + lane;
+            const bool xin = !EDGE || (x >= 0 && x < width);
+            const unsigned lo = nb[q] & 0xFFu, hi = nb[q] >> 8;
+            idn[q] = (xin && lo != 0xFFu) ? bdn + (int)lo : -1;
+            iup[q] = (xin && hi != 0xFFu) ? bup + (int)hi : -1;
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < SX_CHUNK_SUB; ++q) {
+            const int x = x0 + 32 * q + lane;
+            cen[q] = (q < nq && x < ie) ? v[c0 + 32 * q + lane] : (T)0;
+        }
+        // neighbour-row value indices of all four sub-rounds first, then all
+        // their loads at once, so the chunk waits for one round trip
+        sx_row_indices<SX_CHUNK_SUB, EDGE>(dn, x0, nq, ie, width, b, e, coff, lane, idn);
+        sx_row_indices<SX_CHUNK_SUB, EDGE>(upc, x0, nq, ie, width, b, e, coff, lane, iup);
+    }
+    T vdn[SX_CHUNK_SUB], vup[SX_CHUNK_SUB];
+#pragma unroll
+    for (int q = 0; q < SX_CHUNK_SUB; ++q) {
+        vdn[q] = idn[q] >= 0 ? v[idn[q]] : (T)0;
+        vup[q] = iup[q] >= 0 ? v[iup[q]] : (T)0;
+    }
+    T prev_last = (T)0;  // lane 31's centre of the previous sub-round
+#pragma unroll
+    for (int q = 0; q < SX_CHUNK_SUB; ++q) {
+        if (q >= nq) break;
+        const int x = x0 + 32 * q + lane;
+        const bool act = x < ie;
+        const long long c = c0 + 32 * q + lane;
+        const T center = cen[q];
+        T from_left = __shfl_up_sync(0xFFFFFFFFu, center, 1);
+        if (lane == 0) from_left = prev_last;
+        T from_right = __shfl_down_sync(0xFFFFFFFFu, center, 1);
+        const T next_first = q + 1 < SX_CHUNK_SUB ? __shfl_sync(0xFFFFFFFFu, cen[q + 1 < SX_CHUNK_SUB ? q + 1 : q], 0)
+                                                  : (T)0;
+        if (lane == 31) from_right = next_first;
+        prev_last = __shfl_sync(0xFFFFFFFFu, center, 31);
+        T left, right;
+        const bool lin = !EDGE || (x - 1 >= 0 && x - 1 < width), rin = !EDGE || (x + 1 >= 0 && x + 1 < width);
+        if (x - 1 >= ib) left = lin ? ((lane > 0 || q > 0) ? from_left : v[c - 1]) : (T)0;
+        else left = (act && (touch & 1) && lin) ? v[c - 1] : (T)0;
+        if (x + 1 < ie) right = rin ? ((lane < 31 || q + 1 < SX_CHUNK_SUB) ? from_right : v[c + 1]) : (T)0;
+        else right = (act && (touch & 2) && rin) ? v[c + 1] : (T)0;
+        const T down = vdn[q];
+        const T up = vup[q];
+        if (act) {
+            const T du_dx = a >= (T)0 ? sx_over(sx_sub(center, left), dx, pow2) : sx_over(sx_sub(right, center), dx, pow2);
+            const T du_dy = bb >= (T)0 ? sx_over(sx_sub(center, down), dy, pow2) : sx_over(sx_sub(up, center), dy, pow2);
+            out[c] = sx_upwind_update(center, du_dx, du_dy, a, bb, dt);
+        }
+    }
+}
+
 template <typename T, bool BANDS, bool TABLE>
 __global__ void __launch_bounds__(256, TABLE ? SX_UPWIND_TABLE_MIN_BLOCKS : SX_UPWIND_MIN_BLOCKS)
     sx_upwind_chunk_kernel(const int* __restrict__ off, const int* __restrict__ b, const int* __restrict__ e,
@@ -900,8 +985,7 @@ __global__ void __launch_bounds__(256, TABLE ? SX_UPWIND_TABLE_MIN_BLOCKS : SX_U
     for (long long u = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); u < chunks; u += warps) {
         const int4* pl = (const int4*)(info + (long long)SX_PLAN_INTS * u);
         const int4 p0 = __ldg(pl), p1 = __ldg(pl + 1), p2 = __ldg(pl + 2), p3 = __ldg(pl + 3);
-        const int x0 = p0.x, ie = p0.y, touch = p0.w, ib = p3.w;
-        const long long c0 = p0.z;
+        const int x0 = p0.x, ie = p0.y;
         T dt = dt_all, dx = dx_all, dy = dy_all;
         int pow2 = pow2_all;
         if (BANDS) {
@@ -912,77 +996,14 @@ __global__ void __launch_bounds__(256, TABLE ? SX_UPWIND_TABLE_MIN_BLOCKS : SX_U
             dt = __ldg(band_table + 4 * q + 2);
             pow2 = __ldg(band_table + 4 * q + 3) != (T)0;
         }
-        // sub-rounds that hold cells (the same for the whole warp): chunks of
-        // short intervals skip the empty ones instead of issuing them masked
-        const int nq = min(SX_CHUNK_SUB, (ie - x0 + 31) >> 5);
-        T cen[SX_CHUNK_SUB];
-        int idn[SX_CHUNK_SUB], iup[SX_CHUNK_SUB];
-        const SxRowReader dn{p1.x, p1.y, p1.z, p1.w, p2.x};
-        const SxRowReader upc{p2.y, p2.z, p2.w, p3.x, p3.y};
-        if (TABLE) {
-            const int bdn = sx_chunk_base(dn, x0), bup = sx_chunk_base(upc, x0);
-            unsigned nb[SX_CHUNK_SUB];
-#pragma unroll
-            for (int q = 0; q < SX_CHUNK_SUB; ++q) {
-                const int x = x0 + 32 * q + lane;
-                const bool act = q < nq && x < ie;
-                cen[q] = act ? v[c0 + 32 * q + lane] : (T)0;
-                nb[q] = act ? (unsigned)__ldg(nbr + c0 + 32 * q + lane) : 0xFFFFu;
-            }
-#pragma unroll
-            for (int q = 0; q < SX_CHUNK_SUB; ++q) {
-                const int x = x0 + 32 * q + lane;
-                const bool xin = x >= 0 && x < width;
-                const unsigned lo = nb[q] & 0xFFu, hi = nb[q] >> 8;
-                idn[q] = (xin && lo != 0xFFu) ? bdn + (int)lo : -1;
-                iup[q] = (xin && hi != 0xFFu) ? bup + (int)hi : -1;
-            }
-        } else {
-#pragma unroll
-            for (int q = 0; q < SX_CHUNK_SUB; ++q) {
-                const int x = x0 + 32 * q + lane;
-                cen[q] = (q < nq && x < ie) ? v[c0 + 32 * q + lane] : (T)0;
-            }
-            // neighbour-row value indices of all four sub-rounds first, then all
-            // their loads at once, so the chunk waits for one round trip
-            sx_row_indices<SX_CHUNK_SUB>(dn, x0, nq, ie, width, b, e, coff, lane, idn);
-            sx_row_indices<SX_CHUNK_SUB>(upc, x0, nq, ie, width, b, e, coff, lane, iup);
-        }
-        T vdn[SX_CHUNK_SUB], vup[SX_CHUNK_SUB];
-#pragma unroll
-        for (int q = 0; q < SX_CHUNK_SUB; ++q) {
-            vdn[q] = idn[q] >= 0 ? v[idn[q]] : (T)0;
-            vup[q] = iup[q] >= 0 ? v[iup[q]] : (T)0;
-        }
-        T prev_last = (T)0;  // lane 31's centre of the previous sub-round
-#pragma unroll
-        for (int q = 0; q < SX_CHUNK_SUB; ++q) {
-            if (q >= nq) break;
-            const int x = x0 + 32 * q + lane;
-            const bool act = x < ie;
-            const long long c = c0 + 32 * q + lane;
-            const T center = cen[q];
-            T from_left = __shfl_up_sync(0xFFFFFFFFu, center, 1);
-            if (lane == 0) from_left = prev_last;
-            T from_right = __shfl_down_sync(0xFFFFFFFFu, center, 1);
-            const T next_first = q + 1 < SX_CHUNK_SUB ? __shfl_sync(0xFFFFFFFFu, cen[q + 1 < SX_CHUNK_SUB ? q + 1 : q], 0)
-                                                      : (T)0;
-            if (lane == 31) from_right = next_first;
-            prev_last = __shfl_sync(0xFFFFFFFFu, center, 31);
-            T left, right;
-            const bool lin = x - 1 >= 0 && x - 1 < width, rin = x + 1 >= 0 && x + 1 < width;
-            if (x - 1 >= ib) left = lin ? ((lane > 0 || q > 0) ? from_left : v[c - 1]) : (T)0;
-            else left = (act && (touch & 1) && lin) ? v[c - 1] : (T)0;
-            if (x + 1 < ie) right = rin ? ((lane < 31 || q + 1 < SX_CHUNK_SUB) ? from_right : v[c + 1]) : (T)0;
-            else right = (act && (touch & 2) && rin) ? v[c + 1] : (T)0;
-            const T down = vdn[q];
-            const T up = vup[q];
-            if (act) {
-                const T du_dx = a >= (T)0 ? sx_over(sx_sub(center, left), dx, pow2) : sx_over(sx_sub(right, center), dx, pow2);
-                const T du_dy = bb >= (T)0 ? sx_over(sx_sub(center, down), dy, pow2) : sx_over(sx_sub(up, center), dy, pow2);
-                out[c] = sx_upwind_update(center, du_dx, du_dy, a, bb, dt);
-            }
-        }
+        // interior chunk: every cell and its left and right neighbours inside [0, width)
+        const bool edge = !(x0 >= 1 && x0 + min(ie - x0, SX_CHUNK) < width);  // x0 + ... <= ie: no overflow
+        if (edge)
+            sx_chunk_upwind<T, TABLE, true>(p0, p1, p2, p3, lane, b, e, coff, nbr, v, out, width, a, bb, dt, dx, dy,
+                                            pow2);
+        else
+            sx_chunk_upwind<T, TABLE, false>(p0, p1, p2, p3, lane, b, e, coff, nbr, v, out, width, a, bb, dt, dx, dy,
+                                             pow2);
     }
 }
 
