@@ -626,7 +626,9 @@ __global__ void __launch_bounds__(256) sx_sum_pairs_kernel(const double* __restr
 // 1.45 ms at 8).
 // The same for the adjoint chunk kernel: four blocks (64 registers, no
 // spills) took the three-level backward pass from 16.7 to 15.5 ms on a B200;
-// five and six spill and are slower.
+// five and six spill and are slower.  Both knobs apply to float32; the
+// float64 forms keep two (adjoint) and three (table) blocks, where their
+// registers fit without spilling.
 #ifndef SX_UPWIND_ADJOINT_MIN_BLOCKS
 #define SX_UPWIND_ADJOINT_MIN_BLOCKS 4
 #endif
@@ -972,7 +974,7 @@ __device__ __forceinline__ void sx_chunk_upwind(const int4 p0, const int4 p1, co
 }
 
 template <typename T, bool BANDS, bool TABLE>
-__global__ void __launch_bounds__(256, TABLE ? SX_UPWIND_TABLE_MIN_BLOCKS : SX_UPWIND_MIN_BLOCKS)
+__global__ void __launch_bounds__(256, TABLE ? (sizeof(T) == 4 ? SX_UPWIND_TABLE_MIN_BLOCKS : 3) : SX_UPWIND_MIN_BLOCKS)
     sx_upwind_chunk_kernel(const int* __restrict__ off, const int* __restrict__ b, const int* __restrict__ e,
                            const int* __restrict__ coff, const int* __restrict__ info, long long chunks,
                            const int* __restrict__ lookup, const T* __restrict__ v, T* __restrict__ out, int width,
@@ -1011,8 +1013,124 @@ __global__ void __launch_bounds__(256, TABLE ? SX_UPWIND_TABLE_MIN_BLOCKS : SX_U
 // same values as sx_upwind_adjoint_kernel.  One row reader per direction
 // serves both arrays (w and u share the geometry).  Per-block float64
 // partial sums of dL/da, dL/db go to partial[2 * block].
+// One chunk of sx_upwind_adjoint_chunk_kernel; dL/da and dL/db are added
+// into ga and gb.  With EDGE false the chunk's row lies in [0, height) and its
+// cells and their left and right neighbours in [0, width), so the domain tests
+// are known to pass and are left out.
+template <typename T, bool TABLE, bool EDGE>
+__device__ __forceinline__ void sx_chunk_adjoint(const int4 p0, const int4 p1, const int4 p2, const int4 p3, int lane,
+                                                 const int* __restrict__ b, const int* __restrict__ e,
+                                                 const int* __restrict__ coff,
+                                                 const unsigned short* __restrict__ nbr, const T* __restrict__ w,
+                                                 const T* __restrict__ u, T* __restrict__ ubar, int width, int height,
+                                                 T a, T bb, T dt, T dx, T dy, int pow2, double& ga, double& gb)
+{
+    const int x0 = p0.x, ie = p0.y, touch = p0.w, row = p3.z, ib = p3.w;
+    const long long c0 = p0.z;
+    T wc[SX_CHUNK_SUB], uc[SX_CHUNK_SUB];
+#pragma unroll
+    for (int q = 0; q < SX_CHUNK_SUB; ++q) {
+        const bool act = x0 + 32 * q + lane < ie;
+        wc[q] = act ? w[c0 + 32 * q + lane] : (T)0;
+        uc[q] = act ? u[c0 + 32 * q + lane] : (T)0;
+    }
+    SxRowReader dn{p1.x, p1.y, p1.z, p1.w, p2.x};
+    SxRowReader upr{p2.y, p2.z, p2.w, p3.x, p3.y};
+    // neighbour-row value indices of all four sub-rounds first, then all
+    // their loads at once.  u reads need the forward's domain test (made by
+    // the index), w reads need this cell's domain as well (jdom).
+    const bool rdom = !EDGE || (row >= 0 && row < height);
+    int idn[SX_CHUNK_SUB], iup[SX_CHUNK_SUB];
+    if (TABLE) {  // the plan's neighbour table, as in the forward step
+        const int bdn = sx_chunk_base(dn, x0), bup = sx_chunk_base(upr, x0);
+#pragma unroll
+        for (int q = 0; q < SX_CHUNK_SUB; ++q) {
+            const int x = x0 + 32 * q + lane;
+            const unsigned nb = x < ie ? (unsigned)__ldg(nbr + c0 + 32 * q + lane) : 0xFFFFu;
+            const bool xin = !EDGE || (x >= 0 && x < width);
+            idn[q] = (xin && (nb & 0xFFu) != 0xFFu) ? bdn + (int)(nb & 0xFFu) : -1;
+            iup[q] = (xin && (nb >> 8) != 0xFFu) ? bup + (int)(nb >> 8) : -1;
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < SX_CHUNK_SUB; ++q) {
+            const int x = x0 + 32 * q + lane;
+            idn[q] = sx_row_index(dn, x, width, b, e, coff, x < ie);
+            iup[q] = sx_row_index(upr, x, width, b, e, coff, x < ie);
+        }
+    }
+    T wdn[SX_CHUNK_SUB], wup[SX_CHUNK_SUB], udn[SX_CHUNK_SUB], uup[SX_CHUNK_SUB];
+#pragma unroll
+    for (int q = 0; q < SX_CHUNK_SUB; ++q) {
+        udn[q] = idn[q] >= 0 ? u[idn[q]] : (T)0;
+        uup[q] = iup[q] >= 0 ? u[iup[q]] : (T)0;
+        wdn[q] = idn[q] >= 0 && rdom ? w[idn[q]] : (T)0;
+        wup[q] = iup[q] >= 0 && rdom ? w[iup[q]] : (T)0;
+    }
+    T wprev = (T)0, uprev = (T)0;
+#pragma unroll
+    for (int q = 0; q < SX_CHUNK_SUB; ++q) {
+        const int x = x0 + 32 * q + lane;
+        const bool act = x < ie;
+        const long long c = c0 + 32 * q + lane;
+        const bool jdom = !EDGE || (x >= 0 && x < width && row >= 0 && row < height);
+        T wl = __shfl_up_sync(0xFFFFFFFFu, wc[q], 1), ul = __shfl_up_sync(0xFFFFFFFFu, uc[q], 1);
+        if (lane == 0) {
+            wl = wprev;
+            ul = uprev;
+        }
+        T wr = __shfl_down_sync(0xFFFFFFFFu, wc[q], 1), ur = __shfl_down_sync(0xFFFFFFFFu, uc[q], 1);
+        const int qn = q + 1 < SX_CHUNK_SUB ? q + 1 : q;
+        const T wn = __shfl_sync(0xFFFFFFFFu, wc[qn], 0), un = __shfl_sync(0xFFFFFFFFu, uc[qn], 0);
+        if (lane == 31) {
+            wr = wn;
+            ur = un;
+        }
+        wprev = __shfl_sync(0xFFFFFFFFu, wc[q], 31);
+        uprev = __shfl_sync(0xFFFFFFFFu, uc[q], 31);
+        const bool first = lane == 0 && q == 0, last = lane == 31 && q + 1 == SX_CHUNK_SUB;
+        // in-set values of w left and right (the transpose checks only this cell's domain)
+        T w_left, w_right, u_left, u_right;
+        if (x - 1 >= ib) {
+            w_left = first ? w[c - 1] : wl;
+            const T uv = first ? u[c - 1] : ul;
+            u_left = (!EDGE || (x - 1 >= 0 && x - 1 < width)) ? uv : (T)0;
+        } else {
+            const bool t = act && (touch & 1);
+            w_left = t ? w[c - 1] : (T)0;
+            u_left = (t && (!EDGE || (x - 1 >= 0 && x - 1 < width))) ? u[c - 1] : (T)0;
+        }
+        if (x + 1 < ie) {
+            w_right = last ? w[c + 1] : wr;
+            const T uv = last ? u[c + 1] : ur;
+            u_right = (!EDGE || (x + 1 >= 0 && x + 1 < width)) ? uv : (T)0;
+        } else {
+            const bool t = act && (touch & 2);
+            w_right = t ? w[c + 1] : (T)0;
+            u_right = (t && (!EDGE || (x + 1 >= 0 && x + 1 < width))) ? u[c + 1] : (T)0;
+        }
+        // rows above and below: w in-set needs jdom only (x is then inside the domain, so the
+        // reader's domain test is the same), u needs the forward's domain test
+        const T w_dn = wdn[q], w_up = wup[q], u_dn = udn[q], u_up = uup[q];
+        if (act) {
+            const T c_w = wc[q];
+            T tx, ty;
+            if (a >= (T)0) tx = sx_over(sx_sub(c_w, jdom ? w_right : (T)0), dx, pow2);
+            else tx = sx_over(sx_sub(jdom ? w_left : (T)0, c_w), dx, pow2);
+            if (bb >= (T)0) ty = sx_over(sx_sub(c_w, w_up), dy, pow2);
+            else ty = sx_over(sx_sub(w_dn, c_w), dy, pow2);
+            ubar[c] = sx_sub(c_w, sx_mul(dt, sx_add(sx_mul(a, tx), sx_mul(bb, ty))));
+            const T c_u = uc[q];
+            const T dux = a >= (T)0 ? sx_over(sx_sub(c_u, u_left), dx, pow2) : sx_over(sx_sub(u_right, c_u), dx, pow2);
+            const T duy = bb >= (T)0 ? sx_over(sx_sub(c_u, u_dn), dy, pow2) : sx_over(sx_sub(u_up, c_u), dy, pow2);
+            ga -= (double)dt * (double)c_w * (double)dux;
+            gb -= (double)dt * (double)c_w * (double)duy;
+        }
+    }
+}
+
 template <typename T, bool TABLE>
-__global__ void __launch_bounds__(256, SX_UPWIND_ADJOINT_MIN_BLOCKS) sx_upwind_adjoint_chunk_kernel(const int* __restrict__ off,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? SX_UPWIND_ADJOINT_MIN_BLOCKS : 2) sx_upwind_adjoint_chunk_kernel(const int* __restrict__ off,
                                                                       const int* __restrict__ b,
                                                                       const int* __restrict__ e,
                                                                       const int* __restrict__ coff,
@@ -1031,108 +1149,14 @@ __global__ void __launch_bounds__(256, SX_UPWIND_ADJOINT_MIN_BLOCKS) sx_upwind_a
     for (long long q0 = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); q0 < chunks; q0 += warps) {
         const int4* pl = (const int4*)(info + (long long)SX_PLAN_INTS * q0);
         const int4 p0 = __ldg(pl), p1 = __ldg(pl + 1), p2 = __ldg(pl + 2), p3 = __ldg(pl + 3);
-        const int x0 = p0.x, ie = p0.y, touch = p0.w, row = p3.z, ib = p3.w;
-        const long long c0 = p0.z;
-        T wc[SX_CHUNK_SUB], uc[SX_CHUNK_SUB];
-#pragma unroll
-        for (int q = 0; q < SX_CHUNK_SUB; ++q) {
-            const bool act = x0 + 32 * q + lane < ie;
-            wc[q] = act ? w[c0 + 32 * q + lane] : (T)0;
-            uc[q] = act ? u[c0 + 32 * q + lane] : (T)0;
-        }
-        SxRowReader dn{p1.x, p1.y, p1.z, p1.w, p2.x};
-        SxRowReader upr{p2.y, p2.z, p2.w, p3.x, p3.y};
-        // neighbour-row value indices of all four sub-rounds first, then all
-        // their loads at once.  u reads need the forward's domain test (made by
-        // the index), w reads need this cell's domain as well (jdom).
-        const bool rdom = row >= 0 && row < height;
-        int idn[SX_CHUNK_SUB], iup[SX_CHUNK_SUB];
-        if (TABLE) {  // the plan's neighbour table, as in the forward step
-            const int bdn = sx_chunk_base(dn, x0), bup = sx_chunk_base(upr, x0);
-#pragma unroll
-            for (int q = 0; q < SX_CHUNK_SUB; ++q) {
-                const int x = x0 + 32 * q + lane;
-                const unsigned nb = x < ie ? (unsigned)__ldg(nbr + c0 + 32 * q + lane) : 0xFFFFu;
-                const bool xin = x >= 0 && x < width;
-                idn[q] = (xin && (nb & 0xFFu) != 0xFFu) ? bdn + (int)(nb & 0xFFu) : -1;
-                iup[q] = (xin && (nb >> 8) != 0xFFu) ? bup + (int)(nb >> 8) : -1;
-            }
-        } else {
-#pragma unroll
-            for (int q = 0; q < SX_CHUNK_SUB; ++q) {
-                const int x = x0 + 32 * q + lane;
-                idn[q] = sx_row_index(dn, x, width, b, e, coff, x < ie);
-                iup[q] = sx_row_index(upr, x, width, b, e, coff, x < ie);
-            }
-        }
-        T wdn[SX_CHUNK_SUB], wup[SX_CHUNK_SUB], udn[SX_CHUNK_SUB], uup[SX_CHUNK_SUB];
-#pragma unroll
-        for (int q = 0; q < SX_CHUNK_SUB; ++q) {
-            udn[q] = idn[q] >= 0 ? u[idn[q]] : (T)0;
-            uup[q] = iup[q] >= 0 ? u[iup[q]] : (T)0;
-            wdn[q] = idn[q] >= 0 && rdom ? w[idn[q]] : (T)0;
-            wup[q] = iup[q] >= 0 && rdom ? w[iup[q]] : (T)0;
-        }
-        T wprev = (T)0, uprev = (T)0;
-#pragma unroll
-        for (int q = 0; q < SX_CHUNK_SUB; ++q) {
-            const int x = x0 + 32 * q + lane;
-            const bool act = x < ie;
-            const long long c = c0 + 32 * q + lane;
-            const bool jdom = x >= 0 && x < width && row >= 0 && row < height;
-            T wl = __shfl_up_sync(0xFFFFFFFFu, wc[q], 1), ul = __shfl_up_sync(0xFFFFFFFFu, uc[q], 1);
-            if (lane == 0) {
-                wl = wprev;
-                ul = uprev;
-            }
-            T wr = __shfl_down_sync(0xFFFFFFFFu, wc[q], 1), ur = __shfl_down_sync(0xFFFFFFFFu, uc[q], 1);
-            const int qn = q + 1 < SX_CHUNK_SUB ? q + 1 : q;
-            const T wn = __shfl_sync(0xFFFFFFFFu, wc[qn], 0), un = __shfl_sync(0xFFFFFFFFu, uc[qn], 0);
-            if (lane == 31) {
-                wr = wn;
-                ur = un;
-            }
-            wprev = __shfl_sync(0xFFFFFFFFu, wc[q], 31);
-            uprev = __shfl_sync(0xFFFFFFFFu, uc[q], 31);
-            const bool first = lane == 0 && q == 0, last = lane == 31 && q + 1 == SX_CHUNK_SUB;
-            // in-set values of w left and right (the transpose checks only this cell's domain)
-            T w_left, w_right, u_left, u_right;
-            if (x - 1 >= ib) {
-                w_left = first ? w[c - 1] : wl;
-                const T uv = first ? u[c - 1] : ul;
-                u_left = (x - 1 >= 0 && x - 1 < width) ? uv : (T)0;
-            } else {
-                const bool t = act && (touch & 1);
-                w_left = t ? w[c - 1] : (T)0;
-                u_left = (t && x - 1 >= 0 && x - 1 < width) ? u[c - 1] : (T)0;
-            }
-            if (x + 1 < ie) {
-                w_right = last ? w[c + 1] : wr;
-                const T uv = last ? u[c + 1] : ur;
-                u_right = (x + 1 >= 0 && x + 1 < width) ? uv : (T)0;
-            } else {
-                const bool t = act && (touch & 2);
-                w_right = t ? w[c + 1] : (T)0;
-                u_right = (t && x + 1 >= 0 && x + 1 < width) ? u[c + 1] : (T)0;
-            }
-            // rows above and below: w in-set needs jdom only (x is then inside the domain, so the
-            // reader's domain test is the same), u needs the forward's domain test
-            const T w_dn = wdn[q], w_up = wup[q], u_dn = udn[q], u_up = uup[q];
-            if (act) {
-                const T c_w = wc[q];
-                T tx, ty;
-                if (a >= (T)0) tx = sx_over(sx_sub(c_w, jdom ? w_right : (T)0), dx, pow2);
-                else tx = sx_over(sx_sub(jdom ? w_left : (T)0, c_w), dx, pow2);
-                if (bb >= (T)0) ty = sx_over(sx_sub(c_w, w_up), dy, pow2);
-                else ty = sx_over(sx_sub(w_dn, c_w), dy, pow2);
-                ubar[c] = sx_sub(c_w, sx_mul(dt, sx_add(sx_mul(a, tx), sx_mul(bb, ty))));
-                const T c_u = uc[q];
-                const T dux = a >= (T)0 ? sx_over(sx_sub(c_u, u_left), dx, pow2) : sx_over(sx_sub(u_right, c_u), dx, pow2);
-                const T duy = bb >= (T)0 ? sx_over(sx_sub(c_u, u_dn), dy, pow2) : sx_over(sx_sub(u_up, c_u), dy, pow2);
-                ga -= (double)dt * (double)c_w * (double)dux;
-                gb -= (double)dt * (double)c_w * (double)duy;
-            }
-        }
+        const int x0 = p0.x, ie = p0.y, row = p3.z;
+        const bool edge = !(row >= 0 && row < height && x0 >= 1 && x0 + min(ie - x0, SX_CHUNK) < width);
+        if (edge)
+            sx_chunk_adjoint<T, TABLE, true>(p0, p1, p2, p3, lane, b, e, coff, nbr, w, u, ubar, width, height, a, bb,
+                                             dt, dx, dy, pow2, ga, gb);
+        else
+            sx_chunk_adjoint<T, TABLE, false>(p0, p1, p2, p3, lane, b, e, coff, nbr, w, u, ubar, width, height, a, bb,
+                                              dt, dx, dy, pow2, ga, gb);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
