@@ -818,7 +818,7 @@ def main():
     if parity is not None:
         line["parity"] = parity
     line["reference_gpu"] = reference_gpu_section(device, dev, n_in)
-    if not args.no_amr:
+    if not args.no_amr and world == 1:  # one-GPU sections; a multi-GPU run measures the sharded headline only
         line["amr_step"] = amr_section(device)
         line["amr_step_refined"] = amr_section(device, threshold=0.05 / 1024)
         line["adjoint"] = adjoint_section(device)
