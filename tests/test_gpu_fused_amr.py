@@ -213,3 +213,32 @@ def test_batched_upwind_per_set_spacing_and_graph_step(cuda_device):
                       (step.intersection(), batched_binary(A, B, "intersection"))):
         for x, y in zip(mine.split(), ref.split()):
             assert_same(x, tuple(t.cpu().numpy() for t in (y.begin, y.end, y.row_offsets, y.rows)))
+
+
+def test_batched_upwind_at_full_size_equals_per_set_calls(cuda_device):
+    """The banded batch step on the benchmark's 256 uneven sets (238 M cells, dx = 1/side and a CFL time step per
+    set) equals every set's own step_upwind_interval call bit for bit; that per-set path is the one checked against
+    the oracle and the reference's kernels at smaller sizes."""
+    from subsetix_b200 import synth
+    from subsetix_b200.batch import SetBatch, batched_upwind
+    from subsetix_b200.subsetix_cupy import create_interval_field, step_upwind_interval
+    from subsetix_b200.subsetix_cupy.expressions import IntervalSet
+
+    dev = torch.device("cuda", 0)
+    sides, hosts = synth.batched_uneven_sets(count=256, seed=3)
+    A = SetBatch.from_sets([IntervalSet._trusted(*(torch.as_tensor(x, device=dev) for x in h)) for h in hosts], sides)
+    n = A.stencil_plan().cells
+    assert n > 200_000_000
+    vals = torch.rand(n, device=dev, generator=torch.Generator(device=dev).manual_seed(5))
+    dx = [1.0 / s for s in sides]
+    dt = [0.5 / (1.5 / h) for h in dx]
+    got = batched_upwind(A, vals, width=sides, a=1.0, b=0.5, dt=dt, dx=dx, dy=dx)
+    pos = 0
+    for s, side, h, t in zip(A.split(), sides, dx, dt):
+        f = create_interval_field(s, fill_value=0.0, dtype=np.float32)
+        cells = int(f.values.numel())
+        f.values.copy_(vals[pos:pos + cells])
+        want = step_upwind_interval(f, width=side, height=side, a=1.0, b=0.5, dt=t, dx=h, dy=h)
+        assert torch.equal(got[pos:pos + cells], want), side
+        pos += cells
+    assert pos == n
