@@ -242,3 +242,20 @@ def test_batched_upwind_at_full_size_equals_per_set_calls(cuda_device):
         assert torch.equal(got[pos:pos + cells], want), side
         pos += cells
     assert pos == n
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+def test_fused_step_at_full_size_equals_separate_kernels(cuda_device, dtype):
+    """The benchmark's 1024^2 run with the physical threshold (part of the grid refined): the one-kernel step,
+    which updates fine blocks only under refined cells, equals the separate upwind and synchronisation kernels."""
+    res = 1024
+    u0 = torch.as_tensor(_gauss(res, 0.05), device="cuda")
+    runs = []
+    for fused in (True, False):
+        eng = FusedTwoLevelAMR(u0, velocity=(1.0, 0.5), cfl=0.5, refine_threshold=0.05 / res, grading=1, dtype=dtype,
+                               fused=fused)
+        eng.run(30, regrid_every=10)
+        runs.append(eng)
+    assert bool((runs[0].actions != 0).any())
+    for lvl in ("coarse_values", "fine_values"):
+        assert torch.equal(getattr(runs[0], lvl), getattr(runs[1], lvl)), lvl
