@@ -364,3 +364,24 @@ def test_composite_graph_replays_equal_eager_launches(cuda_device):
         assert torch.equal(results[0][1], other[1])
         for x, y in zip(results[0][2], other[2]):
             assert torch.equal(x, y)
+
+
+def test_composite_transpose_identity_at_full_size(cuda_device):
+    """<A v, w> = <v, A^T w> in FP64 on the benchmark's three levels (2048^2 base, disks at x2 and x4, 13.7 M cells);
+    the two sums are compared relative to the sum of the absolute products, the scale of their rounding."""
+    base = 2048
+    hosts = synth.nested_disk_levels(base, [0.3, 0.15])
+    H = adj.Hierarchy([dev_set(h) for h in hosts], base, base)
+    assert sum(H.inner_cells) > 10_000_000
+    g0 = torch.Generator(device="cuda").manual_seed(9)
+    v = [torch.randn(n, device="cuda", dtype=torch.float64, generator=g0) for n in H.inner_cells]
+    w = [torch.randn(n, device="cuda", dtype=torch.float64, generator=g0) for n in H.inner_cells]
+    a, b, dt = 0.8, -0.45, 0.5 / (1.5 * base * 4)
+    new, inputs = H.step(H.extend(v), a, b, dt)
+    mv = H.interior(new)
+    g = torch.zeros(2, dtype=torch.float64, device="cuda")
+    mtw = H.interior(H.step_adjoint(H.extend(w), inputs, a, b, dt, g))
+    lhs = sum(float(torch.dot(x, y)) for x, y in zip(mv, w))
+    rhs = sum(float(torch.dot(x, y)) for x, y in zip(v, mtw))
+    scale = sum(float(torch.sum(torch.abs(x * y))) for x, y in zip(mv, w))
+    assert abs(lhs - rhs) <= 1e-11 * scale, (lhs, rhs, scale)
