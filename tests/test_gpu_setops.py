@@ -366,3 +366,18 @@ def test_lookback_wait_gives_up_and_reports_timeout(cuda_device):
         _core.TUNING.update(saved)
     got = sc.evaluate(sc.make_union(sc.make_input(la), sc.make_input(lb)))
     assert_same(got, O.union(iset(A), iset(B)))
+
+
+def test_headline_expression_at_full_size_against_oracle(cuda_device):
+    """((A|B)-(C&D))^E on the 4096^2 shapes stacked 128 times (37.9 M input intervals, the benchmark's batch)
+    through the public evaluate(), equal to the oracle bit for bit."""
+    import bench
+
+    leaves = bench.workload(128)
+    O, oleaves = bench._oracle_leaves(leaves)
+    want = O.evaluate(bench.SPEC, oleaves)
+    A, B, C, D, F = [sc.make_input(dev_set(h)) for h in leaves]
+    got = sc.evaluate(sc.make_symmetric_difference(sc.make_difference(sc.make_union(A, B), sc.make_intersection(C, D)),
+                                                   F))
+    assert int(got.begin.shape[0]) > 20_000_000
+    assert_same(got, tuple(want[:4]), "headline expression")
