@@ -162,7 +162,15 @@ def peak_hbm():
 
 # sx_tuning kernel kinds (0 = automatic, the warp-tile segmented sweep)
 KERNELS = {1: "sx_sweep_kernel<5,0>", 2: "sx_sweep_smem_kernel<5>", 3: "sx_merge_kernel<5>", 4: "sx_seg_kernel<5>",
-           5: "sx_wseg_kernel<5>", 6: "sx_wseg16_kernel<5>"}
+           5: "sx_wseg_kernel<5>", 6: "sx_wseg16_kernel<5>", 7: "sx_rlane16_kernel<5,2>"}
+
+
+def kernel_name(tuning: dict) -> str:
+    """Name of the launched kernel instance (the row-lane sweep's second parameter is lanes per row)."""
+    kind = int(tuning.get("kernel", 0)) or 5
+    if kind == 7:
+        return f"sx_rlane16_kernel<5,{32 // (int(tuning.get('tile_rows', 0)) or 16)}>"
+    return KERNELS[kind]
 
 
 def traffic_per_launch(copies: int, kernel: str):
@@ -787,7 +795,7 @@ def main():
     e2e_value = world * n_in / (e2e_ms / 1e3) / 1e9
 
     kernel_ms = statistics.mean(per_step)
-    kname = KERNELS[int(tuning.get("kernel", 0)) or 5]
+    kname = kernel_name(tuning)
     peak, peak_kind = peak_hbm()
     achieved = algo / (kernel_ms / 1e3) / 1e9
     traffic, traffic_src = traffic_per_launch(args.copies, kname)

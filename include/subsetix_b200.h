@@ -94,14 +94,17 @@ typedef struct sx_leaf {
  * kernel: 1 = global-memory sweep, 2 = shared-memory staged sweep, 3 =
  * merge-path tile kernel, 4 = segmented sweep in block tiles, 5 = segmented
  * sweep in warp tiles (table mode; the default), 6 = kernel 5 with 16-bit
- * keys (tiles of at most 8 rows; wider-spanning tiles take the row sweep);
+ * keys (tiles of at most 8 rows; wider-spanning tiles take the row sweep),
+ * 7 = row-lane sweep (a warp per 32-row tile, a lane per row, 16-bit
+ * coordinates in shared memory; tiles spanning more than 65534 columns take
+ * the row sweep over global memory);
  * blocks_per_sm: residency cap of the global sweep; staging_cap: elements per
- * warp of the staged sweep, or boundaries per tile of kernels 3 to 6; warps:
- * warps per block of kernels 4 to 6 (in 5 and 6 each warp owns a tile);
- * tile_rows: rows per tile of kernels 4 to 6 (at most 32, at most 8 for 6).
- * Results never depend on the tuning.
+ * warp of the staged sweep, or boundaries per tile of kernels 3 to 7; warps:
+ * warps per block of kernels 4 to 7 (in 5 to 7 each warp owns a tile);
+ * tile_rows: rows per tile of kernels 4 to 6 (at most 32, at most 8 for 6;
+ * kernel 7 takes 0 or 32).  Results never depend on the tuning.
  * Two fields exist for tests of the failure path and are zero otherwise:
- * wait_limit caps the polls of every look-back wait of kernels 4 to 6 (0 =
+ * wait_limit caps the polls of every look-back wait of kernels 4 to 7 (0 =
  * the built-in limit of 2^22 polls); withhold_tile = t + 1 makes tile t of
  * those kernels never publish its look-back status, so the tiles after it
  * wait until the limit, give up and report SX_FLAG_TIMEOUT (their outputs

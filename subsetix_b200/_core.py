@@ -81,19 +81,22 @@ def _default_keys(leaves, rows: int, tile_rows: int = 32) -> int:
 
 
 def auto_tuning(leaves, rows: int, device) -> dict:
-    """The automatic launch shape of a truth-table sweep (one launch and one read-back).
+    """The automatic launch shape of a truth-table sweep (one launch and one read-back, two when rows are skewed).
 
-    Even rows: 8-row warp tiles with buffers sized for the largest tile (no
-    tile leaves the staged sweep, no buffer larger than needed).  Skewed rows
-    (the largest 8-row tile far above the mean): 32-row block tiles sized for
-    their largest tile, which evens out the load.  Tiles spanning at most
-    8190 columns take 16-bit keys (half the shared memory per tile, twice the
-    tiles in flight).
+    Even rows (the largest 8-row tile within 3x the mean plus 256
+    boundaries): the row-lane sweep on 16-row tiles, two lanes per row, when
+    every such tile spans at most 65534 columns (16-bit coordinates), else
+    8-row warp tiles with 32-bit keys; buffers are sized for the largest tile,
+    so no tile leaves the staged sweep.  Skewed rows: 32-row block tiles
+    sized for their largest tile, which evens out the load.
     """
-    need8, need32, span8 = tile_stats(leaves, rows, device, 8, 32)
+    need16, need8, span16 = tile_stats(leaves, rows, device, 16, 8)
     mean8 = 2 * sum(int(leaf[0].numel()) for leaf in leaves) / max(1, (rows + 7) // 8)
     if need8 <= 3 * mean8 + 256:
-        return {"kernel": 6 if span8 <= 8190 else 5, "staging_cap": min(need8, 25000), "tile_rows": 8, "warps": 2}
+        if span16 <= 65534:
+            return {"kernel": 7, "staging_cap": min(need16, 25000), "tile_rows": 16, "warps": 4}
+        return {"kernel": 5, "staging_cap": min(need8, 25000), "tile_rows": 8, "warps": 2}
+    need32 = max_tile_boundaries(leaves, rows, device, tile_rows=32)
     return {"kernel": 4, "staging_cap": min(need32, 25000), "tile_rows": 32, "warps": 4}
 
 
@@ -112,8 +115,8 @@ def bool_eval(leaves: Sequence[Tuple[torch.Tensor, torch.Tensor, torch.Tensor, i
     tuned = TUNED.get(workload_key([int(leaf[0].numel()) for leaf in leaves], rows)) if TUNED else None
     if mode == _lib.MODE_TABLE and not TUNING and rows > 0 and tuned is not None:
         tuning = dict(tuned)
-        if tuning.get("kernel") in (3, 4, 5, 6):
-            tr = int(tuning.get("tile_rows", 0)) or (8 if tuning["kernel"] >= 5 else 32)
+        if tuning.get("kernel") in (3, 4, 5, 6, 7):
+            tr = int(tuning.get("tile_rows", 0)) or {5: 8, 6: 8, 7: 16}.get(tuning["kernel"], 32)
             tuning["staging_cap"] = min(max_tile_boundaries(leaves, rows, device, tile_rows=tr), 25000)
     elif mode == _lib.MODE_TABLE and not TUNING and rows > 0:
         tuning = auto_tuning(leaves, rows, device)

@@ -1,6 +1,7 @@
 """Launch autotuner for the row-sweep set algebra (sx_bool_eval).
 
-The candidates are the kernel kinds of ``sx_tuning``: the warp-tile
+The candidates are the kernel kinds of ``sx_tuning``: the row-lane sweep
+(16-row tiles with two lanes per row, 32-row tiles with one), the warp-tile
 segmented sweep (8-row tiles, 32-bit and 16-bit keys) with several warps
 per block, the block-tile
 segmented sweep (32-row tiles) with two block sizes, the merge-path tile
@@ -31,16 +32,24 @@ _CACHE: Dict[str, dict] = {}
 workload_key = _core.workload_key
 
 
-def candidates(sizes: Sequence[int], rows: int, largest_tile: int = 0, largest_eighth_tile: int = 0) -> List[dict]:
+def candidates(sizes: Sequence[int], rows: int, largest_tile: int = 0, largest_eighth_tile: int = 0,
+               largest_half_tile: int = 0) -> List[dict]:
     tiles = max(1, (int(rows) + 31) // 32)
     avg = 2 * sum(int(s) for s in sizes) / tiles
     out = []
-    cap8 = min(max(int(avg / 4 * 1.25 + 64), int(largest_eighth_tile)), 25000)
+    # buffers for the largest tile when it is known (every tile then stays staged, and no slice is larger than
+    # needed), else 1.25x the mean tile
+    cap16 = min(int(largest_half_tile) or int(avg / 2 * 1.25 + 64), 25000)
+    for w in (1, 4):
+        out.append({"kernel": 7, "staging_cap": cap16, "warps": w, "tile_rows": 16})
+    out.append({"kernel": 7, "staging_cap": min(int(largest_tile) or int(avg * 1.25 + 64), 25000), "warps": 1,
+                "tile_rows": 32})
+    cap8 = min(int(largest_eighth_tile) or int(avg / 4 * 1.25 + 64), 25000)
     for w in (2, 4, 8):
         out.append({"kernel": 5, "staging_cap": cap8, "warps": w, "tile_rows": 8})
     for w in (2, 4, 8):
         out.append({"kernel": 6, "staging_cap": cap8, "warps": w, "tile_rows": 8})
-    cap = min(max(int(avg * 1.25 + 256), int(largest_tile)), 25000)
+    cap = min(int(largest_tile) or int(avg * 1.25 + 256), 25000)
     for w in (4, 8):
         out.append({"kernel": 4, "staging_cap": cap, "warps": w, "tile_rows": 32})
     for f in (1.25, 2.0):
@@ -66,9 +75,9 @@ def tune_bool_eval(leaves, rows: int, table: Sequence[int], device, *, mode: int
         stream = torch.cuda.current_stream(device)
         timings = []
         table_mode = mode == _lib.MODE_TABLE
-        largest = _core.max_tile_boundaries(leaves, rows, device) if table_mode else 0
-        eighth = _core.max_tile_boundaries(leaves, rows, device, tile_rows=8) if table_mode else 0
-        for cand in candidates(sizes, rows, largest, eighth):
+        largest, eighth = _core.max_tile_boundaries(leaves, rows, device, tile_rows=(32, 8)) if table_mode else (0, 0)
+        half = _core.max_tile_boundaries(leaves, rows, device, tile_rows=16) if table_mode else 0
+        for cand in candidates(sizes, rows, largest, eighth, half):
             def launch():
                 _core.bool_eval_async(leaves, rows, table, mode, device, out=(ob, oe), result=res, offsets=off,
                                       tuning=cand)

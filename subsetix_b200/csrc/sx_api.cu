@@ -97,7 +97,7 @@ int sx_bool_eval(const sx_leaf* leaves, int k, int32_t rows, const uint32_t* tab
     A.capacity = capacity;
     A.result = result;
     if (tuning) {
-        if (tuning->kernel < 0 || tuning->kernel > 6 || tuning->blocks_per_sm < 0 || tuning->staging_cap < 0 ||
+        if (tuning->kernel < 0 || tuning->kernel > 7 || tuning->blocks_per_sm < 0 || tuning->staging_cap < 0 ||
             tuning->warps < 0 || tuning->warps > 8 ||
             tuning->tile_rows < 0 || tuning->tile_rows > 32 || tuning->wait_limit < 0 || tuning->withhold_tile < 0)
             return fail(SX_ERR_INVALID, "sx_bool_eval: bad tuning");
@@ -108,6 +108,10 @@ int sx_bool_eval(const sx_leaf* leaves, int k, int32_t rows, const uint32_t* tab
         A.tune_staging_cap = tuning->staging_cap;
         A.tune_warps = tuning->warps;
         A.tune_tile_rows = tuning->tile_rows;
+        if (tuning->kernel == 7 && tuning->tile_rows != 0 && tuning->tile_rows != 8 && tuning->tile_rows != 16 &&
+            tuning->tile_rows != 32)
+            return fail(SX_ERR_INVALID, "sx_bool_eval: bad tuning: kernel 7 sweeps tiles of 8, 16 or 32 rows, got tile_rows=%d",
+                        tuning->tile_rows);
     }
     if (mode == SX_MODE_TABLE && A.tune_tile_rows > 0 && (A.tune_kernel == 0 || A.tune_kernel >= 4)) {
         // an explicit tile height is honoured exactly or refused, never changed behind the caller's back

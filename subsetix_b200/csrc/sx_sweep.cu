@@ -2295,6 +2295,375 @@ __global__ void __launch_bounds__(256, K <= 5 ? 5 : 4) sx_wseg16_kernel(SxBoolAr
     sxs_report(A, tile, tiles, base, total >> 1, flags);
 }
 
+// ---------------------------------------------------------------------------
+// Row-lane sweep with 16-bit coordinates (sx_tuning kernel 7).
+//
+// A warp owns a tile of 32 aligned rows and lane r sweeps row r, so a step
+// needs no combined (row, x) keys, no piece search and no search for the
+// row offsets of the output.
+//
+// Staging.  One bulk copy per leaf array (begins, ends) into the warp's
+// slice of shared memory, above a gap; then interval j of leaf l becomes the
+// word (b - xmin) | (e - xmin) << 16 in leaf l's pair list, which holds one
+// spare word after every non-empty row: word j of row q-th non-empty row
+// goes to j + q.  The spare word holds 0xFFFF in its low half, so a lane's
+// walk (b0 e0 b1 e1 ... as halfwords) stops at its row's end with no
+// per-step limit test, and rows whose lengths are multiples of 32 words
+// (a 64-pixel checkerboard on 4096 columns) no longer put every lane of a
+// step on the same shared-memory bank.  The pair lists grow into the gap
+// while the raw copies above are read: a pair is written at most 31 + 25 l
+// words above its own raw begin's distance from the slice start, below every
+// raw word not yet read.  xmin is the tile's smallest first begin and xmax
+// its largest last end; a tile with xmax - xmin > 65534 takes the
+// global-memory sweep, and a coordinate outside [xmin, xmin + 65534] in a
+// narrower tile breaks the contract (on canonical rows every coordinate lies
+// between its row's first begin and last end).
+//
+// Step: the smallest head c; each leaf whose head equals c toggles its state
+// bit and loads its next halfword (predicated, no divergence); f(state) from
+// the truth table; a change of f stores c.  On canonical rows successive c
+// rise strictly, so one compare per step checks the contract (non-empty,
+// sorted, non-touching intervals).  Row r's output halfwords go to an area
+// as large as its input plus one word (the dead raw copies).  A scan of the
+// per-row counts gives the row offsets, the look-back the tile's base; the
+// lanes pack their output words over the dead pair lists and the warp writes
+// them out coalesced.  Every wait is bounded.
+// ---------------------------------------------------------------------------
+#define SXR_TR 32
+#define SXR_SPAN 65534
+#define SXR_SENTINEL 0xFFFFu
+#define SXR_HDR_WORDS 4
+
+// Words below the raw copies into which the padded pair lists grow.
+__host__ __device__ inline int sxr_gap_words(int k) { return (33 * k + 35) & ~3; }
+
+__host__ __device__ inline size_t sxr_slice_bytes(int cap_words)
+{
+    return 4u * (size_t)(SXR_HDR_WORDS + ((cap_words + 3) & ~3));
+}
+
+// One leaf of a row-lane step: when the head h equals the step's key c, load
+// the next halfword from pa + 2 (the load does not wait for the address
+// update), advance pa and toggle the leaf's state bit.  Predicated.
+__device__ __forceinline__ void sxr_advance16(unsigned& h, unsigned& pa, unsigned& state, unsigned c, unsigned bit)
+{
+    asm volatile(
+        "{\n .reg .pred q;\n setp.eq.u32 q, %0, %3;\n @q ld.shared.u16 %0, [%1+2];\n @q add.u32 %1, %1, 2;\n"
+        " @q xor.b32 %2, %2, %4;\n}\n"
+        : "+r"(h), "+r"(pa), "+r"(state)
+        : "r"(c), "r"(bit));
+}
+
+template <int K>
+__device__ __forceinline__ unsigned sxr_min_head(const unsigned* h)
+{
+    unsigned c = h[0];
+    int l = 1;
+#pragma unroll
+    for (; l + 1 < K; l += 2) c = __vimin3_u32(c, h[l], h[l + 1]);
+#pragma unroll
+    for (; l < K; ++l) c = min(c, h[l]);
+    return c;
+}
+
+// A tile of 32 / LPR rows: lanes LPR r .. LPR r + LPR - 1 sweep row r in
+// pieces [p_i, p_{i+1}) of its keys, the pivots p_i being halfwords of the
+// row's longest leaf at positions i m / LPR (m its boundaries).  A piece
+// starts in every other leaf at the first key not below p_i (a binary search
+// within the row) with the parity of that position as the leaf's state bit,
+// and writes at most as many outputs as it reads inputs, so piece i's output
+// area starts where the inputs of the pieces before it end.  Consecutive
+// pieces must meet: each piece's end positions are checked against the next
+// piece's start positions (with the per-piece rising keys, that checks the
+// contract across pieces).
+template <int K, int LPR>
+__global__ void __launch_bounds__(256) sx_rlane16_kernel(SxBoolArgs A, SxSweepState st, int tiles, int cap_words)
+{
+    extern __shared__ __align__(16) unsigned char sxr_smem[];
+    constexpr int TR = SXR_TR / LPR;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, NW = blockDim.x >> 5;
+    if (blockIdx.x * NW + wid >= tiles) return;  // exactly `tiles` warps take tickets
+    unsigned* base_w = (unsigned*)(sxr_smem + (size_t)wid * sxr_slice_bytes(cap_words));
+    unsigned long long* bar = (unsigned long long*)base_w;
+    unsigned* const W = base_w + SXR_HDR_WORDS;  // pair lists, then the output areas
+    unsigned short* const h16 = (unsigned short*)W;
+    const int gap = sxr_gap_words(K);
+    unsigned* const raw = W + gap;  // the bulk copies
+    const int row = lane / LPR, piece = lane % LPR;
+    const int first_lane = row * LPR;
+
+    int tile = 0;
+    if (lane == 0) {
+        tile = (int)atomicAdd(&st.counters[0], 1u);
+        sxs_bar_init(bar);
+    }
+    tile = __shfl_sync(0xFFFFFFFFu, tile, 0);
+    const int r0 = tile * TR;
+    const int nrows = min(TR, A.rows - r0);
+    const bool act = row < nrows;
+    // this lane's row in every leaf, relative to the tile's first interval
+    int lo[K], hi[K], n[K], g0[K];
+    bool ok = true;
+    long long RBl = 0, PBl = 0;
+#pragma unroll
+    for (int l = 0; l < K; ++l) {
+        const int a = A.leaf[l].off[r0 + min(row, nrows)];
+        const int b = A.leaf[l].off[r0 + min(row + 1, nrows)];
+        g0[l] = __shfl_sync(0xFFFFFFFFu, a, 0);
+        n[l] = __shfl_sync(0xFFFFFFFFu, b, (nrows - 1) * LPR) - g0[l];
+        lo[l] = act ? a - g0[l] : n[l];
+        hi[l] = act ? b - g0[l] : n[l];
+        ok = ok && lo[l] >= 0 && lo[l] <= hi[l] && hi[l] <= n[l];
+        RBl += (long long)((n[l] + 11) & ~3);
+        PBl += (long long)n[l] + TR + 1;
+    }
+    ok = __all_sync(0xFFFFFFFFu, ok);  // row offsets must rise through the tile
+    const bool fits = ok && gap + 2 * RBl <= (long long)cap_words;
+    const int OA = (int)PBl;  // output areas start after the pair lists
+    unsigned flags = ok ? 0u : SXF_CONTRACT;
+    // 1. bulk copies: lane q < K copies leaf q's begins, lane K + q its ends
+    int rb[K], re[K];
+#pragma unroll
+    for (int l = 0; l < K; ++l) rb[l] = re[l] = 0;
+    bool copied = true;
+    if (fits) {
+        const int q = lane < 2 * K ? lane : 0;
+        const bool ends = q >= K;
+        const int lq = ends ? q - K : q;
+        int nl = 0, gq = 0;
+        const int* arr = nullptr;
+#pragma unroll
+        for (int m = 0; m < K; ++m)
+            if (m == lq) {
+                nl = n[m];
+                gq = g0[m];
+                arr = ends ? A.leaf[m].end : A.leaf[m].begin;
+            }
+        const int* g = arr + gq;
+        const uintptr_t a0 = (uintptr_t)g & ~(uintptr_t)15;
+        const unsigned len =
+            (lane < 2 * K && nl > 0) ? (unsigned)((((uintptr_t)(g + nl) + 15) & ~(uintptr_t)15) - a0) : 0u;
+        const int region = lane < 2 * K ? ((nl + 11) & ~3) : 0;  // at most n + 6 copied words
+        int incl = region;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int pos = incl - region;
+        int bytes = (int)len;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) bytes += __shfl_xor_sync(0xFFFFFFFFu, bytes, o);
+        const int first = pos + (int)(((uintptr_t)g & 15) >> 2);
+#pragma unroll
+        for (int l = 0; l < K; ++l) {
+            rb[l] = __shfl_sync(0xFFFFFFFFu, first, l);
+            re[l] = __shfl_sync(0xFFFFFFFFu, first, K + l);
+        }
+        __syncwarp();
+        if (lane == 0) sxs_bar_expect(bar, (unsigned)bytes);
+        __syncwarp();
+        if (len > 0u) sxs_bulk_copy(raw + pos, (const void*)a0, len, bar);
+        copied = __all_sync(0xFFFFFFFFu, sxs_bar_wait(bar));
+        if (!copied) flags |= SXF_TIMEOUT;
+    }
+    // 2. the tile's coordinate range: first begin and last end of every row
+    int xmin = INT_MAX, xmax = INT_MIN;
+    if (fits && copied) {
+        if (act && piece == 0) {
+#pragma unroll
+            for (int l = 0; l < K; ++l)
+                if (lo[l] < hi[l]) {
+                    xmin = min(xmin, (int)raw[rb[l] + lo[l]]);
+                    xmax = max(xmax, (int)raw[re[l] + hi[l] - 1]);
+                }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            xmin = min(xmin, __shfl_xor_sync(0xFFFFFFFFu, xmin, o));
+            xmax = max(xmax, __shfl_xor_sync(0xFFFFFFFFu, xmax, o));
+        }
+    }
+    const bool staged = fits && copied && (xmin > xmax || (long long)xmax - (long long)xmin <= SXR_SPAN);
+    bool bad = false;
+    // 3. padded pair lists, leaf by leaf; qr[l] is this row's rank among the leaf's non-empty rows
+    int qr[K], pb[K];
+    {
+        int p = 0;
+        const unsigned below = (1u << first_lane) - 1u;
+#pragma unroll
+        for (int l = 0; l < K; ++l) {
+            const bool ne = act && piece == 0 && lo[l] < hi[l];
+            qr[l] = __popc(__ballot_sync(0xFFFFFFFFu, ne) & below);
+            pb[l] = p;
+            p += n[l] + TR + 1;
+        }
+    }
+    if (staged) {
+#pragma unroll
+        for (int l = 0; l < K; ++l) {
+            const unsigned* src_b = raw + rb[l];
+            const unsigned* src_e = raw + re[l];
+            unsigned* dst = W + pb[l];
+            const bool ne = act && piece == 0 && lo[l] < hi[l];
+            int qbase = 0;  // non-empty rows starting before the chunk
+            for (int j0 = 0; j0 < n[l]; j0 += 32) {
+                const int j = j0 + lane;
+                const unsigned d = (unsigned)(lo[l] - j0);
+                const unsigned starts = __reduce_or_sync(0xFFFFFFFFu, (ne && d < 32u) ? 1u << d : 0u);
+                const int q = qbase + __popc(starts & (0xFFFFFFFFu >> (31 - lane))) - 1;
+                unsigned word = 0u;
+                if (j < n[l]) {
+                    const unsigned ub = src_b[j] - (unsigned)xmin, ue = src_e[j] - (unsigned)xmin;
+                    if (max(ub, ue) > (unsigned)SXR_SPAN) bad = true;
+                    word = __byte_perm(ub, ue, 0x5410);
+                }
+                __syncwarp();  // the chunk's raw words are read before any pair lands on them
+                if (j < n[l]) dst[j + q] = word;
+                qbase += __popc(starts);
+            }
+        }
+    }
+    __syncwarp();
+    if (staged && act && piece == 0) {
+#pragma unroll
+        for (int l = 0; l < K; ++l)  // the row's spare word
+            if (lo[l] < hi[l]) h16[2 * (pb[l] + hi[l] + qr[l])] = (unsigned short)SXR_SENTINEL;
+    }
+    __syncwarp();
+    // this row's output area: as much as its input, plus one word
+    int cap_r = 0;
+#pragma unroll
+    for (int l = 0; l < K; ++l) cap_r += hi[l] - lo[l];
+    int cap_excl = piece == 0 ? cap_r : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xFFFFFFFFu, cap_excl, o);
+        if (lane >= o) cap_excl += y;
+    }
+    cap_excl = cap_excl - (piece == 0 ? cap_r : 0) + row;
+    cap_excl = __shfl_sync(0xFFFFFFFFu, cap_excl, first_lane);
+    int khw = 0, prov = 0;  // output halfwords of this piece; inputs of the row's earlier pieces
+    unsigned sa[K], pa[K], h[K];
+#pragma unroll
+    for (int l = 0; l < K; ++l) sa[l] = pa[l] = h[l] = 0u;
+    if (staged && act) {
+        // 4. this piece's start in every leaf
+        int big = 0, nbig = -1;
+#pragma unroll
+        for (int l = 0; l < K; ++l)
+            if (hi[l] - lo[l] > nbig) {
+                big = l;
+                nbig = hi[l] - lo[l];
+            }
+        const int m = 2 * nbig;
+        int bigw = 0;
+#pragma unroll
+        for (int l = 0; l < K; ++l)
+            if (l == big) bigw = pb[l] + lo[l] + qr[l];
+        const unsigned short* Lb = h16 + 2 * bigw;
+        unsigned klo = 0u, khi = SXR_SENTINEL;
+        if (LPR > 1) {
+            klo = piece == 0 ? 0u : (m > 0 ? (unsigned)Lb[(piece * m) / LPR] : SXR_SENTINEL);
+            khi = piece == LPR - 1 ? SXR_SENTINEL : (m > 0 ? (unsigned)Lb[((piece + 1) * m) / LPR] : SXR_SENTINEL);
+        }
+        unsigned state = 0u;
+#pragma unroll
+        for (int l = 0; l < K; ++l) {
+            const unsigned short* Ll = h16 + 2 * (pb[l] + lo[l] + qr[l]);
+            const int cnt = 2 * (hi[l] - lo[l]);
+            int pos = 0;
+            if (LPR > 1 && piece > 0) pos = l == big ? (piece * m) / LPR : sxs_lower_bound16(Ll, cnt, klo);
+            if (cnt == 0) pos = 0;
+            sa[l] = pa[l] = sxs_saddr(Ll + pos);
+            h[l] = pos < cnt ? (unsigned)Ll[pos] : SXR_SENTINEL;
+            state |= (unsigned)(pos & 1) << l;
+            prov += pos;
+        }
+        // 5. the sweep of this piece
+        const unsigned tab0 = A.table[0];
+        unsigned fprev = K <= 5 ? (tab0 >> state) & 1u : (A.table[state >> 5] >> (state & 31u)) & 1u;
+        int cprev = -1;
+        const unsigned o0 = sxs_saddr(h16 + 2 * (OA + cap_excl) + prov);
+        unsigned oa = o0;
+        unsigned c = sxr_min_head<K>(h);
+        while (c < khi) {
+            bad = bad || (int)c <= cprev;
+            cprev = (int)c;
+#pragma unroll
+            for (int l = 0; l < K; ++l) sxr_advance16(h[l], pa[l], state, c, 1u << l);
+            const unsigned f = K <= 5 ? (tab0 >> state) & 1u : (A.table[state >> 5] >> (state & 31u)) & 1u;
+            sxs_emit16(oa, f, fprev, c);
+            fprev = f;
+            c = sxr_min_head<K>(h);
+        }
+        khw = (int)((oa - o0) >> 1);
+    }
+    if (LPR > 1) {
+        // consecutive pieces of a row meet: this piece ends where the next one starts
+#pragma unroll
+        for (int l = 0; l < K; ++l) {
+            const unsigned nxt = __shfl_down_sync(0xFFFFFFFFu, sa[l], 1);
+            if (staged && act && piece < LPR - 1 && pa[l] != nxt) bad = true;
+        }
+    }
+    if (__any_sync(0xFFFFFFFFu, bad)) {
+        flags |= SXF_CONTRACT;
+        khw = 0;  // pieces may overlap on such input: the tile writes nothing
+    }
+    // fallback tile: one lane per row over global memory
+    int s_row[K], lim_row[K];
+    int nint = 0;
+    if (ok && !staged) {
+#pragma unroll
+        for (int l = 0; l < K; ++l) {
+            s_row[l] = g0[l] + lo[l];
+            lim_row[l] = 2 * (hi[l] - lo[l]);
+        }
+        bool fb_bad = false, fb_over = false;
+        if (act && piece == 0) nint = sx_sweep_table<K, false>(A, s_row, lim_row, nullptr, nullptr, 0, fb_bad, fb_over);
+        if (__any_sync(0xFFFFFFFFu, fb_bad)) flags |= SXF_CONTRACT;
+        khw = 2 * nint;
+    }
+    int incl = khw;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    const int excl = incl - khw;  // halfwords of the pieces before this one
+    const int total = __shfl_sync(0xFFFFFFFFu, incl, 31) >> 1;
+    // 6. look-back, then pack the output halfwords over the dead pair lists
+    const int base = sxs_lookback(A, st, tile, total, flags);
+    bool over = false;
+    if (staged) {
+        __syncwarp();  // every lane's sweep has read its pairs
+        if (act) {
+            const unsigned short* src = h16 + 2 * (OA + cap_excl) + prov;
+            for (int i = 0; i < khw; ++i) h16[excl + i] = src[i];
+        }
+        __syncwarp();
+        const unsigned* pw = W;
+        for (int i = lane; i < total; i += 32) {
+            const unsigned kv = pw[i];
+            const long long o = (long long)base + i;
+            if (o < A.capacity) {
+                A.out_begin[o] = xmin + (int)(kv & 0xFFFFu);
+                A.out_end[o] = xmin + (int)(kv >> 16);
+            } else {
+                over = true;
+            }
+        }
+    } else if (ok && act && piece == 0 && nint > 0) {
+        bool fb_bad = false;
+        sx_sweep_table<K, true>(A, s_row, lim_row, A.out_begin, A.out_end, (long long)base + (excl >> 1), fb_bad, over);
+    }
+    if (act && piece == LPR - 1) A.out_off[r0 + row + 1] = base + (incl >> 1);
+    if (tile == 0 && lane == 0) A.out_off[0] = 0;
+    (void)over;  // an output beyond the capacity shows in the reported total
+    sxs_report(A, tile, tiles, base, total, flags);
+}
+
 size_t sx_sweep_state_bytes(long long tiles)
 {
     const long long groups = (tiles + SX_GROUP - 1) / SX_GROUP;
@@ -2437,6 +2806,33 @@ static cudaError_t sx_wseg16_launch_k(const SxBoolArgs& A, const SxSweepState& s
     return cudaGetLastError();
 }
 
+template <int K, int LPR>
+static cudaError_t sx_rlane16_launch_kl(const SxBoolArgs& A, const SxSweepState& st, int tiles, int cap_words,
+                                        int warps, cudaStream_t stream)
+{
+    static int configured = 0;  // largest dynamic shared memory set for this instantiation
+    const int bytes = warps * (int)sxr_slice_bytes(cap_words);
+    if (bytes > configured) {
+        cudaError_t err =
+            cudaFuncSetAttribute(sx_rlane16_kernel<K, LPR>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        if (err != cudaSuccess) return err;
+        configured = bytes;
+    }
+    const int blocks = (tiles + warps - 1) / warps;
+    sx_rlane16_kernel<K, LPR><<<blocks, 32 * warps, bytes, stream>>>(A, st, tiles, cap_words);
+    return cudaGetLastError();
+}
+
+// Lanes per row from the tile height: 32 rows one lane each, 16 rows two, 8 rows four.
+template <int K>
+static cudaError_t sx_rlane16_launch_k(const SxBoolArgs& A, const SxSweepState& st, int tiles, int cap_words,
+                                       int warps, int tr, cudaStream_t stream)
+{
+    if (tr == 8) return sx_rlane16_launch_kl<K, 4>(A, st, tiles, cap_words, warps, stream);
+    if (tr == 16) return sx_rlane16_launch_kl<K, 2>(A, st, tiles, cap_words, warps, stream);
+    return sx_rlane16_launch_kl<K, 1>(A, st, tiles, cap_words, warps, stream);
+}
+
 // Segmented sweep shape: `keys` boundaries per tile (0: 1.25x the average
 // plus slack), stored twice (lists and output area), at most 200 KiB per
 // block; `warps` per block (0: about 48 boundaries per thread).
@@ -2488,6 +2884,7 @@ cudaError_t sx_sweep_launch(const SxBoolArgs& A, bool union_mode, void* workspac
     if (seg) {
         tr = A.tune_tile_rows > 0 ? A.tune_tile_rows : (A.tune_kernel == 4 ? 32 : 8);
         if (A.tune_kernel == 6 && tr > 8) tr = 8;  // 16-bit keys hold 3 row bits
+        if (A.tune_kernel == 7) tr = A.tune_tile_rows == 8 || A.tune_tile_rows == 32 ? A.tune_tile_rows : 16;
         if (sx_sweep_state_bytes(((long long)A.rows + tr - 1) / tr) > workspace_bytes) tr = 32;
     }
     const long long tiles = ((long long)A.rows + tr - 1) / tr;
@@ -2516,6 +2913,31 @@ cudaError_t sx_sweep_launch(const SxBoolArgs& A, bool union_mode, void* workspac
     // heavy tiles (measured best on the 4096x4096 shape expression).
     SxBoolArgs B = A;
     if (B.tune_kernel == 0) B.tune_kernel = 5;
+    if (B.tune_kernel == 7) {
+        // words per warp: the staged begins and ends (later pairs and outputs) of the largest tile
+        const long long avg = (2 * A.capacity + tiles - 1) / tiles;
+        const long long e = A.tune_staging_cap > 0 ? A.tune_staging_cap : avg + avg / 4 + 64;
+        long long words = e + 22 * A.k + 8 + sxr_gap_words(A.k);
+        const long long slice = 4 * (SXR_HDR_WORDS + words);
+        // about 50 KiB per block: small blocks pack the SM's shared memory closely
+        int warps = A.tune_warps > 0 ? A.tune_warps : (int)((50 * 1024) / slice);
+        if (warps > 4 && A.tune_warps <= 0) warps = 4;
+        if (warps < 1) warps = 1;
+        const long long limit = (200 * 1024) / warps / 4 - SXR_HDR_WORDS;
+        if (words > limit) words = limit;
+        const int cw = (int)words;
+        switch (A.k) {
+            case 1: return sx_rlane16_launch_k<1>(A, st, t, cw, warps, tr, stream);
+            case 2: return sx_rlane16_launch_k<2>(A, st, t, cw, warps, tr, stream);
+            case 3: return sx_rlane16_launch_k<3>(A, st, t, cw, warps, tr, stream);
+            case 4: return sx_rlane16_launch_k<4>(A, st, t, cw, warps, tr, stream);
+            case 5: return sx_rlane16_launch_k<5>(A, st, t, cw, warps, tr, stream);
+            case 6: return sx_rlane16_launch_k<6>(A, st, t, cw, warps, tr, stream);
+            case 7: return sx_rlane16_launch_k<7>(A, st, t, cw, warps, tr, stream);
+            case 8: return sx_rlane16_launch_k<8>(A, st, t, cw, warps, tr, stream);
+            default: return cudaErrorInvalidValue;
+        }
+    }
     if (B.tune_kernel == 6 && tr <= 8) {
         // words per warp: the staged begins and ends (later keys and outputs) of the largest tile
         const long long avg = (2 * A.capacity + tiles - 1) / tiles;

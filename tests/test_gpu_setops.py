@@ -249,7 +249,8 @@ def test_wide_coordinate_span_vs_oracle(cuda_device):
                                     {"kernel": 4, "tile_rows": 16}, {"kernel": 5}, {"kernel": 5, "tile_rows": 32},
                                     {"kernel": 5, "tile_rows": 1, "warps": 1}, {"kernel": 5, "staging_cap": 64},
                                     {"kernel": 6}, {"kernel": 6, "tile_rows": 3, "warps": 1},
-                                    {"kernel": 6, "staging_cap": 64}, {"kernel": 6, "tile_rows": 32}])
+                                    {"kernel": 6, "staging_cap": 64}, {"kernel": 6, "tile_rows": 32},
+                                    {"kernel": 7}, {"kernel": 7, "staging_cap": 64, "warps": 2}])
 def test_tuning_never_changes_results(cuda_device, tuning):
     from subsetix_b200 import _core
 

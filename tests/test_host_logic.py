@@ -30,7 +30,7 @@ def _one_leaf():
     return arr
 
 
-@pytest.mark.parametrize("field,value", [("kernel", 7), ("kernel", -1), ("warps", 9), ("tile_rows", 33),
+@pytest.mark.parametrize("field,value", [("kernel", 8), ("kernel", -1), ("warps", 9), ("tile_rows", 33),
                                          ("tile_rows", -2), ("staging_cap", -5), ("blocks_per_sm", -1),
                                          ("wait_limit", -1), ("withhold_tile", -3)])
 def test_bool_eval_rejects_bad_tuning_on_the_host(field, value):
@@ -44,6 +44,18 @@ def test_bool_eval_rejects_bad_tuning_on_the_host(field, value):
                           ctypes.byref(tun), None)
     assert rc == _lib.SX_ERR_INVALID
     assert "tuning" in _lib.last_error()
+
+
+def test_bool_eval_rejects_row_lane_tiles_of_other_heights_on_the_host():
+    lib = _lib_or_skip()
+    tun = _lib.SxTuning(7, 0, 0, 0, 12, 0, 0)
+    tab = (ctypes.c_uint32 * 8)(0b1110, 0, 0, 0, 0, 0, 0, 0)
+    rows = 64
+    ws = lib.sx_bool_workspace_bytes(rows)
+    rc = lib.sx_bool_eval(_one_leaf(), 1, rows, tab, _lib.MODE_TABLE, 16, 16, 16, 100, 16, 16, ws,
+                          ctypes.byref(tun), None)
+    assert rc == _lib.SX_ERR_INVALID
+    assert "32 rows" in _lib.last_error()
 
 
 def test_bool_eval_rejects_a_short_workspace_on_the_host():
@@ -96,10 +108,12 @@ def test_workload_key_buckets():
 
 def test_autotune_candidates_cover_every_kernel_kind():
     sizes = [40000] * 5
-    cands = autotune.candidates(sizes, 4096, largest_tile=5000, largest_eighth_tile=1300)
+    cands = autotune.candidates(sizes, 4096, largest_tile=5000, largest_eighth_tile=1300, largest_half_tile=2600)
     kinds = {c["kernel"] for c in cands}
-    assert {1, 3, 4, 5, 6} <= kinds
+    assert {1, 3, 4, 5, 6, 7} <= kinds
     for c in cands:
+        if c["kernel"] == 7:
+            assert c["tile_rows"] in (16, 32) and c["staging_cap"] >= (2600 if c["tile_rows"] == 16 else 5000)
         if c["kernel"] in (5, 6):
             assert c["tile_rows"] == 8 and 1300 <= c["staging_cap"] <= 25000
         if c["kernel"] == 4:
