@@ -339,7 +339,8 @@ def test_many_leaf_expressions(cuda_device, k, tuning):
     assert_same(got, O.evaluate(MANY[k], leaves_h), f"k={k} {tuning}")
 
 
-def test_lookback_wait_gives_up_and_reports_timeout(cuda_device):
+@pytest.mark.parametrize("kernel", [6, 7])
+def test_lookback_wait_gives_up_and_reports_timeout(cuda_device, kernel):
     """A tile that never publishes its look-back status: the tiles after it give up after a few polls,
     the sweep finishes and reports SX_FLAG_TIMEOUT, the public call raises, and the next regular call
     is exact (nothing hangs, the context stays usable)."""
@@ -350,8 +351,9 @@ def test_lookback_wait_gives_up_and_reports_timeout(cuda_device):
     B = rand_set(rows, 4.0, seed=32, row0=0)
     la, lb = dev_set(A), dev_set(B)
     specs = [(la.begin, la.end, la.row_offsets, 0), (lb.begin, lb.end, lb.row_offsets, 0)]
-    cap = _core.max_tile_boundaries(specs, rows, cuda_device, tile_rows=8)
-    tuning = {"kernel": 6, "tile_rows": 8, "warps": 2, "staging_cap": cap, "wait_limit": 256, "withhold_tile": 5}
+    tr = 8 if kernel == 6 else 16
+    cap = _core.max_tile_boundaries(specs, rows, cuda_device, tile_rows=tr)
+    tuning = {"kernel": kernel, "tile_rows": tr, "warps": 2, "staging_cap": cap, "wait_limit": 256, "withhold_tile": 5}
     table = [0b1110] + [0] * 7  # A | B over the state bits (A = 1, B = 2)
     _, _, _, result = _core.bool_eval_async(specs, rows, table, _lib.MODE_TABLE, cuda_device, tuning=tuning)
     total, flags = (int(x) for x in result.cpu())
