@@ -94,7 +94,7 @@ def auto_tuning(leaves, rows: int, device) -> dict:
     mean8 = 2 * sum(int(leaf[0].numel()) for leaf in leaves) / max(1, (rows + 7) // 8)
     if need8 <= 3 * mean8 + 256:
         if span16 <= 65534:
-            return {"kernel": 7, "staging_cap": min(need16, 25000), "tile_rows": 16, "warps": 4}
+            return {"kernel": 7, "staging_cap": min(need16, 25000), "tile_rows": 16, "warps": 2}
         return {"kernel": 5, "staging_cap": min(need8, 25000), "tile_rows": 8, "warps": 2}
     need32 = max_tile_boundaries(leaves, rows, device, tile_rows=32)
     return {"kernel": 4, "staging_cap": min(need32, 25000), "tile_rows": 32, "warps": 4}

@@ -40,7 +40,7 @@ def candidates(sizes: Sequence[int], rows: int, largest_tile: int = 0, largest_e
     # buffers for the largest tile when it is known (every tile then stays staged, and no slice is larger than
     # needed), else 1.25x the mean tile
     cap16 = min(int(largest_half_tile) or int(avg / 2 * 1.25 + 64), 25000)
-    for w in (1, 4):
+    for w in (1, 2, 4):
         out.append({"kernel": 7, "staging_cap": cap16, "warps": w, "tile_rows": 16})
     out.append({"kernel": 7, "staging_cap": min(int(largest_tile) or int(avg * 1.25 + 64), 25000), "warps": 1,
                 "tile_rows": 32})

@@ -2334,8 +2334,20 @@ __global__ void __launch_bounds__(256, K <= 5 ? 5 : 4) sx_wseg16_kernel(SxBoolAr
 #define SXR_SENTINEL 0xFFFFu
 #define SXR_HDR_WORDS 4
 
-// Words below the raw copies into which the padded pair lists grow.
-__host__ __device__ inline int sxr_gap_words(int k) { return (33 * k + 35) & ~3; }
+// Words below the raw copies into which the padded pair lists grow, for k
+// leaves and tiles of tr rows.  Leaf l's list starts at most l (tr - 7) words
+// further from the slice than its raw begins (each list holds its n pairs
+// plus tr + 1 spare words, each raw region at least n + 8 words), and a pair
+// lands at most tr - 1 words above its own index: (k - 1)(tr - 7) + tr
+// keeps every pair below the raw words not yet read.  The output areas
+// (n + tr words in all, after the lists) must also end inside the raw
+// region's 2 (n + 8 k) words: k (tr + 1) + tr - 16 k.
+__host__ __device__ inline int sxr_gap_words(int k, int tr)
+{
+    const int lists = (k - 1) * (tr - 7) + tr;
+    const int outputs = k * (tr + 1) + tr - 16 * k;
+    return ((lists > outputs ? lists : outputs) + 4 + 3) & ~3;
+}
 
 __host__ __device__ inline size_t sxr_slice_bytes(int cap_words)
 {
@@ -2387,7 +2399,7 @@ __global__ void __launch_bounds__(256) sx_rlane16_kernel(SxBoolArgs A, SxSweepSt
     unsigned long long* bar = (unsigned long long*)base_w;
     unsigned* const W = base_w + SXR_HDR_WORDS;  // pair lists, then the output areas
     unsigned short* const h16 = (unsigned short*)W;
-    const int gap = sxr_gap_words(K);
+    const int gap = sxr_gap_words(K, TR);
     unsigned* const raw = W + gap;  // the bulk copies
     const int row = lane / LPR, piece = lane % LPR;
     const int first_lane = row * LPR;
@@ -2917,10 +2929,10 @@ cudaError_t sx_sweep_launch(const SxBoolArgs& A, bool union_mode, void* workspac
         // words per warp: the staged begins and ends (later pairs and outputs) of the largest tile
         const long long avg = (2 * A.capacity + tiles - 1) / tiles;
         const long long e = A.tune_staging_cap > 0 ? A.tune_staging_cap : avg + avg / 4 + 64;
-        long long words = e + 22 * A.k + 8 + sxr_gap_words(A.k);
+        long long words = e + 22 * A.k + 8 + sxr_gap_words(A.k, tr);
         const long long slice = 4 * (SXR_HDR_WORDS + words);
-        // about 50 KiB per block: small blocks pack the SM's shared memory closely
-        int warps = A.tune_warps > 0 ? A.tune_warps : (int)((50 * 1024) / slice);
+        // about 25 KiB per block: small blocks pack the SM's shared memory closely and retire independently
+        int warps = A.tune_warps > 0 ? A.tune_warps : (int)((25 * 1024) / slice);
         if (warps > 4 && A.tune_warps <= 0) warps = 4;
         if (warps < 1) warps = 1;
         const long long limit = (200 * 1024) / warps / 4 - SXR_HDR_WORDS;
