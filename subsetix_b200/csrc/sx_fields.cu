@@ -890,25 +890,28 @@ __global__ void __launch_bounds__(256) sx_chunk_table_kernel(const int* __restri
 // cell, issued together with the cell's own value.
 // One chunk's update (the body of sx_upwind_chunk_kernel).  With EDGE false
 // the chunk's cells and their left and right neighbours all lie in
-// [0, width), so the domain tests are known to pass and are left out.
-template <typename T, bool TABLE, bool EDGE>
+// [0, width), so the domain tests are known to pass and are left out.  SGN
+// holds the upwind sides the velocity selects (bit 0: a >= 0, the left
+// neighbour; bit 1: b >= 0, the row below): the other side's neighbours are
+// never read, as in the reference's update, which uses one side per axis.
+template <typename T, bool TABLE, bool EDGE, int SGN>
 __device__ __forceinline__ void sx_chunk_upwind(const int4 p0, const int4 p1, const int4 p2, const int4 p3, int lane,
                                                 const int* __restrict__ b, const int* __restrict__ e,
                                                 const int* __restrict__ coff, const unsigned short* __restrict__ nbr,
                                                 const T* __restrict__ v, T* __restrict__ out, int width, T a, T bb,
                                                 T dt, T dx, T dy, int pow2)
 {
+    constexpr bool LEFT = (SGN & 1) != 0, DOWN = (SGN & 2) != 0;
     const int x0 = p0.x, ie = p0.y, touch = p0.w, ib = p3.w;
     const long long c0 = p0.z;
     // sub-rounds that hold cells (the same for the whole warp): chunks of
     // short intervals skip the empty ones instead of issuing them masked
     const int nq = min(SX_CHUNK_SUB, (ie - x0 + 31) >> 5);
     T cen[SX_CHUNK_SUB];
-    int idn[SX_CHUNK_SUB], iup[SX_CHUNK_SUB];
-    const SxRowReader dn{p1.x, p1.y, p1.z, p1.w, p2.x};
-    const SxRowReader upc{p2.y, p2.z, p2.w, p3.x, p3.y};
+    int inb[SX_CHUNK_SUB];  // value index of the neighbour in the row the velocity selects, -1 for none
+    const SxRowReader rd = DOWN ? SxRowReader{p1.x, p1.y, p1.z, p1.w, p2.x} : SxRowReader{p2.y, p2.z, p2.w, p3.x, p3.y};
     if (TABLE) {
-        const int bdn = sx_chunk_base(dn, x0), bup = sx_chunk_base(upc, x0);
+        const int base = sx_chunk_base(rd, x0);
         unsigned nb[SX_CHUNK_SUB];
 #pragma unroll
         for (int q = 0; q < SX_CHUNK_SUB; ++q) {
@@ -921,9 +924,8 @@ __device__ __forceinline__ void sx_chunk_upwind(const int4 p0, const int4 p1, co
         for (int q = 0; q < SX_CHUNK_SUB; ++q) {
             const int x = x0 + 32 * q + lane;
             const bool xin = !EDGE || (x >= 0 && x < width);
-            const unsigned lo = nb[q] & 0xFFu, hi = nb[q] >> 8;
-            idn[q] = (xin && lo != 0xFFu) ? bdn + (int)lo : -1;
-            iup[q] = (xin && hi != 0xFFu) ? bup + (int)hi : -1;
+            const unsigned o = DOWN ? nb[q] & 0xFFu : nb[q] >> 8;
+            inb[q] = (xin && o != 0xFFu) ? base + (int)o : -1;
         }
     } else {
 #pragma unroll
@@ -933,15 +935,11 @@ __device__ __forceinline__ void sx_chunk_upwind(const int4 p0, const int4 p1, co
         }
         // neighbour-row value indices of all four sub-rounds first, then all
         // their loads at once, so the chunk waits for one round trip
-        sx_row_indices<SX_CHUNK_SUB, EDGE>(dn, x0, nq, ie, width, b, e, coff, lane, idn);
-        sx_row_indices<SX_CHUNK_SUB, EDGE>(upc, x0, nq, ie, width, b, e, coff, lane, iup);
+        sx_row_indices<SX_CHUNK_SUB, EDGE>(rd, x0, nq, ie, width, b, e, coff, lane, inb);
     }
-    T vdn[SX_CHUNK_SUB], vup[SX_CHUNK_SUB];
+    T vnb[SX_CHUNK_SUB];
 #pragma unroll
-    for (int q = 0; q < SX_CHUNK_SUB; ++q) {
-        vdn[q] = idn[q] >= 0 ? v[idn[q]] : (T)0;
-        vup[q] = iup[q] >= 0 ? v[iup[q]] : (T)0;
-    }
+    for (int q = 0; q < SX_CHUNK_SUB; ++q) vnb[q] = inb[q] >= 0 ? v[inb[q]] : (T)0;
     T prev_last = (T)0;  // lane 31's centre of the previous sub-round
 #pragma unroll
     for (int q = 0; q < SX_CHUNK_SUB; ++q) {
@@ -950,30 +948,32 @@ __device__ __forceinline__ void sx_chunk_upwind(const int4 p0, const int4 p1, co
         const bool act = x < ie;
         const long long c = c0 + 32 * q + lane;
         const T center = cen[q];
-        T from_left = __shfl_up_sync(0xFFFFFFFFu, center, 1);
-        if (lane == 0) from_left = prev_last;
-        T from_right = __shfl_down_sync(0xFFFFFFFFu, center, 1);
-        const T next_first = q + 1 < SX_CHUNK_SUB ? __shfl_sync(0xFFFFFFFFu, cen[q + 1 < SX_CHUNK_SUB ? q + 1 : q], 0)
-                                                  : (T)0;
-        if (lane == 31) from_right = next_first;
-        prev_last = __shfl_sync(0xFFFFFFFFu, center, 31);
-        T left, right;
-        const bool lin = !EDGE || (x - 1 >= 0 && x - 1 < width), rin = !EDGE || (x + 1 >= 0 && x + 1 < width);
-        if (x - 1 >= ib) left = lin ? ((lane > 0 || q > 0) ? from_left : v[c - 1]) : (T)0;
-        else left = (act && (touch & 1) && lin) ? v[c - 1] : (T)0;
-        if (x + 1 < ie) right = rin ? ((lane < 31 || q + 1 < SX_CHUNK_SUB) ? from_right : v[c + 1]) : (T)0;
-        else right = (act && (touch & 2) && rin) ? v[c + 1] : (T)0;
-        const T down = vdn[q];
-        const T up = vup[q];
+        T side;  // the horizontal neighbour the velocity selects
+        if (LEFT) {
+            T from_left = __shfl_up_sync(0xFFFFFFFFu, center, 1);
+            if (lane == 0) from_left = prev_last;
+            prev_last = __shfl_sync(0xFFFFFFFFu, center, 31);
+            const bool lin = !EDGE || (x - 1 >= 0 && x - 1 < width);
+            if (x - 1 >= ib) side = lin ? ((lane > 0 || q > 0) ? from_left : v[c - 1]) : (T)0;
+            else side = (act && (touch & 1) && lin) ? v[c - 1] : (T)0;
+        } else {
+            T from_right = __shfl_down_sync(0xFFFFFFFFu, center, 1);
+            const T next_first =
+                q + 1 < SX_CHUNK_SUB ? __shfl_sync(0xFFFFFFFFu, cen[q + 1 < SX_CHUNK_SUB ? q + 1 : q], 0) : (T)0;
+            if (lane == 31) from_right = next_first;
+            const bool rin = !EDGE || (x + 1 >= 0 && x + 1 < width);
+            if (x + 1 < ie) side = rin ? ((lane < 31 || q + 1 < SX_CHUNK_SUB) ? from_right : v[c + 1]) : (T)0;
+            else side = (act && (touch & 2) && rin) ? v[c + 1] : (T)0;
+        }
         if (act) {
-            const T du_dx = a >= (T)0 ? sx_over(sx_sub(center, left), dx, pow2) : sx_over(sx_sub(right, center), dx, pow2);
-            const T du_dy = bb >= (T)0 ? sx_over(sx_sub(center, down), dy, pow2) : sx_over(sx_sub(up, center), dy, pow2);
+            const T du_dx = sx_over(LEFT ? sx_sub(center, side) : sx_sub(side, center), dx, pow2);
+            const T du_dy = sx_over(DOWN ? sx_sub(center, vnb[q]) : sx_sub(vnb[q], center), dy, pow2);
             out[c] = sx_upwind_update(center, du_dx, du_dy, a, bb, dt);
         }
     }
 }
 
-template <typename T, bool BANDS, bool TABLE>
+template <typename T, bool BANDS, bool TABLE, int SGN>
 __global__ void __launch_bounds__(256, TABLE ? (sizeof(T) == 4 ? SX_UPWIND_TABLE_MIN_BLOCKS : 3) : SX_UPWIND_MIN_BLOCKS)
     sx_upwind_chunk_kernel(const int* __restrict__ off, const int* __restrict__ b, const int* __restrict__ e,
                            const int* __restrict__ coff, const int* __restrict__ info, long long chunks,
@@ -1001,11 +1001,11 @@ __global__ void __launch_bounds__(256, TABLE ? (sizeof(T) == 4 ? SX_UPWIND_TABLE
         // interior chunk: every cell and its left and right neighbours inside [0, width)
         const bool edge = !(x0 >= 1 && x0 + min(ie - x0, SX_CHUNK) < width);  // x0 + ... <= ie: no overflow
         if (edge)
-            sx_chunk_upwind<T, TABLE, true>(p0, p1, p2, p3, lane, b, e, coff, nbr, v, out, width, a, bb, dt, dx, dy,
-                                            pow2);
+            sx_chunk_upwind<T, TABLE, true, SGN>(p0, p1, p2, p3, lane, b, e, coff, nbr, v, out, width, a, bb, dt, dx,
+                                                 dy, pow2);
         else
-            sx_chunk_upwind<T, TABLE, false>(p0, p1, p2, p3, lane, b, e, coff, nbr, v, out, width, a, bb, dt, dx, dy,
-                                             pow2);
+            sx_chunk_upwind<T, TABLE, false, SGN>(p0, p1, p2, p3, lane, b, e, coff, nbr, v, out, width, a, bb, dt, dx,
+                                                  dy, pow2);
     }
 }
 
@@ -1017,7 +1017,7 @@ __global__ void __launch_bounds__(256, TABLE ? (sizeof(T) == 4 ? SX_UPWIND_TABLE
 // into ga and gb.  With EDGE false the chunk's row lies in [0, height) and its
 // cells and their left and right neighbours in [0, width), so the domain tests
 // are known to pass and are left out.
-template <typename T, bool TABLE, bool EDGE>
+template <typename T, bool TABLE, bool EDGE, int SGN>
 __device__ __forceinline__ void sx_chunk_adjoint(const int4 p0, const int4 p1, const int4 p2, const int4 p3, int lane,
                                                  const int* __restrict__ b, const int* __restrict__ e,
                                                  const int* __restrict__ coff,
@@ -1059,13 +1059,14 @@ __device__ __forceinline__ void sx_chunk_adjoint(const int4 p0, const int4 p1, c
             iup[q] = sx_row_index(upr, x, width, b, e, coff, x < ie);
         }
     }
-    T wdn[SX_CHUNK_SUB], wup[SX_CHUNK_SUB], udn[SX_CHUNK_SUB], uup[SX_CHUNK_SUB];
+    // u is read on the forward's upwind side, w on the other one (SGN as in sx_chunk_upwind)
+    constexpr bool LEFT = (SGN & 1) != 0, DOWN = (SGN & 2) != 0;
+    T urow[SX_CHUNK_SUB], wrow[SX_CHUNK_SUB];
 #pragma unroll
     for (int q = 0; q < SX_CHUNK_SUB; ++q) {
-        udn[q] = idn[q] >= 0 ? u[idn[q]] : (T)0;
-        uup[q] = iup[q] >= 0 ? u[iup[q]] : (T)0;
-        wdn[q] = idn[q] >= 0 && rdom ? w[idn[q]] : (T)0;
-        wup[q] = iup[q] >= 0 && rdom ? w[iup[q]] : (T)0;
+        const int iu = DOWN ? idn[q] : iup[q], iw = DOWN ? iup[q] : idn[q];
+        urow[q] = iu >= 0 ? u[iu] : (T)0;
+        wrow[q] = iw >= 0 && rdom ? w[iw] : (T)0;
     }
     T wprev = (T)0, uprev = (T)0;
 #pragma unroll
@@ -1074,62 +1075,63 @@ __device__ __forceinline__ void sx_chunk_adjoint(const int4 p0, const int4 p1, c
         const bool act = x < ie;
         const long long c = c0 + 32 * q + lane;
         const bool jdom = !EDGE || (x >= 0 && x < width && row >= 0 && row < height);
-        T wl = __shfl_up_sync(0xFFFFFFFFu, wc[q], 1), ul = __shfl_up_sync(0xFFFFFFFFu, uc[q], 1);
-        if (lane == 0) {
-            wl = wprev;
-            ul = uprev;
-        }
-        T wr = __shfl_down_sync(0xFFFFFFFFu, wc[q], 1), ur = __shfl_down_sync(0xFFFFFFFFu, uc[q], 1);
-        const int qn = q + 1 < SX_CHUNK_SUB ? q + 1 : q;
-        const T wn = __shfl_sync(0xFFFFFFFFu, wc[qn], 0), un = __shfl_sync(0xFFFFFFFFu, uc[qn], 0);
-        if (lane == 31) {
-            wr = wn;
-            ur = un;
-        }
-        wprev = __shfl_sync(0xFFFFFFFFu, wc[q], 31);
-        uprev = __shfl_sync(0xFFFFFFFFu, uc[q], 31);
         const bool first = lane == 0 && q == 0, last = lane == 31 && q + 1 == SX_CHUNK_SUB;
-        // in-set values of w left and right (the transpose checks only this cell's domain)
-        T w_left, w_right, u_left, u_right;
-        if (x - 1 >= ib) {
-            w_left = first ? w[c - 1] : wl;
-            const T uv = first ? u[c - 1] : ul;
-            u_left = (!EDGE || (x - 1 >= 0 && x - 1 < width)) ? uv : (T)0;
-        } else {
-            const bool t = act && (touch & 1);
-            w_left = t ? w[c - 1] : (T)0;
-            u_left = (t && (!EDGE || (x - 1 >= 0 && x - 1 < width))) ? u[c - 1] : (T)0;
-        }
-        if (x + 1 < ie) {
-            w_right = last ? w[c + 1] : wr;
-            const T uv = last ? u[c + 1] : ur;
-            u_right = (!EDGE || (x + 1 >= 0 && x + 1 < width)) ? uv : (T)0;
-        } else {
-            const bool t = act && (touch & 2);
-            w_right = t ? w[c + 1] : (T)0;
-            u_right = (t && (!EDGE || (x + 1 >= 0 && x + 1 < width))) ? u[c + 1] : (T)0;
+        // in-set values of w on one side and u on the other (the transpose checks only this cell's domain)
+        T w_side, u_side;
+        if (LEFT) {  // u from the left, w from the right
+            T ul = __shfl_up_sync(0xFFFFFFFFu, uc[q], 1);
+            if (lane == 0) ul = uprev;
+            uprev = __shfl_sync(0xFFFFFFFFu, uc[q], 31);
+            T wr = __shfl_down_sync(0xFFFFFFFFu, wc[q], 1);
+            const int qn = q + 1 < SX_CHUNK_SUB ? q + 1 : q;
+            const T wn = __shfl_sync(0xFFFFFFFFu, wc[qn], 0);
+            if (lane == 31) wr = wn;
+            if (x - 1 >= ib) {
+                const T uv = first ? u[c - 1] : ul;
+                u_side = (!EDGE || (x - 1 >= 0 && x - 1 < width)) ? uv : (T)0;
+            } else {
+                const bool t = act && (touch & 1);
+                u_side = (t && (!EDGE || (x - 1 >= 0 && x - 1 < width))) ? u[c - 1] : (T)0;
+            }
+            if (x + 1 < ie) w_side = last ? w[c + 1] : wr;
+            else w_side = (act && (touch & 2)) ? w[c + 1] : (T)0;
+        } else {  // u from the right, w from the left
+            T wl = __shfl_up_sync(0xFFFFFFFFu, wc[q], 1);
+            if (lane == 0) wl = wprev;
+            wprev = __shfl_sync(0xFFFFFFFFu, wc[q], 31);
+            T ur = __shfl_down_sync(0xFFFFFFFFu, uc[q], 1);
+            const int qn = q + 1 < SX_CHUNK_SUB ? q + 1 : q;
+            const T un = __shfl_sync(0xFFFFFFFFu, uc[qn], 0);
+            if (lane == 31) ur = un;
+            if (x - 1 >= ib) w_side = first ? w[c - 1] : wl;
+            else w_side = (act && (touch & 1)) ? w[c - 1] : (T)0;
+            if (x + 1 < ie) {
+                const T uv = last ? u[c + 1] : ur;
+                u_side = (!EDGE || (x + 1 >= 0 && x + 1 < width)) ? uv : (T)0;
+            } else {
+                const bool t = act && (touch & 2);
+                u_side = (t && (!EDGE || (x + 1 >= 0 && x + 1 < width))) ? u[c + 1] : (T)0;
+            }
         }
         // rows above and below: w in-set needs jdom only (x is then inside the domain, so the
         // reader's domain test is the same), u needs the forward's domain test
-        const T w_dn = wdn[q], w_up = wup[q], u_dn = udn[q], u_up = uup[q];
+        const T w_r = wrow[q], u_r = urow[q];
         if (act) {
             const T c_w = wc[q];
-            T tx, ty;
-            if (a >= (T)0) tx = sx_over(sx_sub(c_w, jdom ? w_right : (T)0), dx, pow2);
-            else tx = sx_over(sx_sub(jdom ? w_left : (T)0, c_w), dx, pow2);
-            if (bb >= (T)0) ty = sx_over(sx_sub(c_w, w_up), dy, pow2);
-            else ty = sx_over(sx_sub(w_dn, c_w), dy, pow2);
+            const T tx = LEFT ? sx_over(sx_sub(c_w, jdom ? w_side : (T)0), dx, pow2)
+                              : sx_over(sx_sub(jdom ? w_side : (T)0, c_w), dx, pow2);
+            const T ty = DOWN ? sx_over(sx_sub(c_w, w_r), dy, pow2) : sx_over(sx_sub(w_r, c_w), dy, pow2);
             ubar[c] = sx_sub(c_w, sx_mul(dt, sx_add(sx_mul(a, tx), sx_mul(bb, ty))));
             const T c_u = uc[q];
-            const T dux = a >= (T)0 ? sx_over(sx_sub(c_u, u_left), dx, pow2) : sx_over(sx_sub(u_right, c_u), dx, pow2);
-            const T duy = bb >= (T)0 ? sx_over(sx_sub(c_u, u_dn), dy, pow2) : sx_over(sx_sub(u_up, c_u), dy, pow2);
+            const T dux = LEFT ? sx_over(sx_sub(c_u, u_side), dx, pow2) : sx_over(sx_sub(u_side, c_u), dx, pow2);
+            const T duy = DOWN ? sx_over(sx_sub(c_u, u_r), dy, pow2) : sx_over(sx_sub(u_r, c_u), dy, pow2);
             ga -= (double)dt * (double)c_w * (double)dux;
             gb -= (double)dt * (double)c_w * (double)duy;
         }
     }
 }
 
-template <typename T, bool TABLE>
+template <typename T, bool TABLE, int SGN>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? SX_UPWIND_ADJOINT_MIN_BLOCKS : 2) sx_upwind_adjoint_chunk_kernel(const int* __restrict__ off,
                                                                       const int* __restrict__ b,
                                                                       const int* __restrict__ e,
@@ -1152,11 +1154,11 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? SX_UPWIND_ADJOINT_MIN_BL
         const int x0 = p0.x, ie = p0.y, row = p3.z;
         const bool edge = !(row >= 0 && row < height && x0 >= 1 && x0 + min(ie - x0, SX_CHUNK) < width);
         if (edge)
-            sx_chunk_adjoint<T, TABLE, true>(p0, p1, p2, p3, lane, b, e, coff, nbr, w, u, ubar, width, height, a, bb,
-                                             dt, dx, dy, pow2, ga, gb);
+            sx_chunk_adjoint<T, TABLE, true, SGN>(p0, p1, p2, p3, lane, b, e, coff, nbr, w, u, ubar, width, height, a,
+                                                  bb, dt, dx, dy, pow2, ga, gb);
         else
-            sx_chunk_adjoint<T, TABLE, false>(p0, p1, p2, p3, lane, b, e, coff, nbr, w, u, ubar, width, height, a, bb,
-                                              dt, dx, dy, pow2, ga, gb);
+            sx_chunk_adjoint<T, TABLE, false, SGN>(p0, p1, p2, p3, lane, b, e, coff, nbr, w, u, ubar, width, height, a,
+                                                   bb, dt, dx, dy, pow2, ga, gb);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -1731,20 +1733,46 @@ cudaError_t sx_upwind_table_launch(const int* b, const int* e, const int* coff, 
     return cudaGetLastError();
 }
 
+// The upwind sides of the velocity (SGN) select the kernel instance.
+template <typename T, bool BANDS, int SGN>
+static void sx_upwind_chunk_go_s(int blocks, const int* off, const int* b, const int* e, const int* coff,
+                                 const int* info, long long chunks, const int* lookup, const T* v, T* out, int width,
+                                 int height, T a, T bb, T dt, T dx, T dy, int p, const int* row_band,
+                                 const T* band_table, int nbands, const unsigned short* nbr, cudaStream_t stream)
+{
+    if (nbr)
+        sx_upwind_chunk_kernel<T, BANDS, true, SGN><<<blocks, 256, 0, stream>>>(off, b, e, coff, info, chunks, lookup,
+                                                                               v, out, width, height, a, bb, dt, dx,
+                                                                               dy, p, row_band, band_table, nbands,
+                                                                               nbr);
+    else
+        sx_upwind_chunk_kernel<T, BANDS, false, SGN><<<blocks, 256, 0, stream>>>(off, b, e, coff, info, chunks,
+                                                                                lookup, v, out, width, height, a, bb,
+                                                                                dt, dx, dy, p, row_band, band_table,
+                                                                                nbands, nullptr);
+}
+
 template <typename T, bool BANDS>
 static void sx_upwind_chunk_go(int blocks, const int* off, const int* b, const int* e, const int* coff,
                                const int* info, long long chunks, const int* lookup, const T* v, T* out, int width,
                                int height, T a, T bb, T dt, T dx, T dy, int p, const int* row_band, const T* band_table,
                                int nbands, const unsigned short* nbr, cudaStream_t stream)
 {
-    if (nbr)
-        sx_upwind_chunk_kernel<T, BANDS, true><<<blocks, 256, 0, stream>>>(off, b, e, coff, info, chunks, lookup, v,
-                                                                          out, width, height, a, bb, dt, dx, dy, p,
-                                                                          row_band, band_table, nbands, nbr);
-    else
-        sx_upwind_chunk_kernel<T, BANDS, false><<<blocks, 256, 0, stream>>>(off, b, e, coff, info, chunks, lookup, v,
-                                                                           out, width, height, a, bb, dt, dx, dy, p,
-                                                                           row_band, band_table, nbands, nullptr);
+    const int sgn = (a >= (T)0 ? 1 : 0) | (bb >= (T)0 ? 2 : 0);
+    switch (sgn) {
+        case 0: return sx_upwind_chunk_go_s<T, BANDS, 0>(blocks, off, b, e, coff, info, chunks, lookup, v, out, width,
+                                                         height, a, bb, dt, dx, dy, p, row_band, band_table, nbands,
+                                                         nbr, stream);
+        case 1: return sx_upwind_chunk_go_s<T, BANDS, 1>(blocks, off, b, e, coff, info, chunks, lookup, v, out, width,
+                                                         height, a, bb, dt, dx, dy, p, row_band, band_table, nbands,
+                                                         nbr, stream);
+        case 2: return sx_upwind_chunk_go_s<T, BANDS, 2>(blocks, off, b, e, coff, info, chunks, lookup, v, out, width,
+                                                         height, a, bb, dt, dx, dy, p, row_band, band_table, nbands,
+                                                         nbr, stream);
+        default: return sx_upwind_chunk_go_s<T, BANDS, 3>(blocks, off, b, e, coff, info, chunks, lookup, v, out,
+                                                          width, height, a, bb, dt, dx, dy, p, row_band, band_table,
+                                                          nbands, nbr, stream);
+    }
 }
 
 static int sx_chunk_blocks(long long chunks)
@@ -1822,20 +1850,41 @@ int sx_upwind_adjoint_chunk_parts(long long chunks)
     return (int)blocks;
 }
 
+template <typename T, int SGN>
+static void sx_upwind_adjoint_chunk_go_s(int blocks, const int* off, const int* b, const int* e, const int* coff,
+                                         const int* info, long long chunks, const int* lookup,
+                                         const unsigned short* nbr, const T* w, const T* u, T* ubar, int width,
+                                         int height, T a, T bb, T dt, T dx, T dy, int p, double* partial,
+                                         cudaStream_t stream)
+{
+    if (nbr)
+        sx_upwind_adjoint_chunk_kernel<T, true, SGN><<<blocks, 256, 0, stream>>>(off, b, e, coff, info, chunks, lookup,
+                                                                                 nbr, w, u, ubar, width, height, a, bb,
+                                                                                 dt, dx, dy, p, partial);
+    else
+        sx_upwind_adjoint_chunk_kernel<T, false, SGN><<<blocks, 256, 0, stream>>>(off, b, e, coff, info, chunks,
+                                                                                  lookup, nullptr, w, u, ubar, width,
+                                                                                  height, a, bb, dt, dx, dy, p,
+                                                                                  partial);
+}
+
+// The upwind sides of the velocity select the kernel instance (as in the forward step).
 template <typename T>
 static void sx_upwind_adjoint_chunk_go(int blocks, const int* off, const int* b, const int* e, const int* coff,
                                        const int* info, long long chunks, const int* lookup, const unsigned short* nbr,
                                        const T* w, const T* u, T* ubar, int width, int height, T a, T bb, T dt, T dx,
                                        T dy, int p, double* partial, cudaStream_t stream)
 {
-    if (nbr)
-        sx_upwind_adjoint_chunk_kernel<T, true><<<blocks, 256, 0, stream>>>(off, b, e, coff, info, chunks, lookup, nbr,
-                                                                            w, u, ubar, width, height, a, bb, dt, dx,
-                                                                            dy, p, partial);
-    else
-        sx_upwind_adjoint_chunk_kernel<T, false><<<blocks, 256, 0, stream>>>(off, b, e, coff, info, chunks, lookup,
-                                                                             nullptr, w, u, ubar, width, height, a, bb,
-                                                                             dt, dx, dy, p, partial);
+    switch ((a >= (T)0 ? 1 : 0) | (bb >= (T)0 ? 2 : 0)) {
+        case 0: return sx_upwind_adjoint_chunk_go_s<T, 0>(blocks, off, b, e, coff, info, chunks, lookup, nbr, w, u,
+                                                          ubar, width, height, a, bb, dt, dx, dy, p, partial, stream);
+        case 1: return sx_upwind_adjoint_chunk_go_s<T, 1>(blocks, off, b, e, coff, info, chunks, lookup, nbr, w, u,
+                                                          ubar, width, height, a, bb, dt, dx, dy, p, partial, stream);
+        case 2: return sx_upwind_adjoint_chunk_go_s<T, 2>(blocks, off, b, e, coff, info, chunks, lookup, nbr, w, u,
+                                                          ubar, width, height, a, bb, dt, dx, dy, p, partial, stream);
+        default: return sx_upwind_adjoint_chunk_go_s<T, 3>(blocks, off, b, e, coff, info, chunks, lookup, nbr, w, u,
+                                                           ubar, width, height, a, bb, dt, dx, dy, p, partial, stream);
+    }
 }
 
 cudaError_t sx_upwind_adjoint_chunk_launch(const int* off, const int* b, const int* e, const int* coff, const int* info,

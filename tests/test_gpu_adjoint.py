@@ -134,7 +134,7 @@ def test_checkpoint_spacing_and_fp32(cuda_device):
         assert float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b)) < 1e-5
 
 
-@pytest.mark.parametrize("a,b", [(0.7, 0.4), (-0.5, -0.9)])
+@pytest.mark.parametrize("a,b", [(0.7, 0.4), (-0.5, -0.9), (0.7, -0.4), (-0.5, 0.9)])  # every upwind side
 @pytest.mark.parametrize("table", [True, False])
 def test_chunked_adjoint_equals_generic(cuda_device, a, b, table):
     from subsetix_b200 import _lib

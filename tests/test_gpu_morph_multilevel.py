@@ -300,7 +300,7 @@ def test_upwind_chunked_equals_generic(cuda_device, dtype):
         chunk_off, chunks = _core.upwind_plan(rows, off, b, e, coff, lookup, H, dev)
         table = _core.upwind_table(b, e, coff, chunk_off, chunks, cells, dev)
         v = torch.as_tensor(rng.standard_normal(cells), device=dev).to(dtype)
-        for a_, b_ in ((0.6, 0.3), (-0.4, -0.9)):
+        for a_, b_ in ((0.6, 0.3), (-0.4, -0.9), (0.6, -0.3), (-0.4, 0.9), (0.0, -0.0)):  # every upwind side
             ref = torch.empty_like(v)
             _core.upwind(rows, off, b, e, coff, cells, lookup, v, ref, W, H, a_, b_, 1e-3, 1e-2, 1e-2, False, dev)
             for tab in (None, table):  # neighbour rows searched, then read from the plan's table
