@@ -57,7 +57,19 @@ __device__ __forceinline__ T sxa_over(T x, T d, int pow2)
 }
 
 // One thread per cell; x fastest.  blockIdx.z is the batch entry.
-template <typename T>
+// The upwind update of one cell from the neighbours the velocity selects:
+// SGN bit 0 (a >= 0) the left one in h, else the right one; bit 1 (b >= 0)
+// the one below in v, else the one above.  The reference's formula uses one
+// side per axis, so the other side is never read.
+template <typename T, int SGN>
+__device__ __forceinline__ T sxa_upwind_side(T c, T h, T v, T a, T b, T dt, T dx, T dy, int pow2)
+{
+    const T du_dx = (SGN & 1) ? sxa_over(sxa_sub(c, h), dx, pow2) : sxa_over(sxa_sub(h, c), dx, pow2);
+    const T du_dy = (SGN & 2) ? sxa_over(sxa_sub(c, v), dy, pow2) : sxa_over(sxa_sub(v, c), dy, pow2);
+    return sx_upwind_update(c, du_dx, du_dy, a, b, dt);
+}
+
+template <typename T, int SGN>
 __global__ void __launch_bounds__(256) sx_upwind_full_kernel(const T* __restrict__ in, T* __restrict__ out, int W,
                                                              int H, T a, T b, T dt, T dx, T dy, int pow2)
 {
@@ -69,13 +81,9 @@ __global__ void __launch_bounds__(256) sx_upwind_full_kernel(const T* __restrict
     if (x >= W) return;
     const long long idx = (long long)y * W + x;
     const T c = v[idx];
-    const T l = x > 0 ? v[idx - 1] : (T)0;
-    const T r = x + 1 < W ? v[idx + 1] : (T)0;
-    const T d = y > 0 ? v[idx - W] : (T)0;
-    const T u = y + 1 < H ? v[idx + W] : (T)0;
-    const T du_dx = a >= (T)0 ? sxa_over(sxa_sub(c, l), dx, pow2) : sxa_over(sxa_sub(r, c), dx, pow2);
-    const T du_dy = b >= (T)0 ? sxa_over(sxa_sub(c, d), dy, pow2) : sxa_over(sxa_sub(u, c), dy, pow2);
-    o[idx] = sx_upwind_update(c, du_dx, du_dy, a, b, dt);
+    const T h = (SGN & 1) ? (x > 0 ? v[idx - 1] : (T)0) : (x + 1 < W ? v[idx + 1] : (T)0);
+    const T w = (SGN & 2) ? (y > 0 ? v[idx - W] : (T)0) : (y + 1 < H ? v[idx + W] : (T)0);
+    o[idx] = sxa_upwind_side<T, SGN>(c, h, w, a, b, dt, dx, dy, pow2);
 }
 
 // One thread per coarse cell.  R is the refinement ratio (template for the
@@ -111,16 +119,9 @@ __global__ void __launch_bounds__(256) sx_amr_sync_full_kernel(T* __restrict__ c
 // synchronisation of that coarse cell with its block.  A step's
 // synchronisation of a coarse cell reads only that cell's and that block's
 // new values, so this equals upwind(coarse); upwind(fine); sync, value for
-// value.  in/out are distinct buffers.
-template <typename T>
-__device__ __forceinline__ T sxa_upwind_cell(T c, T l, T r, T d, T u, T a, T b, T dt, T dx, T dy, int pow2)
-{
-    const T du_dx = a >= (T)0 ? sxa_over(sxa_sub(c, l), dx, pow2) : sxa_over(sxa_sub(r, c), dx, pow2);
-    const T du_dy = b >= (T)0 ? sxa_over(sxa_sub(c, d), dy, pow2) : sxa_over(sxa_sub(u, c), dy, pow2);
-    return sx_upwind_update(c, du_dx, du_dy, a, b, dt);
-}
-
-template <typename T>
+// value.  in/out are distinct buffers.  SGN: the velocity's upwind sides, as
+// in sxa_upwind_side.
+template <typename T, int SGN>
 __global__ void __launch_bounds__(256) sx_amr_step_full_kernel(const T* __restrict__ cin, const T* __restrict__ fin,
                                                                T* __restrict__ cout, T* __restrict__ fout,
                                                                const signed char* __restrict__ actions, int W, int H,
@@ -135,13 +136,11 @@ __global__ void __launch_bounds__(256) sx_amr_step_full_kernel(const T* __restri
     const T* C = cin + plane * blockIdx.z;
     const T* F = fin + 4 * plane * blockIdx.z;
     const long long ci = (long long)y * W + x;
-    // coarse cell
+    // coarse cell, with the neighbours the velocity selects
     const T c = C[ci];
-    const T cl = x > 0 ? C[ci - 1] : (T)0;
-    const T cr = x + 1 < W ? C[ci + 1] : (T)0;
-    const T cd = y > 0 ? C[ci - W] : (T)0;
-    const T cu = y + 1 < H ? C[ci + W] : (T)0;
-    const T cn = sxa_upwind_cell(c, cl, cr, cd, cu, a, b, dt, dxc, dyc, pow2c);
+    const T ch = (SGN & 1) ? (x > 0 ? C[ci - 1] : (T)0) : (x + 1 < W ? C[ci + 1] : (T)0);
+    const T cv = (SGN & 2) ? (y > 0 ? C[ci - W] : (T)0) : (y + 1 < H ? C[ci + W] : (T)0);
+    const T cn = sxa_upwind_side<T, SGN>(c, ch, cv, a, b, dt, dxc, dyc, pow2c);
     const int fx = 2 * x, fy = 2 * y;
     T* CO = cout + plane * blockIdx.z;
     T* FO = fout + 4 * plane * blockIdx.z;
@@ -157,7 +156,8 @@ __global__ void __launch_bounds__(256) sx_amr_step_full_kernel(const T* __restri
         }
         return;
     }
-    // refined: fine block, rows 2y-1 .. 2y+2, columns 2x-1 .. 2x+2
+    // refined: fine block, rows 2y-1 .. 2y+2, columns 2x-1 .. 2x+2; only the
+    // 2 x 2 block and the column and row on its upwind sides are read
     T v[4][4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
@@ -165,8 +165,11 @@ __global__ void __launch_bounds__(256) sx_amr_step_full_kernel(const T* __restri
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
             const int xx = fx - 1 + i;
-            const bool corner = (j == 0 || j == 3) && (i == 0 || i == 3);
-            v[j][i] = (!corner && yy >= 0 && yy < FH && xx >= 0 && xx < FW) ? F[(long long)yy * FW + xx] : (T)0;
+            const bool inner_row = j == 1 || j == 2, inner_col = i == 1 || i == 2;
+            const bool needed = (inner_row && inner_col) ||
+                                (inner_row && (((SGN & 1) && i == 0) || (!(SGN & 1) && i == 3))) ||
+                                (inner_col && (((SGN & 2) && j == 0) || (!(SGN & 2) && j == 3)));
+            v[j][i] = (needed && yy >= 0 && yy < FH && xx >= 0 && xx < FW) ? F[(long long)yy * FW + xx] : (T)0;
         }
     }
     T fn[2][2];
@@ -174,8 +177,8 @@ __global__ void __launch_bounds__(256) sx_amr_step_full_kernel(const T* __restri
     for (int j = 0; j < 2; ++j)
 #pragma unroll
         for (int i = 0; i < 2; ++i)
-            fn[j][i] = sxa_upwind_cell(v[j + 1][i + 1], v[j + 1][i], v[j + 1][i + 2], v[j][i + 1], v[j + 2][i + 1], a, b,
-                                       dt, dxf, dyf, pow2f);
+            fn[j][i] = sxa_upwind_side<T, SGN>(v[j + 1][i + 1], (SGN & 1) ? v[j + 1][i] : v[j + 1][i + 2],
+                                               (SGN & 2) ? v[j][i + 1] : v[j + 2][i + 1], a, b, dt, dxf, dyf, pow2f);
     T acc = sxa_add(sxa_add(sxa_add(sxa_add((T)0, fn[0][0]), fn[0][1]), fn[1][0]), fn[1][1]);
     CO[ci] = sxa_mul(acc, norm);
 #pragma unroll
@@ -259,6 +262,44 @@ static int sxa_pow2_pair(T& dx, T& dy)
     return 1;
 }
 
+// Kernel instances by the velocity's upwind sides, tested in the kernel's precision.
+template <typename T>
+static void sxa_upwind_full_go(dim3 g, const T* in, T* out, int W, int H, T a, T b, T dt, T dx, T dy, int p,
+                               cudaStream_t stream)
+{
+    switch ((a >= (T)0 ? 1 : 0) | (b >= (T)0 ? 2 : 0)) {
+        case 0: sx_upwind_full_kernel<T, 0><<<g, 256, 0, stream>>>(in, out, W, H, a, b, dt, dx, dy, p); break;
+        case 1: sx_upwind_full_kernel<T, 1><<<g, 256, 0, stream>>>(in, out, W, H, a, b, dt, dx, dy, p); break;
+        case 2: sx_upwind_full_kernel<T, 2><<<g, 256, 0, stream>>>(in, out, W, H, a, b, dt, dx, dy, p); break;
+        default: sx_upwind_full_kernel<T, 3><<<g, 256, 0, stream>>>(in, out, W, H, a, b, dt, dx, dy, p); break;
+    }
+}
+
+template <typename T>
+static void sxa_step_full_go(dim3 g, const T* cin, const T* fin, T* cout, T* fout, const signed char* actions, int W,
+                             int H, T a, T b, T dt, T cx, T cy, T fx, T fy, T norm, int pc, int pf,
+                             cudaStream_t stream)
+{
+    switch ((a >= (T)0 ? 1 : 0) | (b >= (T)0 ? 2 : 0)) {
+        case 0:
+            sx_amr_step_full_kernel<T, 0><<<g, 256, 0, stream>>>(cin, fin, cout, fout, actions, W, H, a, b, dt, cx, cy,
+                                                                 fx, fy, norm, pc, pf);
+            break;
+        case 1:
+            sx_amr_step_full_kernel<T, 1><<<g, 256, 0, stream>>>(cin, fin, cout, fout, actions, W, H, a, b, dt, cx, cy,
+                                                                 fx, fy, norm, pc, pf);
+            break;
+        case 2:
+            sx_amr_step_full_kernel<T, 2><<<g, 256, 0, stream>>>(cin, fin, cout, fout, actions, W, H, a, b, dt, cx, cy,
+                                                                 fx, fy, norm, pc, pf);
+            break;
+        default:
+            sx_amr_step_full_kernel<T, 3><<<g, 256, 0, stream>>>(cin, fin, cout, fout, actions, W, H, a, b, dt, cx, cy,
+                                                                 fx, fy, norm, pc, pf);
+            break;
+    }
+}
+
 cudaError_t sx_upwind_full_launch(int dbl, const void* in, void* out, int W, int H, int batch, double a, double b,
                                   double dt, double dx, double dy, cudaStream_t stream)
 {
@@ -266,13 +307,12 @@ cudaError_t sx_upwind_full_launch(int dbl, const void* in, void* out, int W, int
     if (dbl) {
         double ddx = dx, ddy = dy;
         const int p = sxa_pow2_pair(ddx, ddy);
-        sx_upwind_full_kernel<double><<<g, 256, 0, stream>>>((const double*)in, (double*)out, W, H, a, b, dt, ddx, ddy,
-                                                             p);
+        sxa_upwind_full_go<double>(g, (const double*)in, (double*)out, W, H, a, b, dt, ddx, ddy, p, stream);
     } else {
         float fdx = (float)dx, fdy = (float)dy;
         const int p = sxa_pow2_pair(fdx, fdy);
-        sx_upwind_full_kernel<float><<<g, 256, 0, stream>>>((const float*)in, (float*)out, W, H, (float)a, (float)b,
-                                                            (float)dt, fdx, fdy, p);
+        sxa_upwind_full_go<float>(g, (const float*)in, (float*)out, W, H, (float)a, (float)b, (float)dt, fdx, fdy, p,
+                                  stream);
     }
     return cudaGetLastError();
 }
@@ -320,15 +360,13 @@ cudaError_t sx_amr_step_full_launch(int dbl, const void* cin, const void* fin, v
     if (dbl) {
         double cx = dxc, cy = dyc, fx = dxf, fy = dyf;
         const int pc = sxa_pow2_pair(cx, cy), pf = sxa_pow2_pair(fx, fy);
-        sx_amr_step_full_kernel<double><<<g, 256, 0, stream>>>((const double*)cin, (const double*)fin, (double*)cout,
-                                                               (double*)fout, actions, W, H, a, b, dt, cx, cy, fx, fy,
-                                                               0.25, pc, pf);
+        sxa_step_full_go<double>(g, (const double*)cin, (const double*)fin, (double*)cout, (double*)fout, actions, W,
+                                 H, a, b, dt, cx, cy, fx, fy, 0.25, pc, pf, stream);
     } else {
         float cx = (float)dxc, cy = (float)dyc, fx = (float)dxf, fy = (float)dyf;
         const int pc = sxa_pow2_pair(cx, cy), pf = sxa_pow2_pair(fx, fy);
-        sx_amr_step_full_kernel<float><<<g, 256, 0, stream>>>((const float*)cin, (const float*)fin, (float*)cout,
-                                                              (float*)fout, actions, W, H, (float)a, (float)b,
-                                                              (float)dt, cx, cy, fx, fy, 0.25f, pc, pf);
+        sxa_step_full_go<float>(g, (const float*)cin, (const float*)fin, (float*)cout, (float*)fout, actions, W, H,
+                                (float)a, (float)b, (float)dt, cx, cy, fx, fy, 0.25f, pc, pf, stream);
     }
     return cudaGetLastError();
 }

@@ -146,27 +146,29 @@ def test_batched_uneven_sets_against_oracle(cuda_device):
         pos += exp.size
 
 
+@pytest.mark.parametrize("velocity", [(0.9, -0.4), (-0.6, -0.8), (0.5, 0.7), (-0.8, 0.3)])  # every upwind side
 @pytest.mark.parametrize("res", [32, 40])
-def test_power_of_two_spacing_matches_division(cuda_device, res):
+def test_power_of_two_spacing_matches_division(cuda_device, res, velocity):
     # res 32 has power-of-two spacings (multiplication by the exact reciprocal),
     # res 40 does not (division); both must equal the FP64 oracle and AMR2Simulation
     u0 = _gauss(res, 0.08)
-    ref = O.AMR2(res, (0.9, -0.4), cfl=0.5, threshold=0.05, grading_pad=1, dtype=np.float64)
+    ref = O.AMR2(res, velocity, cfl=0.5, threshold=0.05, grading_pad=1, dtype=np.float64)
     ref.init(u0)
     ref.run(6, 3)
-    eng = FusedTwoLevelAMR(torch.as_tensor(u0, device="cuda"), velocity=(0.9, -0.4), cfl=0.5, dtype=torch.float64)
+    eng = FusedTwoLevelAMR(torch.as_tensor(u0, device="cuda"), velocity=velocity, cfl=0.5, dtype=torch.float64)
     eng.run(6, regrid_every=3)
     np.testing.assert_array_equal(_vals(eng.fine_values).reshape(-1), ref.fine.values)
 
 
+@pytest.mark.parametrize("velocity", [(0.8, -0.6), (-0.5, -0.7)])
 @pytest.mark.parametrize("res", [40, 70, 300])
 @pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
-def test_fused_step_any_width(cuda_device, res, dtype):
+def test_fused_step_any_width(cuda_device, res, dtype, velocity):
     # widths that leave partial warps and blocks: the one-kernel step equals the separate kernels
     u0 = torch.as_tensor(_gauss(res, 0.07), device="cuda")
     runs = []
     for fused in (True, False):
-        eng = FusedTwoLevelAMR(u0, velocity=(0.8, -0.6), cfl=0.5, refine_threshold=0.05 / res, grading=1,
+        eng = FusedTwoLevelAMR(u0, velocity=velocity, cfl=0.5, refine_threshold=0.05 / res, grading=1,
                                dtype=dtype, fused=fused)
         eng.run(9, regrid_every=4, graph=False)
         runs.append(eng)
