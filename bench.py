@@ -66,7 +66,7 @@ def parse():
     p.add_argument("--no-amr", action="store_true", help="skip the AMR, adjoint and batched sections")
     p.add_argument("--no-autotune", action="store_true", help="use the automatic launch choice")
     p.add_argument("--batched-sets", type=int, default=256, help="sets in the batched section (smaller for profiling)")
-    p.add_argument("--section", default="all", choices=["all", "setops", "amr", "adjoint", "batched"],
+    p.add_argument("--section", default="all", choices=["all", "setops", "amr", "adjoint", "batched", "kernels"],
                    help="run one part alone (profiling); setops = the headline launch only")
     return p.parse_args()
 
@@ -394,6 +394,72 @@ def amr_section(device, steps: int = 200, every: int = 10, res: int = 1024, thre
     return out
 
 
+def kernels_section(device, copies: int = 4, res: int = 8192):
+    """Every interval kernel of the path once, after one warm-up pass: morphology and multilevel operations on the
+    64-px checkerboard of the 4096x4096 shapes (``copies`` stacked copies, every row non-empty), and the regrid,
+    upwind, subset, mass and VTK operations on a ``res``^2 Gaussian as an interval field.  This is the command of
+    the per-kernel ncu table (device time and DRAM bytes of every launch); the wall times it prints include the
+    public calls' host work and are not benchmark figures."""
+    import torch
+
+    from subsetix_b200 import _core
+    from subsetix_b200.subsetix_amr2 import fields as FD
+    from subsetix_b200.subsetix_amr2 import regrid as RG
+    from subsetix_b200.subsetix_cupy import expressions as E
+    from subsetix_b200.subsetix_cupy import export_vtk as VTK
+    from subsetix_b200.subsetix_cupy import interval_stencil as ST
+    from subsetix_b200.subsetix_cupy import morphology as M
+    from subsetix_b200.subsetix_cupy import multilevel as ML
+    from subsetix_b200.subsetix_cupy.interval_field import create_interval_field
+
+    C = E.IntervalSet._trusted(*(torch.as_tensor(a, device=device) for a in workload(copies)[2]))
+    H = 4096 * copies
+    xs = (torch.arange(res, device=device, dtype=torch.float32) + 0.5) / res
+    gauss = torch.exp(-((xs[None, :] - 0.5) ** 2 + (xs[:, None] - 0.5) ** 2) / (2 * 0.05 ** 2)).reshape(-1)
+    full = E.IntervalSet._trusted(torch.zeros(res, dtype=torch.int32, device=device),
+                                  torch.full((res,), res, dtype=torch.int32, device=device),
+                                  torch.arange(res + 1, dtype=torch.int32, device=device),
+                                  torch.arange(res, dtype=torch.int32, device=device))
+    dx = 1.0 / res
+    dt = 0.5 / (1.0 / dx + 0.5 / dx)
+
+    def ops():
+        out = {}
+        for r in (1, 2, 4):
+            out[f"dilate{r}"] = lambda r=r: M.dilate_interval_set(C, halo_x=r, halo_y=r)
+        out["erode1"] = lambda: M.erode_interval_set(C, 1, 1, width=4096, height=H)
+        out["prolong_set2"] = lambda: ML.prolong_set(C, 2)
+        out["restrict_set2"] = lambda: ML.restrict_set(fine, 2)
+        out["prolong_field2"] = lambda: ML.prolong_field(cf, 2)
+        out["restrict_field2"] = lambda: ML.restrict_field(pf, 2)
+        out["upwind"] = lambda: ST.step_upwind_interval(gf, width=res, height=res, a=1.0, b=0.5, dt=dt, dx=dx, dy=dx)
+        out["gradient"] = lambda: RG.gradient_magnitude_interval_field(gf, width=res, height=res)
+        out["gradient_tag"] = lambda: RG.gradient_tag_threshold_set(gf, width=res, height=res, threshold=0.05 * dx)
+        out["grading"] = lambda: RG.enforce_two_level_grading_set(tag, padding=1, width=res, height=res)
+        out["gather"] = lambda: FD.gather_interval_subset(gf, tag)
+        out["mass"] = lambda: _core.mass_integral(gf.values, dx * dx, device)
+        out["vtk_quads"] = lambda: VTK.interval_field_quads(gf, 0, dx, dx)
+        return out
+
+    fine = ML.prolong_set(C, 2)
+    cf = create_interval_field(C, fill_value=1.0)
+    pf = ML.prolong_field(cf, 2)
+    gf = create_interval_field(full, fill_value=0.0)
+    gf.values.copy_(gauss)
+    tag = RG.gradient_tag_threshold_set(gf, width=res, height=res, threshold=0.05 * dx)
+    for fn in ops().values():  # warm-up: plans, tables and buffers of each operation
+        fn()
+    times = {}
+    for name, fn in ops().items():
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        fn()
+        torch.cuda.synchronize()
+        times[name] = round((time.perf_counter() - t0) * 1e3, 3)
+    return {"copies": copies, "checkerboard_intervals": int(C.begin.numel()), "field_cells": res * res,
+            "refined_intervals": int(tag.begin.numel()), "wall_ms": times}
+
+
 def adjoint_section(device, base: int = 2048, steps: int = 50, every: int = 10, directions: int = 32):
     """Adjoint advection on fixed three-level composite geometry.
 
@@ -627,12 +693,12 @@ def main():
         dist.init_process_group("nccl", init_method="env://", timeout=timedelta(seconds=120),
                                 device_id=device)
 
-    if args.section in ("amr", "adjoint", "batched"):
+    if args.section in ("amr", "adjoint", "batched", "kernels"):
         # one section alone (profiling runs); prints that section's JSON object
         if args.section == "batched":
             out = batched_section(device, count=args.batched_sets)
         else:
-            out = {"amr": amr_section, "adjoint": adjoint_section}[args.section](device)
+            out = {"amr": amr_section, "adjoint": adjoint_section, "kernels": kernels_section}[args.section](device)
         if rank == 0:
             print(json.dumps({args.section: out}), flush=True)
         if world > 1:
