@@ -175,13 +175,15 @@ __global__ void sx_prolong_set_intervals_kernel(const int* __restrict__ b, const
 // as the reference's alignment check does).  Coarse interval i (ordinal o
 // in row ordinal p) maps in sub-row d to the fine interval
 // f = fine_off[p*r + d] + o, and fine cell k of f takes coarse cell k / r.
-// One warp handles one coarse interval.
+// One warp handles one coarse interval.  RT > 0 fixes the ratio at compile
+// time (2, the common one: k / r becomes a shift), RT = 0 takes r.
 // ---------------------------------------------------------------------------
-template <typename T>
+template <typename T, int RT>
 __global__ void sx_prolong_field_kernel(const int* __restrict__ off, int rows, const int* __restrict__ coff, int n,
-                                        const int* __restrict__ foff_rows, const int* __restrict__ fcoff, int r,
+                                        const int* __restrict__ foff_rows, const int* __restrict__ fcoff, int rr,
                                         const T* __restrict__ cv, T* __restrict__ fv)
 {
+    const int r = RT > 0 ? RT : rr;
     const int lane = threadIdx.x & 31;
     const int warps = (gridDim.x * blockDim.x) >> 5;
     const long long ncells = coff[n];
@@ -244,11 +246,13 @@ __global__ void sx_restrict_check_kernel(const int* __restrict__ crows, int crow
     }
 }
 
-template <typename T>
+// RT as in sx_prolong_field_kernel.
+template <typename T, int RT>
 __global__ void sx_restrict_field_kernel(const int* __restrict__ coff_rows, int crow_count, const int* __restrict__ ccoff,
-                                         int cn, const int* __restrict__ foff_rows, const int* __restrict__ fcoff, int r,
-                                         int reducer, T norm, const T* __restrict__ fv, T* __restrict__ cv)
+                                         int cn, const int* __restrict__ foff_rows, const int* __restrict__ fcoff,
+                                         int rr, int reducer, T norm, const T* __restrict__ fv, T* __restrict__ cv)
 {
+    const int r = RT > 0 ? RT : rr;
     const int lane = threadIdx.x & 31;
     const int warps = (gridDim.x * blockDim.x) >> 5;
     for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < cn; i += warps) {
@@ -1559,12 +1563,21 @@ cudaError_t sx_prolong_field_launch(const int* off, int rows, const int* coff, i
                                     const int* fcoff, int r, const void* cv, void* fv, int dbl, cudaStream_t stream)
 {
     const int grid = sx_grid((long long)n * 32, 256);
-    if (dbl)
-        sx_prolong_field_kernel<double><<<grid, 256, 0, stream>>>(off, rows, coff, n, foff_rows, fcoff, r,
-                                                                  (const double*)cv, (double*)fv);
-    else
-        sx_prolong_field_kernel<float><<<grid, 256, 0, stream>>>(off, rows, coff, n, foff_rows, fcoff, r,
-                                                                 (const float*)cv, (float*)fv);
+    if (dbl) {
+        if (r == 2)
+            sx_prolong_field_kernel<double, 2><<<grid, 256, 0, stream>>>(off, rows, coff, n, foff_rows, fcoff, r,
+                                                                         (const double*)cv, (double*)fv);
+        else
+            sx_prolong_field_kernel<double, 0><<<grid, 256, 0, stream>>>(off, rows, coff, n, foff_rows, fcoff, r,
+                                                                         (const double*)cv, (double*)fv);
+    } else {
+        if (r == 2)
+            sx_prolong_field_kernel<float, 2><<<grid, 256, 0, stream>>>(off, rows, coff, n, foff_rows, fcoff, r,
+                                                                        (const float*)cv, (float*)fv);
+        else
+            sx_prolong_field_kernel<float, 0><<<grid, 256, 0, stream>>>(off, rows, coff, n, foff_rows, fcoff, r,
+                                                                        (const float*)cv, (float*)fv);
+    }
     return cudaGetLastError();
 }
 
@@ -1583,12 +1596,25 @@ cudaError_t sx_restrict_field_launch(const int* coff_rows, int crow_count, const
                                      const void* fv, void* cv, int dbl, cudaStream_t stream)
 {
     const int grid = sx_grid((long long)cn * 32, 256);
-    if (dbl)
-        sx_restrict_field_kernel<double><<<grid, 256, 0, stream>>>(coff_rows, crow_count, ccoff, cn, foff_rows, fcoff, r,
-                                                                   reducer, norm, (const double*)fv, (double*)cv);
-    else
-        sx_restrict_field_kernel<float><<<grid, 256, 0, stream>>>(coff_rows, crow_count, ccoff, cn, foff_rows, fcoff, r,
-                                                                  reducer, (float)norm, (const float*)fv, (float*)cv);
+    if (dbl) {
+        if (r == 2)
+            sx_restrict_field_kernel<double, 2><<<grid, 256, 0, stream>>>(coff_rows, crow_count, ccoff, cn, foff_rows,
+                                                                          fcoff, r, reducer, norm, (const double*)fv,
+                                                                          (double*)cv);
+        else
+            sx_restrict_field_kernel<double, 0><<<grid, 256, 0, stream>>>(coff_rows, crow_count, ccoff, cn, foff_rows,
+                                                                          fcoff, r, reducer, norm, (const double*)fv,
+                                                                          (double*)cv);
+    } else {
+        if (r == 2)
+            sx_restrict_field_kernel<float, 2><<<grid, 256, 0, stream>>>(coff_rows, crow_count, ccoff, cn, foff_rows,
+                                                                         fcoff, r, reducer, (float)norm,
+                                                                         (const float*)fv, (float*)cv);
+        else
+            sx_restrict_field_kernel<float, 0><<<grid, 256, 0, stream>>>(coff_rows, crow_count, ccoff, cn, foff_rows,
+                                                                         fcoff, r, reducer, (float)norm,
+                                                                         (const float*)fv, (float*)cv);
+    }
     return cudaGetLastError();
 }
 
