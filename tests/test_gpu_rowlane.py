@@ -207,3 +207,24 @@ def test_tuning_rejects_other_tile_heights(cuda_device):
     finally:
         _core.TUNING.clear()
         _core.TUNING.update(saved)
+
+
+@pytest.mark.parametrize("x0", [2**31 - 70000, -2**31 + 5])
+def test_coordinates_next_to_the_int32_limits(cuda_device, x0):
+    """Narrow tiles (staged, 16-bit offsets from the tile's xmin) whose coordinates lie next to INT_MAX or INT_MIN."""
+    rng = np.random.default_rng(17)
+    rows = 80
+    leaves = [_rows(rng, rows, 6.0, x0=x0, spread=200, gap=7.0 + l, length=5.0 + l) for l in range(3)]
+    assert all(int(leaf[1].max()) < 2**31 - 1 for leaf in leaves)
+    words = [sum(1 << s for s in range(8) if (s & 1) and not (s & 4)) | (1 << 2)] + [0] * 7  # (A - C) | (B alone)
+    bits = np.array([(words[0] >> s) & 1 for s in range(8)])
+    width = max(int(leaf[1].max()) - x0 + 1 for leaf in leaves)
+    masks = [_masks(leaf, rows, x0, width) for leaf in leaves]
+    state = sum(m.astype(np.int64) << l for l, m in enumerate(masks))
+    want = _runs(bits[state].astype(bool), 0)
+    for tr in (8, 16, 32):
+        got_b, got_e, got_off, flags = _table_eval(leaves, rows, words, {"kernel": 7, "tile_rows": tr}, cuda_device)
+        assert flags == 0
+        np.testing.assert_array_equal(got_b.astype(np.int64) - x0, want[0])
+        np.testing.assert_array_equal(got_e.astype(np.int64) - x0, want[1])
+        np.testing.assert_array_equal(got_off, want[2])
